@@ -1,0 +1,334 @@
+"""Benchmark: Mrays/s of the cloud march at 1920x1080 (three layers, 128
+primary + 6 light steps), one primary ray per pixel, march + composite.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--storage f16|u8|f32|bf16|fp8] [--schedule plain|fast]
+
+One process per GPU (torchrun for N > 1).  The forward march has no exchange
+step, so each rank renders its own full frame of the sequence (weak scaling);
+time is the max over ranks of the device-timed step.  `--impl reference`
+times the CPU restatement of the reference's FP32 march on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s at 1080p, FP16-stored vs FP32 march at <=1e-3 rel err; % L2/tex roofline"
+UNIT = "Mrays/s"
+WORKLOAD = "precision_1080p"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f16")
+    ap.add_argument("--schedule", default="plain", choices=["plain", "fast"])
+    ap.add_argument("--filter", default="exact", choices=["exact", "texture"])
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for s in self.samples for n, v in zip(names, s[5:9]) if v == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def bytes_per_ray(storage: str) -> dict:
+    """Algorithmic texel bytes per primary ray of this workload (executed
+    fetches counted by the instrumented CPU restatement on the same scene,
+    committed in tests/golden/fetch_counts.json) in this kernel's formats."""
+    p = ROOT / "tests" / "golden" / "fetch_counts.json"
+    if not p.exists():
+        return {}
+    d = json.loads(p.read_text()).get(WORKLOAD)
+    if not d:
+        return {}
+    tex = {"u8": 4, "fp8": 4, "f16": 8, "bf16": 8, "f32": 16}[storage]
+    c = d["counts"]
+    per_kind = {
+        "weather": 4 * 4, "type": 1, "base": 8 * tex, "curl": 4 * 2, "detail": 8 * tex,
+        "light": 8 * tex, "trans": 4 * 16, "sky": 4 * 16, "ap": 8 * 16, "blue": 4, "depth": 4,
+    }
+    total = sum(c[k] * v for k, v in per_kind.items()) + c["pixels"] * (32 + 32)
+    return {"bytes_per_ray": total / c["pixels"], "pixels": c["pixels"],
+            "dense_per_ray": c["dense"] / c["pixels"], "steps_per_ray": c["steps"] / c["pixels"]}
+
+
+def cpu_baseline(scene, sample_rows: int, reps: int = 1):
+    """The FP32 CPU restatement on a bounded row sample; returns (rays/s, rays, threads)."""
+    from oracle import pyoracle
+    noise = pyoracle.bake_noise()
+    luts = pyoracle.bake_luts(scene.frame, scene.world)
+    h = scene.height
+    step = max(1, h // sample_rows)
+    rows = list(range(0, h, step))[:sample_rows]
+    threads = os.cpu_count() or 1
+    # bands of consecutive rows spread over the image: `rows` start rows
+    band = max(1, sample_rows // 8)
+    starts = np.linspace(0, h - band, 8).astype(int)
+    times = []
+    rays = 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        rays = 0
+        for r0 in starts:
+            pyoracle.render(scene, noise, luts, precision=pyoracle.FP32, threads=threads,
+                            rows=(int(r0), int(r0) + band))
+            rays += band * scene.width
+        times.append(time.perf_counter() - t0)
+    del rows
+    return rays / float(np.median(times)), rays, threads, float(np.median(times))
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from pedalsky_b200 import scenes
+    s = scenes.precision_1080p(args.width, args.height)
+    sample = 64  # rows per step
+    for _ in range(args.warmup):
+        cpu_baseline(s, sample)
+    vals = []
+    for _ in range(args.steps):
+        v, rays, threads, secs = cpu_baseline(s, sample)
+        vals.append(v)
+    value = float(np.median(vals)) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * args.width * args.height / (value * 1e6),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded reference noise hash, reference synthesis)",
+        "impl": "reference",
+        "config": {"workload": f"{WORKLOAD} {args.width}x{args.height}", "layers": 3,
+                   "primary_steps": 128, "light_steps": 6,
+                   "note": "CPU restatement of the reference FP32 march (the reference's WGSL "
+                           "cannot run here: no graphics stack)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{rays} rays per step (8 row bands of the 1080p frame)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from pedalsky_b200 import capi, scenes
+    from pedalsky_b200.capi import call
+    from pedalsky_b200.subsystem import subsystem_for_scene
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    storage = capi.STORAGE_NAMES[args.storage]
+    schedule = capi.SCHED_FAST if args.schedule == "fast" else capi.SCHED_PLAIN
+    filt = capi.FILTER_TEXTURE if args.filter == "texture" else capi.FILTER_EXACT
+    W, H = args.width, args.height
+    # each rank renders frame `rank` of the sequence (weak scaling)
+    s = scenes.precision_1080p(W, H, storage=storage, schedule=schedule, filt=filt)
+    s.frame.frame_index = rank
+    sub = subsystem_for_scene(s, device=local, luts=None)  # noise + LUTs baked on the device
+    stream = torch.cuda.Stream(device=dev)
+    sh = C.c_void_p(stream.cuda_stream)
+
+    L = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    T = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    bg = torch.from_numpy(s.background).to(dev)
+    hdr = torch.empty_like(bg)
+    depth = torch.from_numpy(s.depth).to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    o = capi.MarchOptions.from_buffer_copy(sub.options)
+    o.composite = 1
+    sub.set_options(o)
+    view = capi.View(W, H, depth.data_ptr(), L.data_ptr(), T.data_ptr(), hdr.data_ptr())
+
+    def step():
+        hdr.copy_(bg, non_blocking=True)
+        call("psc_render", sub.handle, C.byref(view), 1, sh)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    launches0 = sub.launch_count()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.zero_()                      # evict L2 between timed steps
+                hdr.copy_(bg, non_blocking=True)
+                evs[i][0].record(stream)
+                call("psc_render", sub.handle, C.byref(view), 1, sh)
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    ms = float(np.mean(step_ms))
+    kernel_launches = sub.launch_count() - launches0
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * W * H / (ms_max * 1e-3) / 1e6
+
+    # end to end through the C ABI with host buffers: pinned H2D of the
+    # depth and background, march + composite, D2H of the composited frame.
+    h_bg = torch.from_numpy(s.background).pin_memory()
+    h_depth = torch.from_numpy(s.depth).pin_memory()
+    h_out = torch.empty_like(h_bg).pin_memory()
+    e2e_ms = []
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup + args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            hdr.copy_(h_bg, non_blocking=True)
+            depth.copy_(h_depth, non_blocking=True)
+            call("psc_render", sub.handle, C.byref(view), 1, sh)
+            h_out.copy_(hdr, non_blocking=True)
+            b.record(stream)
+            b.synchronize()
+            if i >= args.warmup:
+                e2e_ms.append(a.elapsed_time(b))
+    te = torch.tensor([float(np.mean(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * W * H / (float(te.item()) * 1e-3) / 1e6
+    h2d = h_bg.numel() * 4 + h_depth.numel() * 4
+    d2h = h_out.numel() * 4
+
+    if rank == 0:
+        peaks = {}
+        pk = ROOT / "MEASURED_PEAKS.json"
+        if pk.exists():
+            peaks = json.loads(pk.read_text())
+        hbm = peaks.get("hbm_gbs")
+        bpr = bytes_per_ray(args.storage)
+        roof = None
+        if bpr:
+            achieved = bpr["bytes_per_ray"] * W * H / (ms_max * 1e-3) / 1e9
+            peak = hbm if hbm else 6650.0
+            roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_source": "measured" if hbm else "fallback",
+                    "bytes_per_ray": bpr["bytes_per_ray"],
+                    "note": "algorithmic texel bytes of executed fetches; the noise/LUT working "
+                            "set is L2-resident, so these are served from L1/L2, not HBM"}
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                v, rays, threads, secs = cpu_baseline(s, 64)
+                cpu = {"value": v / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+                       "sample": f"{rays} rays (8 row bands of the 1080p frame), {secs:.1f} s"}
+            except Exception as e:  # the baseline is reported, never the product
+                cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                       "sample": f"failed: {e}"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded reference noise hash, reference synthesis)",
+            "config": {"workload": f"{WORKLOAD} {W}x{H}", "layers": 3, "primary_steps": 128,
+                       "light_steps": 6, "storage": args.storage, "schedule": args.schedule,
+                       "filter": args.filter, "composite": "fused",
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"views{world}"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": kernel_launches,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "step_ms": [round(x, 4) for x in step_ms],
+        }
+        print(json.dumps(line), flush=True)
+    sub.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,415 @@
+/*
+ * psclouds.h — C ABI of the B200-native volumetric cloud march.
+ *
+ * This library is a drop-in for PedalSky's `ps-clouds` march + composite
+ * pass.  In the reference that pass sits behind the `RenderSubsystem` trait
+ * (crates/ps-core/src/subsystem.rs:66-118) and is implemented by
+ * `CloudsSubsystem` (crates/ps-clouds/src/lib.rs:95); its device side is the
+ * WGSL fragment shader `fs_main` (shaders/clouds/cloud_march.wgsl:731-1054)
+ * plus the composite (shaders/clouds/cloud_composite.wgsl:48-57).
+ *
+ * Conventions
+ *   - Every entry point returns an `int` status: PSC_OK (0) or a negative
+ *     PSC_ERR_* code.  `psc_last_error()` returns a thread-local message for
+ *     the last failure on the calling thread.  Nothing throws or aborts
+ *     across this boundary.
+ *   - A `psc_ctx` is single-threaded: one caller thread drives it, like the
+ *     reference's `&mut self` subsystem.  Work is enqueued on the caller's
+ *     `cudaStream_t`, passed as `void*` (NULL = legacy default stream).
+ *   - Device output buffers are caller-owned device pointers.  Host inputs
+ *     are copied into context-owned device memory by the upload calls.
+ *   - The uniform structs below are byte-identical to the reference's
+ *     std140 layouts (sizes and offsets pinned by static asserts here and by
+ *     the reference's tests crates/ps-clouds/src/params.rs:220-231,
+ *     crates/ps-core/src/weather.rs:537-555, crates/ps-app/tests/wgsl_layout.rs).
+ */
+#ifndef PSCLOUDS_H
+#define PSCLOUDS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSC_ABI_VERSION 1u
+
+/* ---------------------------------------------------------------- status */
+enum {
+  PSC_OK = 0,
+  PSC_ERR_INVALID_ARGUMENT = -1, /* null pointer, zero size, bad enum      */
+  PSC_ERR_NOT_FINITE = -2,       /* NaN / Inf in a parameter or uniform    */
+  PSC_ERR_LAYERS = -3,           /* >8 layers, top <= base, overlapping    */
+  PSC_ERR_MISSING_INPUT = -4,    /* render before noise / LUTs / weather   */
+  PSC_ERR_CUDA = -5,             /* a CUDA runtime call failed             */
+  PSC_ERR_OUT_OF_MEMORY = -6,
+  PSC_ERR_TIMEOUT = -7,          /* a bounded device wait gave up          */
+  PSC_ERR_UNSUPPORTED = -8,      /* mode not built / not available         */
+  PSC_ERR_DEVICE_CHECK = -9      /* device-side bounds check tripped       */
+};
+
+/* --------------------------------------------------- reference constants */
+#define PSC_MAX_CLOUD_LAYERS 8u          /* cloud_uniforms.wgsl:8           */
+#define PSC_BASE_NOISE_SIZE 128u         /* noise.rs BASE_SIZE              */
+#define PSC_DETAIL_NOISE_SIZE 32u        /* noise.rs DETAIL_SIZE            */
+#define PSC_CURL_NOISE_SIZE 128u         /* noise.rs CURL_SIZE              */
+#define PSC_BLUE_NOISE_SIZE 64u          /* noise.rs BLUE_NOISE_SIZE        */
+#define PSC_TRANSMITTANCE_W 256u         /* atmosphere_luts.rs:16           */
+#define PSC_TRANSMITTANCE_H 64u
+#define PSC_MULTISCATTER_W 32u
+#define PSC_MULTISCATTER_H 32u
+#define PSC_SKYVIEW_W 192u
+#define PSC_SKYVIEW_H 108u
+#define PSC_AP_W 32u
+#define PSC_AP_H 32u
+#define PSC_AP_D 64u
+#define PSC_WIND_X 32u                   /* wind_field.rs:36-41             */
+#define PSC_WIND_Y 16u
+#define PSC_WIND_Z 32u
+#define PSC_TYPE_SENTINEL 255u           /* cloud_type_grid.rs SENTINEL     */
+
+/* ------------------------------------------------- byte-exact uniforms */
+
+/* Mirrors `CloudParamsGpu` (crates/ps-clouds/src/params.rs:33-140) and WGSL
+ * `CloudParams` (shaders/clouds/cloud_uniforms.wgsl:23-83). 112 bytes. */
+typedef struct PscCloudParamsGpu {
+  float sigma_s[3];
+  float _pad_after_sigma_s;
+  float sigma_a[3];
+  float droplet_diameter_bias;
+  uint32_t cone_light_sampling;
+  float forward_bias;
+  float detail_strength;
+  float curl_strength;
+  float powder_strength;
+  float multi_scatter_a;
+  float multi_scatter_b;
+  float multi_scatter_c;
+  float ambient_strength;
+  float base_scale_m;
+  float detail_scale_m;
+  float weather_scale_m;
+  uint32_t light_steps;
+  uint32_t cloud_steps;
+  uint32_t multi_scatter_octaves;
+  uint32_t cloud_layer_count;
+  uint32_t temporal_jitter;
+  float wind_drift_strength;
+  float wind_skew_strength;
+  float diurnal_strength;
+} PscCloudParamsGpu;
+
+/* Mirrors `CloudLayerGpu` (crates/ps-core/src/weather.rs:100-134) and WGSL
+ * `CloudLayerGpu` (shaders/clouds/cloud_uniforms.wgsl:85-106). 48 bytes. */
+typedef struct PscCloudLayerGpu {
+  float base_m;
+  float top_m;
+  float coverage;
+  float density_scale;
+  uint32_t cloud_type;
+  float shape_bias;
+  float detail_bias;
+  float anvil_bias;
+  float droplet_diameter_um;
+  float _pad_after_droplets_0;
+  float _pad_after_droplets_1;
+  float _pad_after_droplets_2;
+} PscCloudLayerGpu;
+
+/* Mirrors `FrameUniformsGpu` (crates/ps-core/src/frame_uniforms.rs:121-160)
+ * and WGSL `FrameUniforms` (shaders/common/uniforms.wgsl:11-33).  Matrices
+ * are column-major (`m[col][row]`).  448 bytes. */
+typedef struct PscFrameUniformsGpu {
+  float view[4][4];
+  float proj[4][4];
+  float view_proj[4][4];
+  float inv_view_proj[4][4];
+  float camera_position_world[4];
+  float camera_velocity_world[4];
+  float sun_direction[4];          /* xyz dir, w angular radius (rad)   */
+  float sun_illuminance[4];        /* rgb illuminance, w TOA lux         */
+  float lightning_illuminance[4];  /* rgb emission, w falloff radius (m) */
+  float lightning_origin_world[4];
+  float viewport_size[4];          /* w, h, 1/w, 1/h                     */
+  float time_seconds;
+  float simulated_seconds;
+  uint32_t frame_index;
+  float ev100;
+  float prev_view_proj[4][4];
+} PscFrameUniformsGpu;
+
+/* Mirrors `AtmosphereParams` / `WorldUniformsGpu`
+ * (crates/ps-core/src/weather.rs:23-58, defaults :60-84) and WGSL
+ * `WorldUniforms` (shaders/common/uniforms.wgsl:39-58).  144 bytes. */
+typedef struct PscWorldUniformsGpu {
+  float planet_radius_m;
+  float atmosphere_top_m;
+  float rayleigh_scale_height_m;
+  float mie_scale_height_m;
+  float rayleigh_scattering[4];
+  float mie_scattering[4];
+  float mie_absorption[4];
+  float mie_g;
+  float _pad_after_mie_g[3];
+  float ozone_absorption[4];
+  float ozone_center_m;
+  float ozone_thickness_m;
+  float _pad_after_ozone[2];
+  float ground_albedo[4];
+  float haze_extinction_per_m[4];
+} PscWorldUniformsGpu;
+
+/* ------------------------------------------------ extension settings */
+
+/* Phase function used by the multi-scatter octave loop. */
+enum {
+  PSC_PHASE_APPROX_MIE = 0, /* reference: Jendersie & d'Eon 2023 fit,
+                               cloud_march.wgsl:256-296                    */
+  PSC_PHASE_DUAL_LOBE_HG = 1 /* mix(HG(gf*c^n), HG(gb*c^n), blend)        */
+};
+
+/* Storage form of the base/detail noise volumes on the device. */
+enum {
+  PSC_STORAGE_U8 = 0,   /* RGBA8 unorm, the reference's own format (exact) */
+  PSC_STORAGE_F32 = 1,  /* float4 per texel (the plain FP32 drop-in)      */
+  PSC_STORAGE_F16 = 2,  /* half4, per-volume scale 1/255 (exact)          */
+  PSC_STORAGE_BF16 = 3, /* bf16x4, per-volume scale 1/255 (exact)         */
+  PSC_STORAGE_FP8 = 4   /* e4m3x4, per-volume scale (lossy experiment)    */
+};
+
+/* How the noise volumes are filtered. */
+enum {
+  PSC_FILTER_EXACT = 0, /* FP32 trilinear weights from point loads        */
+  PSC_FILTER_TEXTURE = 1 /* texture-unit trilinear (8-bit fixed weights)  */
+};
+
+/* Kernel schedule. */
+enum {
+  PSC_SCHED_PLAIN = 0,     /* straight restatement, one thread per ray      */
+  PSC_SCHED_FAST = 1       /* hoisted per-ray constants, lane-compacted
+                              dense shading, fast transcendentals          */
+};
+
+/* Settings the reference does not expose in `CloudParamsGpu`.  Zero-filled
+ * means "reference behaviour" except where a default is stated. */
+typedef struct PscMarchOptions {
+  uint32_t phase_mode;      /* PSC_PHASE_*                                */
+  float hg_g_forward;       /* dual-lobe HG only (default 0.8)            */
+  float hg_g_backward;      /* dual-lobe HG only (default -0.2)           */
+  float hg_blend;           /* dual-lobe HG only (default 0.5)            */
+  uint32_t storage;         /* PSC_STORAGE_*                              */
+  uint32_t filter;          /* PSC_FILTER_*                               */
+  uint32_t schedule;        /* PSC_SCHED_*                                */
+  uint32_t kahan;           /* 1: compensated optical-depth sums          */
+  uint32_t composite;       /* 1: fuse `hdr = L + hdr*T` into the march   */
+  uint32_t debug_checks;    /* 1: bounds-check every texel index          */
+  uint32_t tile_w;          /* CTA tile width in pixels (0 = default)     */
+  uint32_t tile_h;          /* CTA tile height in pixels (0 = default)    */
+  uint32_t _reserved[4];
+} PscMarchOptions;
+
+/* One view to render.  `depth` is an optional D32F reverse-Z buffer
+ * (width*height floats, device, 0 = sky); NULL means "sky everywhere",
+ * matching a headless render with no opaque geometry. */
+typedef struct PscView {
+  uint32_t width;
+  uint32_t height;
+  const float* depth;          /* device, nullable                       */
+  float* out_luminance;        /* device, width*height*4 floats (RGBA)   */
+  float* out_transmittance;    /* device, width*height*4 floats (RGBA)   */
+  float* hdr;                  /* device, RGBA, read-modify-write when
+                                  options.composite = 1; else unused     */
+} PscView;
+
+/* Noise volume kinds for upload/download. */
+enum {
+  PSC_NOISE_BASE = 0,    /* 128^3 RGBA8                                  */
+  PSC_NOISE_DETAIL = 1,  /* 32^3 RGBA8                                   */
+  PSC_NOISE_CURL = 2,    /* 128^2 RG8                                    */
+  PSC_NOISE_BLUE = 3     /* 64^2 R8                                      */
+};
+
+/* LUT kinds for upload. */
+enum {
+  PSC_LUT_TRANSMITTANCE = 0, /* 256x64 RGBA16F                           */
+  PSC_LUT_MULTISCATTER = 1,  /* 32x32 RGBA16F                            */
+  PSC_LUT_SKYVIEW = 2,       /* 192x108 RGBA16F                          */
+  PSC_LUT_AERIAL = 3         /* 32x32x64 RGBA16F                         */
+};
+
+/* Weather-map texel formats (only the R channel is read by the march). */
+enum {
+  PSC_WEATHER_RGBA16F = 0,   /* reference: 128^2 RGBA16F (weather_map.rs)*/
+  PSC_WEATHER_RG8 = 1,       /* 2 x unorm8 per texel                     */
+  PSC_WEATHER_R32F = 2       /* 1 float per texel                        */
+};
+
+/* ------------------------------------------------------- diagnostics */
+const char* psc_last_error(void);
+uint32_t psc_abi_version(void);
+size_t psc_sizeof_params(void);     /* 112 */
+size_t psc_sizeof_layer(void);      /* 48  */
+size_t psc_sizeof_frame(void);      /* 448 */
+size_t psc_sizeof_world(void);      /* 144 */
+
+/* ----------------------------------------------- defaults and helpers */
+
+/* `CloudParamsGpu::default()` (crates/ps-clouds/src/params.rs:142-212). */
+int psc_params_default(PscCloudParamsGpu* out);
+/* `AtmosphereParams::default()` (crates/ps-core/src/weather.rs:60-84). */
+int psc_world_default(PscWorldUniformsGpu* out);
+/* Reference-behaviour options: approx-Mie, U8 storage, exact filtering,
+ * plain schedule, no composite fusion. */
+int psc_options_default(PscMarchOptions* out);
+
+/* Scene-side cloud layer (`CloudLayer`, crates/ps-core/src/scene.rs:410-480).
+ * Negative `density_scale` / `anvil_bias` / `droplet_diameter_um` select
+ * the per-type defaults (the reference's `None`). */
+typedef struct PscCloudLayerDesc {
+  uint32_t cloud_type;        /* 0..7: Cu St Sc Ac As Ci Cs Cb           */
+  float base_m;
+  float top_m;
+  float coverage;
+  float density_scale;
+  float shape_octave_bias;
+  float detail_octave_bias;
+  float anvil_bias;
+  float droplet_diameter_um;
+} PscCloudLayerDesc;
+
+/* `synthesise_cloud_layers` + `check_non_overlap`
+ * (crates/ps-synthesis/src/cloud_layers.rs:44-74,136-150). */
+int psc_synthesise_layers(const PscCloudLayerDesc* layers, uint32_t n,
+                          PscCloudLayerGpu* out);
+
+/* `FlyCamera` (crates/ps-core/src/camera.rs:11-71) plus
+ * `FrameUniforms::{set_matrices,set_sun}` as used by the headless render
+ * (crates/ps-app/src/test_harness.rs:335-390). */
+typedef struct PscFlyCamera {
+  float position[3];
+  float pitch_rad;
+  float yaw_rad;
+  float roll_rad;
+  float fov_y_rad;
+  float near_m;
+} PscFlyCamera;
+
+int psc_frame_from_camera(const PscFlyCamera* cam, uint32_t width,
+                          uint32_t height, float sun_altitude_rad,
+                          float sun_azimuth_rad, float sun_angular_radius_rad,
+                          float toa_illuminance_lux,
+                          PscFrameUniformsGpu* out);
+
+/* CPU void-and-cluster blue noise (crates/ps-clouds/src/noise.rs:646-704),
+ * 64*64 bytes. */
+int psc_generate_blue_noise(uint8_t* out_4096);
+
+/* Reference weather map: 128^2 RGBA16F, R = spatial gate
+ * (crates/ps-synthesis/src/weather_map.rs:46-101).  `coverage_grid` may be
+ * NULL; otherwise it is a row-major `grid_w*grid_h` f32 grid spanning
+ * `grid_extent_m` (coverage_grid.rs:34-60). */
+int psc_synthesise_weather_map(uint32_t n_layers, float precip_mm_per_h,
+                               float ground_wetness,
+                               const float* coverage_grid, uint32_t grid_w,
+                               uint32_t grid_h, float grid_extent_m,
+                               uint16_t* out_rgba16f /* 128*128*4 */);
+
+/* Procedural wind field, u/v channels (wind_field.rs:71-116,150-170);
+ * 32x16x32 RGBA16F, w and turbulence channels zero. */
+int psc_synthesise_wind_field(float surface_speed_mps, float wind_dir_deg,
+                              uint16_t* out_rgba16f);
+
+/* ------------------------------------------------------ context life */
+typedef struct psc_ctx psc_ctx;
+
+int psc_create(int cuda_device, psc_ctx** out);
+int psc_destroy(psc_ctx* ctx);
+
+/* `CloudsSubsystem::set_march_steps` (crates/ps-clouds/src/lib.rs:709-712):
+ * clamps cloud steps to [8,256] and light steps to [1,16]. */
+int psc_set_march_steps(psc_ctx* ctx, uint32_t cloud_steps,
+                        uint32_t light_steps);
+int psc_set_params(psc_ctx* ctx, const PscCloudParamsGpu* params);
+int psc_get_params(psc_ctx* ctx, PscCloudParamsGpu* out);
+/* Validates n <= 8, finite fields, top > base, disjoint half-open
+ * intervals.  Also sets params.cloud_layer_count = n. */
+int psc_set_layers(psc_ctx* ctx, const PscCloudLayerGpu* layers, uint32_t n);
+int psc_set_frame(psc_ctx* ctx, const PscFrameUniformsGpu* frame,
+                  const PscWorldUniformsGpu* world);
+int psc_set_options(psc_ctx* ctx, const PscMarchOptions* options);
+
+/* ----------------------------------------------------------- inputs */
+
+/* Bake base/detail/curl noise on the device (shaders/clouds/noise_*.comp.wgsl)
+ * and generate the blue-noise tile on the host.  Byte-identical to the
+ * oracle's CPU bake.  Synchronous. */
+int psc_bake_noise(psc_ctx* ctx);
+/* Upload one noise volume from host memory (RGBA8 / RG8 / R8 texels). */
+int psc_upload_noise(psc_ctx* ctx, int kind, const void* texels,
+                     size_t bytes);
+/* Copy a noise volume back to the host in its RGBA8/RG8/R8 form. */
+int psc_download_noise(psc_ctx* ctx, int kind, void* texels, size_t bytes);
+
+int psc_upload_weather(psc_ctx* ctx, const void* texels, uint32_t width,
+                       uint32_t height, int format);
+/* Cloud-type grid: row-major u8, 255 = use the layer's type. */
+int psc_upload_type_grid(psc_ctx* ctx, const uint8_t* texels, uint32_t width,
+                         uint32_t height);
+/* Wind field 32x16x32 RGBA16F (wind_field.rs layout). */
+int psc_upload_wind(psc_ctx* ctx, const uint16_t* rgba16f, size_t count);
+/* One atmosphere LUT, RGBA16F texels in x-fastest order. */
+int psc_upload_lut(psc_ctx* ctx, int kind, const uint16_t* rgba16f,
+                   size_t count);
+/* Bake all four atmosphere LUTs on the device from the current frame and
+ * world uniforms (shaders/atmosphere/{transmittance,multiscatter,skyview,
+ * aerialperspective}.comp.wgsl). */
+int psc_bake_luts(psc_ctx* ctx, void* stream);
+/* Copy one LUT back to the host as RGBA16F. */
+int psc_download_lut(psc_ctx* ctx, int kind, uint16_t* rgba16f, size_t count);
+
+/* ----------------------------------------------------------- render */
+
+/* March `n` views (each with the context's frame uniforms rescaled to the
+ * view size) and write L/T per pixel — the `clouds::march` pass
+ * (crates/ps-clouds/src/lib.rs:736-994).  With options.composite = 1 the
+ * `clouds::composite` blend is fused into the same kernel. */
+int psc_render(psc_ctx* ctx, const PscView* views, uint32_t n, void* stream);
+
+/* `clouds::composite` (cloud_composite.wgsl:48-57, blend One/Src1,
+ * pipeline.rs:469-484): hdr.rgba = L.rgba + hdr.rgba * T.rgba. */
+int psc_composite(const float* luminance, const float* transmittance,
+                  float* hdr, uint32_t width, uint32_t height, void* stream);
+
+/* Number of march-kernel launches issued by this context so far. */
+int psc_launch_count(psc_ctx* ctx, uint64_t* out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+
+static_assert(sizeof(PscCloudParamsGpu) == 112, "CloudParamsGpu is 112 B");
+static_assert(sizeof(PscCloudLayerGpu) == 48, "CloudLayerGpu is 48 B");
+static_assert(sizeof(PscFrameUniformsGpu) == 448, "FrameUniformsGpu is 448 B");
+static_assert(sizeof(PscWorldUniformsGpu) == 144, "WorldUniformsGpu is 144 B");
+static_assert(offsetof(PscCloudParamsGpu, sigma_a) == 16, "std140 sigma_a");
+static_assert(offsetof(PscCloudParamsGpu, droplet_diameter_bias) == 28, "");
+static_assert(offsetof(PscCloudParamsGpu, cone_light_sampling) == 32, "");
+static_assert(offsetof(PscCloudParamsGpu, powder_strength) == 48, "");
+static_assert(offsetof(PscCloudParamsGpu, ambient_strength) == 64, "");
+static_assert(offsetof(PscCloudParamsGpu, light_steps) == 80, "");
+static_assert(offsetof(PscCloudParamsGpu, temporal_jitter) == 96, "");
+static_assert(offsetof(PscCloudLayerGpu, cloud_type) == 16, "");
+static_assert(offsetof(PscCloudLayerGpu, droplet_diameter_um) == 32, "");
+static_assert(offsetof(PscFrameUniformsGpu, camera_position_world) == 256, "");
+static_assert(offsetof(PscFrameUniformsGpu, viewport_size) == 352, "");
+static_assert(offsetof(PscFrameUniformsGpu, time_seconds) == 368, "");
+static_assert(offsetof(PscFrameUniformsGpu, prev_view_proj) == 384, "");
+static_assert(offsetof(PscWorldUniformsGpu, rayleigh_scattering) == 16, "");
+static_assert(offsetof(PscWorldUniformsGpu, mie_g) == 64, "");
+static_assert(offsetof(PscWorldUniformsGpu, ozone_absorption) == 80, "");
+static_assert(offsetof(PscWorldUniformsGpu, ozone_center_m) == 96, "");
+static_assert(offsetof(PscWorldUniformsGpu, ground_albedo) == 112, "");
+static_assert(offsetof(PscWorldUniformsGpu, haze_extinction_per_m) == 128, "");
+#endif
+
+#endif /* PSCLOUDS_H */

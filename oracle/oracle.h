@@ -1,0 +1,133 @@
+/*
+ * ORACLE — test infrastructure, not product code.
+ *
+ * A CPU restatement of PedalSky's volumetric-cloud march path, used only as
+ * the checker for the CUDA implementation: by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline leg.  The product
+ * library (pedalsky_b200/libpsclouds.so) never links or calls it.
+ *
+ * Parity status: the reference publishes no numeric HDR goldens for this
+ * path and its WGSL cannot execute here (no graphics stack), so radiance
+ * parity of this restatement is UNPINNED.  What IS pinned against the
+ * reference's own tests: struct layouts, the coverage remap endpoints,
+ * per-type density/droplet defaults, the weather-map gate, the type-grid
+ * sentinel, the blue-noise histogram and the noise channel statistics
+ * (see tests/test_oracle_pins.py for the file:line of each).
+ *
+ * Every function cites the reference file:line it restates.
+ */
+#ifndef PSC_ORACLE_H
+#define PSC_ORACLE_H
+
+#include <stdint.h>
+#include "../include/psclouds.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- noise bakes (shaders/clouds/noise_*.comp.wgsl), FP32 as in WGSL ---- */
+int oracle_bake_noise_base(uint8_t* out_rgba8);    /* 128^3 * 4 */
+int oracle_bake_noise_detail(uint8_t* out_rgba8);  /* 32^3 * 4  */
+int oracle_bake_noise_curl(uint8_t* out_rg8);      /* 128^2 * 2 */
+int oracle_blue_noise(uint8_t* out_r8);            /* 64^2      */
+
+/* ---- synthesis (crates/ps-synthesis) ---- */
+float oracle_remap_coverage(float scene_coverage);
+int oracle_synthesise_layers(const PscCloudLayerDesc* in, uint32_t n,
+                             PscCloudLayerGpu* out);
+int oracle_weather_map(uint32_t n_layers, float precip_mm_per_h,
+                       float ground_wetness, const float* grid, uint32_t gw,
+                       uint32_t gh, float grid_extent_m, uint16_t* out);
+float oracle_value_noise_2d(float x, float y);
+int oracle_wind_field(float surface_speed, float wind_dir_deg, uint16_t* out);
+int oracle_frame_from_camera(const PscFlyCamera* cam, uint32_t width,
+                             uint32_t height, float sun_alt, float sun_az,
+                             float sun_ang_radius, float toa_lux,
+                             PscFrameUniformsGpu* out);
+
+/* ---- f16 helpers (IEEE binary16, round-to-nearest-even) ---- */
+uint16_t oracle_f32_to_f16(float f);
+float oracle_f16_to_f32(uint16_t h);
+
+/* ---- atmosphere LUT bakes (shaders/atmosphere/...), FP32, f16 output ---- */
+int oracle_bake_transmittance(const PscWorldUniformsGpu* world, uint16_t* out);
+int oracle_bake_multiscatter(const PscWorldUniformsGpu* world,
+                             const uint16_t* trans, uint16_t* out);
+int oracle_bake_skyview(const PscFrameUniformsGpu* frame,
+                        const PscWorldUniformsGpu* world,
+                        const uint16_t* trans, const uint16_t* ms,
+                        uint16_t* out);
+int oracle_bake_aerial(const PscFrameUniformsGpu* frame,
+                       const PscWorldUniformsGpu* world, const uint16_t* trans,
+                       const uint16_t* ms, uint16_t* out);
+
+/* ---- the march ---- */
+typedef struct OracleScene {
+  PscCloudParamsGpu params;
+  PscCloudLayerGpu layers[8];
+  PscFrameUniformsGpu frame;
+  PscWorldUniformsGpu world;
+  PscMarchOptions options;           /* phase_mode + HG lobes read here    */
+  const uint8_t* noise_base;         /* 128^3 RGBA8                       */
+  const uint8_t* noise_detail;       /* 32^3 RGBA8                        */
+  const uint8_t* noise_curl;         /* 128^2 RG8                         */
+  const uint8_t* blue_noise;         /* 64^2 R8                           */
+  const void* weather;               /* R channel read                    */
+  uint32_t weather_w, weather_h;
+  int weather_format;                /* PSC_WEATHER_*                     */
+  const uint8_t* type_grid;          /* may be NULL = all sentinel        */
+  uint32_t type_w, type_h;
+  const uint16_t* wind;              /* 32x16x32 RGBA16F                  */
+  const uint16_t* lut_transmittance; /* 256x64 RGBA16F                    */
+  const uint16_t* lut_skyview;       /* 192x108 RGBA16F                   */
+  const uint16_t* lut_aerial;        /* 32x32x64 RGBA16F                  */
+  const float* depth;                /* width*height, may be NULL         */
+} OracleScene;
+
+enum { ORACLE_FP32 = 32, ORACLE_FP64 = 64 };
+enum { ORACLE_FILTER_EXACT = 0, ORACLE_FILTER_Q8 = 1 };
+
+/* Fetch counters accumulated over the image (executed fetches). */
+enum {
+  ORACLE_CNT_WEATHER = 0,  /* bilinear weather tap per primary step       */
+  ORACLE_CNT_TYPE,         /* type-grid load per primary step             */
+  ORACLE_CNT_BASE,         /* primary base-noise trilinear taps           */
+  ORACLE_CNT_CURL,         /* curl bilinear taps                          */
+  ORACLE_CNT_DETAIL,       /* detail trilinear taps                       */
+  ORACLE_CNT_LIGHT,        /* light-march base trilinear taps             */
+  ORACLE_CNT_TRANS,        /* transmittance LUT bilinear taps             */
+  ORACLE_CNT_SKY,          /* sky-view LUT bilinear taps                  */
+  ORACLE_CNT_WIND,         /* per-layer wind-field trilinear taps         */
+  ORACLE_CNT_AP,           /* aerial-perspective trilinear taps           */
+  ORACLE_CNT_BLUE,         /* blue-noise loads                            */
+  ORACLE_CNT_DEPTH,        /* depth loads                                 */
+  ORACLE_CNT_STEPS,        /* primary steps executed                      */
+  ORACLE_CNT_DENSE,        /* dense (density > 1e-3) primary steps        */
+  ORACLE_CNT_PIXELS,
+  ORACLE_CNT__COUNT
+};
+
+/* Render width x height pixels of the view described by `scene`.
+ * out_lum / out_trans: width*height*4 floats (RGBA) each.  `counters` may
+ * be NULL, else ORACLE_CNT__COUNT entries.  `threads` <= 0 = all cores.
+ * Rows [row0, row1) only (row1 = 0 means all rows); other rows untouched. */
+int oracle_render(const OracleScene* scene, uint32_t width, uint32_t height,
+                  int precision, int filter, int threads, uint32_t row0,
+                  uint32_t row1, float* out_lum, float* out_trans,
+                  uint64_t* counters);
+
+/* Same march, one pixel, both outputs in double (for spot checks). */
+int oracle_render_pixel(const OracleScene* scene, uint32_t width,
+                        uint32_t height, uint32_t x, uint32_t y,
+                        int precision, int filter, double* lum4,
+                        double* trans4);
+
+/* `dst = L + dst*T` per channel (cloud_composite.wgsl + blend One/Src1). */
+int oracle_composite(const float* lum, const float* trans, float* hdr,
+                     uint32_t n_pixels);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,176 @@
+"""ORACLE — test infrastructure, not product code.
+
+ctypes wrapper around oracle/liboracle.so, the CPU restatement of the
+reference's cloud-march path.  Only tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg may import this module; it is the checker,
+never the thing measured or shipped.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from pedalsky_b200 import capi
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+FP32, FP64 = 32, 64
+FILTER_EXACT, FILTER_Q8 = 0, 1
+COUNTERS = ("weather", "type", "base", "curl", "detail", "light", "trans", "sky", "wind", "ap",
+            "blue", "depth", "steps", "dense", "pixels")
+
+
+class OracleScene(C.Structure):
+    _fields_ = [
+        ("params", capi.CloudParamsGpu), ("layers", capi.CloudLayerGpu * 8),
+        ("frame", capi.FrameUniformsGpu), ("world", capi.WorldUniformsGpu),
+        ("options", capi.MarchOptions),
+        ("noise_base", C.c_void_p), ("noise_detail", C.c_void_p), ("noise_curl", C.c_void_p),
+        ("blue_noise", C.c_void_p), ("weather", C.c_void_p), ("weather_w", C.c_uint32),
+        ("weather_h", C.c_uint32), ("weather_format", C.c_int), ("type_grid", C.c_void_p),
+        ("type_w", C.c_uint32), ("type_h", C.c_uint32), ("wind", C.c_void_p),
+        ("lut_transmittance", C.c_void_p), ("lut_skyview", C.c_void_p),
+        ("lut_aerial", C.c_void_p), ("depth", C.c_void_p),
+    ]
+
+
+_LIB = None
+
+
+def build() -> Path:
+    res = subprocess.run(["make", "-s", "-C", str(HERE)], capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + res.stdout + res.stderr)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        vp, u32, f32 = C.c_void_p, C.c_uint32, C.c_float
+        for name, args, res in [
+            ("oracle_bake_noise_base", [vp], C.c_int),
+            ("oracle_bake_noise_detail", [vp], C.c_int),
+            ("oracle_bake_noise_curl", [vp], C.c_int),
+            ("oracle_blue_noise", [vp], C.c_int),
+            ("oracle_remap_coverage", [f32], f32),
+            ("oracle_synthesise_layers", [vp, u32, vp], C.c_int),
+            ("oracle_weather_map", [u32, f32, f32, vp, u32, u32, f32, vp], C.c_int),
+            ("oracle_value_noise_2d", [f32, f32], f32),
+            ("oracle_wind_field", [f32, f32, vp], C.c_int),
+            ("oracle_frame_from_camera", [vp, u32, u32, f32, f32, f32, f32, vp], C.c_int),
+            ("oracle_f32_to_f16", [f32], C.c_uint16),
+            ("oracle_f16_to_f32", [C.c_uint16], f32),
+            ("oracle_bake_transmittance", [vp, vp], C.c_int),
+            ("oracle_bake_multiscatter", [vp, vp, vp], C.c_int),
+            ("oracle_bake_skyview", [vp, vp, vp, vp, vp], C.c_int),
+            ("oracle_bake_aerial", [vp, vp, vp, vp, vp], C.c_int),
+            ("oracle_render", [vp, u32, u32, C.c_int, C.c_int, C.c_int, u32, u32, vp, vp, vp], C.c_int),
+            ("oracle_render_pixel", [vp, u32, u32, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
+            ("oracle_composite", [vp, vp, vp, u32], C.c_int),
+        ]:
+            fn = getattr(L, name)
+            fn.argtypes, fn.restype = args, res
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return C.c_void_p(None) if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _ok(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} returned {rc}")
+
+
+def bake_noise() -> dict:
+    base = np.zeros(128 ** 3 * 4, np.uint8)
+    detail = np.zeros(32 ** 3 * 4, np.uint8)
+    curl = np.zeros(128 * 128 * 2, np.uint8)
+    blue = np.zeros(64 * 64, np.uint8)
+    _ok(lib().oracle_bake_noise_base(_p(base)), "base")
+    _ok(lib().oracle_bake_noise_detail(_p(detail)), "detail")
+    _ok(lib().oracle_bake_noise_curl(_p(curl)), "curl")
+    _ok(lib().oracle_blue_noise(_p(blue)), "blue")
+    return {"base": base, "detail": detail, "curl": curl, "blue": blue}
+
+
+def bake_luts(frame: capi.FrameUniformsGpu, world: capi.WorldUniformsGpu) -> dict:
+    L = lib()
+    t = np.zeros(256 * 64 * 4, np.uint16)
+    ms = np.zeros(32 * 32 * 4, np.uint16)
+    sky = np.zeros(192 * 108 * 4, np.uint16)
+    ap = np.zeros(32 * 32 * 64 * 4, np.uint16)
+    _ok(L.oracle_bake_transmittance(C.byref(world), _p(t)), "transmittance")
+    _ok(L.oracle_bake_multiscatter(C.byref(world), _p(t), _p(ms)), "multiscatter")
+    _ok(L.oracle_bake_skyview(C.byref(frame), C.byref(world), _p(t), _p(ms), _p(sky)), "skyview")
+    _ok(L.oracle_bake_aerial(C.byref(frame), C.byref(world), _p(t), _p(ms), _p(ap)), "aerial")
+    return {"transmittance": t, "multiscatter": ms, "skyview": sky, "aerial": ap}
+
+
+def make_scene(scene, noise: dict, luts: dict) -> tuple[OracleScene, list]:
+    """Build an OracleScene from a pedalsky_b200.scenes.Scene; returns (struct, keepalive)."""
+    keep = []
+
+    def arr(a, dtype):
+        if a is None:
+            return C.c_void_p(None)
+        a = np.ascontiguousarray(a, dtype)
+        keep.append(a)
+        return C.c_void_p(a.ctypes.data)
+
+    s = OracleScene()
+    s.params, s.frame, s.world, s.options = scene.params, scene.frame, scene.world, scene.options
+    for i in range(8):
+        s.layers[i] = scene.layers[i]
+    s.noise_base = arr(noise["base"], np.uint8)
+    s.noise_detail = arr(noise["detail"], np.uint8)
+    s.noise_curl = arr(noise["curl"], np.uint8)
+    s.blue_noise = arr(noise["blue"], np.uint8)
+    wdt = {capi.WEATHER_RGBA16F: np.uint16, capi.WEATHER_RG8: np.uint8,
+           capi.WEATHER_R32F: np.float32}[scene.weather_format]
+    s.weather = arr(scene.weather, wdt)
+    s.weather_w, s.weather_h, s.weather_format = scene.weather_w, scene.weather_h, scene.weather_format
+    if scene.type_grid is not None:
+        s.type_grid = arr(scene.type_grid, np.uint8)
+        side = int(round(np.sqrt(scene.type_grid.size)))
+        s.type_w = s.type_h = side
+    s.wind = arr(scene.wind, np.uint16)
+    s.lut_transmittance = arr(luts["transmittance"], np.uint16)
+    s.lut_skyview = arr(luts["skyview"], np.uint16)
+    s.lut_aerial = arr(luts["aerial"], np.uint16)
+    s.depth = arr(scene.depth, np.float32)
+    return s, keep
+
+
+def render(scene, noise, luts, precision=FP64, filt=FILTER_EXACT, threads=0, rows=None,
+           counters=False):
+    """Returns (L, T[, counters]) as (h, w, 4) float32 arrays."""
+    s, keep = make_scene(scene, noise, luts)
+    w, h = scene.width, scene.height
+    L = np.zeros((h, w, 4), np.float32)
+    T = np.zeros((h, w, 4), np.float32)
+    cnt = np.zeros(len(COUNTERS), np.uint64)
+    r0, r1 = rows if rows else (0, 0)
+    _ok(lib().oracle_render(C.byref(s), w, h, precision, filt, threads, r0, r1, _p(L), _p(T),
+                            _p(cnt) if counters else C.c_void_p(None)), "oracle_render")
+    del keep
+    if counters:
+        return L, T, dict(zip(COUNTERS, (int(c) for c in cnt)))
+    return L, T
+
+
+def composite(L, T, bg):
+    out = np.ascontiguousarray(bg, np.float32).copy()
+    _ok(lib().oracle_composite(_p(np.ascontiguousarray(L, np.float32)),
+                               _p(np.ascontiguousarray(T, np.float32)), _p(out),
+                               out.size // 4), "composite")
+    return out

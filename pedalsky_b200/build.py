@@ -1,0 +1,102 @@
+"""Build libpsclouds.so (the CUDA kernels + C ABI) in-tree for sm_100a.
+
+Usage: python -m pedalsky_b200.build [--verbose]
+
+Each translation unit is compiled separately so per-file flags apply
+(noise_bake.cu needs -fmad=false for byte-exact bakes), then linked into one
+shared library next to this file.  Rebuilds only when a source or header is
+newer than the library.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+ROOT = HERE.parent
+LIB = HERE / "libpsclouds.so"
+BUILD_DIR = HERE / "_build"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include")]
+CUDA_UNITS = {
+    "march.cu": [],
+    "noise_bake.cu": ["-fmad=false"],
+    "atmosphere.cu": [],
+}
+CXX_UNITS = ["psc_host.cpp"]
+
+
+def _host_cxx() -> str:
+    for cand in ("g++-13", "g++"):
+        path = shutil.which(cand)
+        if path:
+            return path
+    raise RuntimeError("no host C++ compiler found")
+
+
+def _nvcc() -> str:
+    path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(path).exists():
+        raise RuntimeError("nvcc not found")
+    return path
+
+
+def _sources() -> list[Path]:
+    return sorted(CSRC.glob("*")) + [ROOT / "include" / "psclouds.h"]
+
+
+def needs_build() -> bool:
+    if not LIB.exists():
+        return True
+    t = LIB.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in _sources() if p.is_file())
+
+
+def _run(cmd: list[str], verbose: bool) -> None:
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd[:3])} ... ({res.returncode})")
+    if verbose and (res.stdout or res.stderr):
+        sys.stderr.write(res.stdout + res.stderr)
+
+
+def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> Path:
+    if not force and not needs_build():
+        return LIB
+    BUILD_DIR.mkdir(exist_ok=True)
+    nvcc, cxx = _nvcc(), _host_cxx()
+    env_ccbin = ["-ccbin", cxx]
+    objs = []
+    for unit, extra in CUDA_UNITS.items():
+        obj = BUILD_DIR / (unit + ".o")
+        cmd = [nvcc, *env_ccbin, *ARCH, *NVCC_COMMON, *extra, "-c", str(CSRC / unit), "-o", str(obj)]
+        if ptxas_info:
+            cmd += ["-Xptxas", "-v"]
+        _run(cmd, verbose or ptxas_info)
+        objs.append(obj)
+    cuda_inc = Path(nvcc).resolve().parent.parent / "include"
+    for unit in CXX_UNITS:
+        obj = BUILD_DIR / (unit + ".o")
+        cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-I", str(ROOT / "include"),
+               "-I", str(cuda_inc), "-c", str(CSRC / unit), "-o", str(obj)]
+        _run(cmd, verbose)
+        objs.append(obj)
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [nvcc, *env_ccbin, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static"]
+    _run(cmd, verbose)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose="--verbose" in sys.argv, force="--force" in sys.argv,
+          ptxas_info="--ptxas" in sys.argv)
+    print(LIB)

@@ -1,0 +1,1057 @@
+// Host side of the C ABI declared in include/psclouds.h.
+//
+// Mirrors the reference's `CloudsSubsystem` (crates/ps-clouds/src/lib.rs):
+// it owns the device copies of the noise volumes, weather inputs and LUTs,
+// keeps CloudParams / the layer array / the frame and world uniforms, and
+// turns them into one flattened `MarchUniforms` block per launch.  Every
+// entry point validates its arguments and reports failures as an int status
+// plus a thread-local message; nothing throws across the boundary.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/psclouds.h"
+#include "psc_internal.h"
+
+namespace psc {
+int launch_convert_storage(const uint8_t* src, void* dst, uint32_t n_texels, int storage,
+                           float fp8_scale, cudaStream_t s);
+}
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? PSC_ERR_OUT_OF_MEMORY : PSC_ERR_CUDA, "%s: %s", what,
+              cudaGetErrorString(e));
+}
+
+#define PSC_CUDA(call, what)                    \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+bool all_finite(const float* p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+float half_bits_to_float(uint16_t h) {
+  __half_raw r;
+  r.x = h;
+  return __half2float(__half(r));
+}
+uint16_t float_to_half_bits(float f) {
+  __half_raw r = __half_raw(__float2half_rn(f));
+  return r.x;
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+}  // namespace
+
+struct psc_ctx {
+  int device = 0;
+  PscCloudParamsGpu params{};
+  PscCloudLayerGpu layers[8]{};
+  uint32_t n_layers = 0;
+  PscFrameUniformsGpu frame{};
+  PscWorldUniformsGpu world{};
+  bool have_frame = false;
+  PscMarchOptions opts{};
+
+  uint8_t* d_base_u8 = nullptr;    // 128^3 RGBA8 (canonical)
+  uint8_t* d_detail_u8 = nullptr;  // 32^3 RGBA8
+  void* d_base_store = nullptr;    // storage form
+  void* d_detail_store = nullptr;
+  int store_form = -1;
+  float fp8_scale = 448.0f;
+  uint8_t* d_curl = nullptr;       // 128^2 RG8
+  float* d_blue = nullptr;         // 64^2 floats
+  std::vector<uint8_t> h_blue;
+  bool have_base = false, have_detail = false, have_curl = false, have_blue = false;
+
+  float* d_weather = nullptr;
+  uint32_t weather_w = 0, weather_h = 0;
+  uint8_t* d_type = nullptr;
+  uint32_t type_w = 0, type_h = 0;
+  std::vector<uint16_t> h_wind;    // 32x16x32 RGBA16F
+
+  float4* d_lut[4] = {nullptr, nullptr, nullptr, nullptr};  // float4 copies
+  uint16_t* d_lut_h[4] = {nullptr, nullptr, nullptr, nullptr};  // RGBA16F bake outputs
+  bool have_lut[4] = {false, false, false, false};
+
+  // texture-unit path
+  cudaArray_t arr_base = nullptr, arr_detail = nullptr;
+  cudaTextureObject_t tex_base = 0, tex_detail = 0;
+  bool tex_dirty = true;
+
+  uint64_t launches = 0;
+};
+
+namespace {
+
+const uint32_t kLutW[4] = {256, 32, 192, 32};
+const uint32_t kLutH[4] = {64, 32, 108, 32};
+const uint32_t kLutD[4] = {1, 1, 1, 64};
+
+size_t lut_texels(int k) { return (size_t)kLutW[k] * kLutH[k] * kLutD[k]; }
+
+int ensure_device(psc_ctx* c) {
+  int n = 0;
+  PSC_CUDA(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+  if (c->device >= n) return fail(PSC_ERR_INVALID_ARGUMENT, "device %d not in [0,%d)", c->device, n);
+  PSC_CUDA(cudaSetDevice(c->device), "cudaSetDevice");
+  return PSC_OK;
+}
+
+int validate_params(const PscCloudParamsGpu& p) {
+  const float* f = reinterpret_cast<const float*>(&p);
+  // every float field (the u32 fields are checked by value below)
+  const size_t float_fields[] = {0, 1, 2, 4, 5, 6, 7, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 25, 26, 27};
+  for (size_t i : float_fields)
+    if (!std::isfinite(f[i])) return fail(PSC_ERR_NOT_FINITE, "CloudParams field %zu is not finite", i);
+  if (p.cloud_steps == 0 || p.cloud_steps > 4096)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "cloud_steps %u out of range [1,4096]", p.cloud_steps);
+  if (p.light_steps == 0 || p.light_steps > 256)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "light_steps %u out of range [1,256]", p.light_steps);
+  if (p.multi_scatter_octaves > 64)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "multi_scatter_octaves %u > 64", p.multi_scatter_octaves);
+  if (p.cloud_layer_count > PSC_MAX_CLOUD_LAYERS)
+    return fail(PSC_ERR_LAYERS, "cloud_layer_count %u > 8", p.cloud_layer_count);
+  return PSC_OK;
+}
+
+int validate_layers(const PscCloudLayerGpu* l, uint32_t n) {
+  if (n > PSC_MAX_CLOUD_LAYERS) return fail(PSC_ERR_LAYERS, "%u layers exceeds the maximum of 8", n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const float f[] = {l[i].base_m, l[i].top_m, l[i].coverage, l[i].density_scale, l[i].shape_bias,
+                       l[i].detail_bias, l[i].anvil_bias, l[i].droplet_diameter_um};
+    if (!all_finite(f, 8)) return fail(PSC_ERR_NOT_FINITE, "layer %u has a non-finite field", i);
+    if (!(l[i].top_m > l[i].base_m))
+      return fail(PSC_ERR_LAYERS, "layer %u: top_m %g <= base_m %g", i, l[i].top_m, l[i].base_m);
+    if (l[i].cloud_type > 7u) return fail(PSC_ERR_LAYERS, "layer %u: cloud_type %u > 7", i, l[i].cloud_type);
+  }
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t j = i + 1; j < n; ++j)  // check_non_overlap, cloud_layers.rs:136-150
+      if (l[i].base_m < l[j].top_m && l[j].base_m < l[i].top_m)
+        return fail(PSC_ERR_LAYERS, "cloud layers %u and %u overlap", i, j);
+  return PSC_OK;
+}
+
+float smoothstep_h(float e0, float e1, float x) {
+  float t = (x - e0) / (e1 - e0);
+  t = std::fmin(std::fmax(t, 0.0f), 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+
+// LayerWindCache (cloud_density_common.wgsl:154-183): one trilinear, repeat
+// sample of the wind field at (0.5, mid_alt / 12 km, 0.5).
+void wind_cache(const psc_ctx* c, const PscCloudLayerGpu& L, psc::LayerConst& o) {
+  float wx = 0.0f, wz = 0.0f;
+  if (c->h_wind.size() == 32u * 16u * 32u * 4u) {
+    const float mid = (L.base_m + L.top_m) * 0.5f;
+    const float uy = std::fmin(std::fmax(mid / 12000.0f, 0.0f), 0.9999f);
+    auto axis = [](float u, int n, int& i0, int& i1, float& w) {
+      const float x = u * (float)n - 0.5f;
+      const float fl = std::floor(x);
+      const int i = (int)fl;
+      i0 = ((i % n) + n) % n;
+      i1 = (((i + 1) % n) + n) % n;
+      w = x - fl;
+    };
+    int x0, x1, y0, y1, z0, z1;
+    float ax, ay, az;
+    axis(0.5f, 32, x0, x1, ax);
+    axis(uy, 16, y0, y1, ay);
+    axis(0.5f, 32, z0, z1, az);
+    auto tx = [&](int x, int y, int z, int ch) {
+      return half_bits_to_float(c->h_wind[(((size_t)z * 16 + y) * 32 + x) * 4 + ch]);
+    };
+    float r[2];
+    for (int ch = 0; ch < 2; ++ch) {
+      auto l = [](float a, float b, float t) { return a + (b - a) * t; };
+      const float a0 = l(l(tx(x0, y0, z0, ch), tx(x1, y0, z0, ch), ax),
+                         l(tx(x0, y1, z0, ch), tx(x1, y1, z0, ch), ax), ay);
+      const float a1 = l(l(tx(x0, y0, z1, ch), tx(x1, y0, z1, ch), ax),
+                         l(tx(x0, y1, z1, ch), tx(x1, y1, z1, ch), ax), ay);
+      r[ch] = l(a0, a1, az);
+    }
+    wx = r[0];
+    wz = r[1];
+  }
+  const float drift = c->params.wind_drift_strength * c->frame.simulated_seconds;
+  o.wind_off_x = wx * drift;
+  o.wind_off_z = wz * drift;
+  o.skew_x = o.skew_z = o.skew_thickness = 0.0f;
+  if (c->params.wind_skew_strength != 0.0f) {
+    const float sp = std::sqrt(wx * wx + wz * wz);
+    if (sp >= 0.1f) {
+      o.skew_x = wx / sp;
+      o.skew_z = wz / sp;
+      o.skew_thickness = std::fmax(L.top_m - L.base_m, 1.0f) * c->params.wind_skew_strength;
+    }
+  }
+}
+
+void build_uniforms(const psc_ctx* c, uint32_t width, uint32_t height, psc::MarchUniforms& u) {
+  std::memset(&u, 0, sizeof(u));
+  const PscFrameUniformsGpu& f = c->frame;
+  const PscWorldUniformsGpu& w = c->world;
+  const PscCloudParamsGpu& p = c->params;
+  for (int col = 0; col < 4; ++col)
+    for (int row = 0; row < 4; ++row) {
+      u.inv_vp[col][row] = f.inv_view_proj[col][row];
+      u.inv_vp_d[col][row] = (double)f.inv_view_proj[col][row];
+    }
+  for (int k = 0; k < 3; ++k) {
+    u.cam[k] = f.camera_position_world[k];
+    u.sun[k] = f.sun_direction[k];
+    u.sun_illum[k] = f.sun_illuminance[k];
+    u.lightning_rgb[k] = f.lightning_illuminance[k];
+    u.sigma_s[k] = p.sigma_s[k];
+  }
+  u.lightning_radius = f.lightning_illuminance[3];
+  u.lightning_origin_x = f.lightning_origin_world[0];
+  u.lightning_origin_z = f.lightning_origin_world[2];
+  u.vp_w = (float)width;
+  u.vp_h = (float)height;
+  u.temporal_jitter = p.temporal_jitter;
+  u.frame_index = f.frame_index;
+  u.planet_r = w.planet_radius_m;
+  u.planet_r_d = (double)w.planet_radius_m;
+  u.atmo_top = w.atmosphere_top_m;
+  u.droplet_bias = p.droplet_diameter_bias;
+  u.forward_bias = p.forward_bias;
+  u.detail_strength = p.detail_strength;
+  u.curl_strength = p.curl_strength;
+  u.powder = p.powder_strength;
+  u.ms_a = p.multi_scatter_a;
+  u.ms_b = p.multi_scatter_b;
+  u.ms_c = p.multi_scatter_c;
+  u.ambient = p.ambient_strength;
+  u.base_scale = std::fmax(p.base_scale_m, 1.0f);
+  u.detail_scale = std::fmax(p.detail_scale_m, 1.0f);
+  u.weather_scale = std::fmax(p.weather_scale_m, 1.0f);
+  u.light_steps = p.light_steps;
+  u.cloud_steps = p.cloud_steps;
+  u.octaves = p.multi_scatter_octaves;
+  u.layer_count = std::min<uint32_t>(p.cloud_layer_count, 8u);
+  u.cone = p.cone_light_sampling;
+  u.phase_mode = c->opts.phase_mode;
+  u.hg_f = c->opts.hg_g_forward;
+  u.hg_b = c->opts.hg_g_backward;
+  u.hg_w = c->opts.hg_blend;
+  u.kahan = c->opts.kahan;
+  u.composite = c->opts.composite;
+  u.debug_checks = c->opts.debug_checks;
+
+  // diurnal_modulation (cloud_density_common.wgsl:204-219), per layer type
+  const float bell = smoothstep_h(-0.1f, 0.4f, f.sun_direction[1]);
+  for (uint32_t i = 0; i < 8; ++i) {
+    const PscCloudLayerGpu& L = c->layers[i];
+    psc::LayerConst& o = u.layers[i];
+    o.base_m = L.base_m;
+    o.top_m = L.top_m;
+    o.inv_thickness = 1.0f / std::fmax(L.top_m - L.base_m, 1.0f);
+    o.coverage = L.coverage;
+    o.density_scale = L.density_scale;
+    o.cloud_type = L.cloud_type;
+    const uint32_t t = L.cloud_type;
+    const bool conv = t == 0 || t == 2 || t == 3 || t == 7;
+    const float di = (p.diurnal_strength == 0.0f || !conv) ? 0.0f : bell * p.diurnal_strength;
+    o.lf_bias = (L.shape_bias * di) * 0.5f;
+    o.layer_detail = std::fmin(std::fmax(p.detail_strength + L.detail_bias * di, 0.0f), 1.0f);
+    o.anvil_bias = L.anvil_bias;
+    o.droplet_um = L.droplet_diameter_um;
+    // chromatic_mie_modulation, cloud_march.wgsl:122-145
+    float cm[3] = {1.0f, 1.0f, 1.0f};
+    const float tt = std::fmin(std::fmax(1.0f - L.droplet_diameter_um / 20.0f, 0.0f), 1.0f);
+    if (tt > 0.0f) {
+      const float s = 0.25f * tt * tt;
+      cm[0] = 1.0f - 0.5f * s;
+      cm[2] = 1.0f + s;
+    }
+    for (int k = 0; k < 3; ++k) o.sigma_t[k] = (p.sigma_s[k] + p.sigma_a[k]) * cm[k];
+    wind_cache(c, L, o);
+    // cloud_phase_constants (cloud_march.wgsl:256-272) for non-Cb layers
+    const float d = std::fmin(std::fmax(L.droplet_diameter_um * p.droplet_diameter_bias, 5.0f), 50.0f);
+    o.g_hg = std::exp(-0.0990567f / (d - 1.67154f));
+    o.g_d = std::exp(-2.20679f / (d + 3.91029f)) - 0.428934f;
+    o.alpha = std::exp(3.62489f - 8.29288f / (d + 5.52825f));
+    o.w_d = std::exp(-0.599085f / (d - 0.641583f) - 0.665888f);
+    o.ice = smoothstep_h(35.0f, 50.0f, d);
+    o.r_bottom = (double)w.planet_radius_m + (double)L.base_m;
+    o.r_top = (double)w.planet_radius_m + (double)L.top_m;
+  }
+
+  u.noise_base = c->d_base_store;
+  u.noise_detail = c->d_detail_store;
+  u.noise_scale = 1.0f / c->fp8_scale;
+  u.curl = c->d_curl;
+  u.blue = c->d_blue;
+  u.weather = c->d_weather;
+  u.weather_w = c->weather_w;
+  u.weather_h = c->weather_h;
+  u.type_grid = c->d_type;
+  u.type_w = c->type_w;
+  u.type_h = c->type_h;
+  u.lut_trans = c->d_lut[PSC_LUT_TRANSMITTANCE];
+  u.lut_sky = c->d_lut[PSC_LUT_SKYVIEW];
+  u.lut_ap = c->d_lut[PSC_LUT_AERIAL];
+  u.tex_base = c->tex_base;
+  u.tex_detail = c->tex_detail;
+}
+
+int build_storage(psc_ctx* c) {
+  if (!c->have_base || !c->have_detail) return PSC_OK;
+  const int st = (int)c->opts.storage;
+  if (st == c->store_form && c->d_base_store) return PSC_OK;
+  const size_t tex_bytes[] = {4, 16, 8, 8, 4};
+  dfree(c->d_base_store);
+  dfree(c->d_detail_store);
+  PSC_CUDA(cudaMalloc(&c->d_base_store, 128u * 128u * 128u * tex_bytes[st]), "cudaMalloc base storage");
+  PSC_CUDA(cudaMalloc(&c->d_detail_store, 32u * 32u * 32u * tex_bytes[st]), "cudaMalloc detail storage");
+  if (psc::launch_convert_storage(c->d_base_u8, c->d_base_store, 128u * 128u * 128u, st, c->fp8_scale, 0) ||
+      psc::launch_convert_storage(c->d_detail_u8, c->d_detail_store, 32u * 32u * 32u, st, c->fp8_scale, 0))
+    return fail(PSC_ERR_CUDA, "storage conversion launch failed");
+  PSC_CUDA(cudaDeviceSynchronize(), "storage conversion");
+  c->store_form = st;
+  return PSC_OK;
+}
+
+void destroy_textures(psc_ctx* c) {
+  if (c->tex_base) cudaDestroyTextureObject(c->tex_base);
+  if (c->tex_detail) cudaDestroyTextureObject(c->tex_detail);
+  if (c->arr_base) cudaFreeArray(c->arr_base);
+  if (c->arr_detail) cudaFreeArray(c->arr_detail);
+  c->tex_base = c->tex_detail = 0;
+  c->arr_base = c->arr_detail = nullptr;
+  c->tex_dirty = true;
+}
+
+int make_volume_texture(const uint8_t* d_src, uint32_t n, cudaArray_t* arr, cudaTextureObject_t* tex) {
+  const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<uchar4>();
+  const cudaExtent ext = make_cudaExtent(n, n, n);
+  PSC_CUDA(cudaMalloc3DArray(arr, &fmt, ext), "cudaMalloc3DArray");
+  cudaMemcpy3DParms cp{};
+  cp.srcPtr = make_cudaPitchedPtr((void*)d_src, n * 4, n, n);
+  cp.dstArray = *arr;
+  cp.extent = ext;
+  cp.kind = cudaMemcpyDeviceToDevice;
+  PSC_CUDA(cudaMemcpy3D(&cp), "cudaMemcpy3D volume");
+  cudaResourceDesc rd{};
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = *arr;
+  cudaTextureDesc td{};
+  td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeWrap;
+  td.filterMode = cudaFilterModeLinear;
+  td.readMode = cudaReadModeNormalizedFloat;
+  td.normalizedCoords = 1;
+  PSC_CUDA(cudaCreateTextureObject(tex, &rd, &td, nullptr), "cudaCreateTextureObject");
+  return PSC_OK;
+}
+
+int build_textures(psc_ctx* c) {
+  if (c->opts.filter != PSC_FILTER_TEXTURE || !c->tex_dirty) return PSC_OK;
+  destroy_textures(c);
+  int rc = make_volume_texture(c->d_base_u8, 128, &c->arr_base, &c->tex_base);
+  if (rc) return rc;
+  rc = make_volume_texture(c->d_detail_u8, 32, &c->arr_detail, &c->tex_detail);
+  if (rc) return rc;
+  c->tex_dirty = false;
+  return PSC_OK;
+}
+
+int upload_lut_float4(psc_ctx* c, int kind, const uint16_t* h16) {
+  const size_t n = lut_texels(kind);
+  std::vector<float> f(n * 4);
+  for (size_t i = 0; i < n * 4; ++i) f[i] = half_bits_to_float(h16[i]);
+  if (!c->d_lut[kind]) PSC_CUDA(cudaMalloc(&c->d_lut[kind], n * sizeof(float4)), "cudaMalloc LUT");
+  PSC_CUDA(cudaMemcpy(c->d_lut[kind], f.data(), n * sizeof(float4), cudaMemcpyHostToDevice), "LUT upload");
+  c->have_lut[kind] = true;
+  return PSC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* psc_last_error(void) { return g_last_error.c_str(); }
+uint32_t psc_abi_version(void) { return PSC_ABI_VERSION; }
+size_t psc_sizeof_params(void) { return sizeof(PscCloudParamsGpu); }
+size_t psc_sizeof_layer(void) { return sizeof(PscCloudLayerGpu); }
+size_t psc_sizeof_frame(void) { return sizeof(PscFrameUniformsGpu); }
+size_t psc_sizeof_world(void) { return sizeof(PscWorldUniformsGpu); }
+
+int psc_params_default(PscCloudParamsGpu* o) {  // params.rs:142-212
+  if (!o) return fail(PSC_ERR_INVALID_ARGUMENT, "null output");
+  std::memset(o, 0, sizeof(*o));
+  o->sigma_s[0] = 0.030f;
+  o->sigma_s[1] = 0.040f;
+  o->sigma_s[2] = 0.060f;
+  o->droplet_diameter_bias = 1.0f;
+  o->detail_strength = 0.05f;
+  o->curl_strength = 0.1f;
+  o->powder_strength = 1.0f;
+  o->multi_scatter_a = o->multi_scatter_b = o->multi_scatter_c = 0.5f;
+  o->ambient_strength = 1.0f;
+  o->base_scale_m = 4500.0f;
+  o->detail_scale_m = 800.0f;
+  o->weather_scale_m = 32000.0f;
+  o->light_steps = 6;
+  o->cloud_steps = 192;
+  o->multi_scatter_octaves = 4;
+  o->wind_drift_strength = 1.0f;
+  o->wind_skew_strength = 0.5f;
+  o->diurnal_strength = 1.0f;
+  return PSC_OK;
+}
+
+int psc_world_default(PscWorldUniformsGpu* o) {  // weather.rs:60-84
+  if (!o) return fail(PSC_ERR_INVALID_ARGUMENT, "null output");
+  std::memset(o, 0, sizeof(*o));
+  o->planet_radius_m = 6360000.0f;
+  o->atmosphere_top_m = 6460000.0f;
+  o->rayleigh_scale_height_m = 8000.0f;
+  o->mie_scale_height_m = 1200.0f;
+  const float ray[3] = {5.802e-6f, 13.558e-6f, 33.100e-6f};
+  const float oz[3] = {0.650e-6f, 1.881e-6f, 0.085e-6f};
+  for (int k = 0; k < 3; ++k) {
+    o->rayleigh_scattering[k] = ray[k];
+    o->mie_scattering[k] = 3.996e-6f;
+    o->mie_absorption[k] = 4.4e-6f;
+    o->ozone_absorption[k] = oz[k];
+    o->ground_albedo[k] = 0.18f;
+  }
+  o->mie_g = 0.8f;
+  o->ozone_center_m = 25000.0f;
+  o->ozone_thickness_m = 30000.0f;
+  return PSC_OK;
+}
+
+int psc_options_default(PscMarchOptions* o) {
+  if (!o) return fail(PSC_ERR_INVALID_ARGUMENT, "null output");
+  std::memset(o, 0, sizeof(*o));
+  o->phase_mode = PSC_PHASE_APPROX_MIE;
+  o->hg_g_forward = 0.8f;
+  o->hg_g_backward = -0.2f;
+  o->hg_blend = 0.5f;
+  o->storage = PSC_STORAGE_U8;
+  o->filter = PSC_FILTER_EXACT;
+  o->schedule = PSC_SCHED_PLAIN;
+  return PSC_OK;
+}
+
+// cloud_layers.rs:106-126
+static float remap_coverage(float sc) {
+  const float lo = 0.40f, hi = 0.60f, knee = 0.10f;
+  const float t = std::fmin(std::fmax(sc, 0.0f), 1.0f);
+  if (t <= 0.0f) return 0.0f;
+  if (t < knee) {
+    const float s = t / knee;
+    return (s * s * (3.0f - 2.0f * s)) * lo;
+  }
+  const float bt = std::fmin(std::fmax((t - knee) / (1.0f - knee), 0.0f), 1.0f);
+  return lo + bt * (hi - lo);
+}
+
+int psc_synthesise_layers(const PscCloudLayerDesc* in, uint32_t n, PscCloudLayerGpu* out) {
+  if ((n && !in) || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null layer pointer");
+  if (n > PSC_MAX_CLOUD_LAYERS) return fail(PSC_ERR_LAYERS, "%u layers exceeds the maximum of 8", n);
+  static const float dens[8] = {1.0f, 1.0f, 1.0f, 0.85f, 0.7f, 0.55f, 0.4f, 1.4f};  // scene.rs:293-302
+  static const float drop[8] = {20.0f, 16.0f, 16.0f, 14.0f, 30.0f, 50.0f, 50.0f, 20.0f};  // :334-352
+  for (uint32_t i = 0; i < n; ++i) {
+    const PscCloudLayerDesc& d = in[i];
+    if (d.cloud_type > 7) return fail(PSC_ERR_LAYERS, "layer %u: cloud_type %u > 7", i, d.cloud_type);
+    PscCloudLayerGpu g{};
+    g.base_m = d.base_m;
+    g.top_m = d.top_m;
+    g.coverage = remap_coverage(d.coverage);
+    g.density_scale = d.density_scale >= 0.0f ? d.density_scale : dens[d.cloud_type];
+    g.cloud_type = d.cloud_type;
+    g.shape_bias = d.shape_octave_bias;
+    g.detail_bias = d.detail_octave_bias;
+    g.anvil_bias = d.anvil_bias >= 0.0f ? d.anvil_bias : (d.cloud_type == 7 ? 1.0f : 0.0f);
+    g.droplet_diameter_um = d.droplet_diameter_um >= 0.0f ? d.droplet_diameter_um : drop[d.cloud_type];
+    out[i] = g;
+  }
+  return validate_layers(out, n);
+}
+
+int psc_frame_from_camera(const PscFlyCamera* cam, uint32_t width, uint32_t height, float sun_alt,
+                          float sun_az, float sun_ang, float lux, PscFrameUniformsGpu* o) {
+  if (!cam || !o) return fail(PSC_ERR_INVALID_ARGUMENT, "null camera or output");
+  if (!width || !height) return fail(PSC_ERR_INVALID_ARGUMENT, "zero-size viewport");
+  const float vals[] = {cam->position[0], cam->position[1], cam->position[2], cam->pitch_rad,
+                        cam->yaw_rad, cam->roll_rad, cam->fov_y_rad, cam->near_m, sun_alt, sun_az,
+                        sun_ang, lux};
+  if (!all_finite(vals, 12)) return fail(PSC_ERR_NOT_FINITE, "non-finite camera or sun value");
+  if (!(cam->fov_y_rad > 0.0f && cam->fov_y_rad < 3.14159f) || !(cam->near_m > 0.0f))
+    return fail(PSC_ERR_INVALID_ARGUMENT, "fov_y must be in (0, pi) and near_m > 0");
+  std::memset(o, 0, sizeof(*o));
+  // FlyCamera::forward / look_to_rh / perspective_infinite_reverse_rh
+  const double yaw = cam->yaw_rad, pitch = cam->pitch_rad;
+  double fw[3] = {std::cos(pitch) * std::sin(yaw), std::sin(pitch), -std::cos(pitch) * std::cos(yaw)};
+  double n = std::sqrt(fw[0] * fw[0] + fw[1] * fw[1] + fw[2] * fw[2]);
+  for (double& v : fw) v /= n;
+  double rt[3] = {-fw[2], 0.0, fw[0]};  // forward x (0,1,0)
+  n = std::sqrt(rt[0] * rt[0] + rt[2] * rt[2]);
+  for (double& v : rt) v /= n;
+  const double up[3] = {rt[1] * fw[2] - rt[2] * fw[1], rt[2] * fw[0] - rt[0] * fw[2],
+                        rt[0] * fw[1] - rt[1] * fw[0]};
+  const double eye[3] = {cam->position[0], cam->position[1], cam->position[2]};
+  double V[4][4] = {};  // [col][row]
+  for (int k = 0; k < 3; ++k) {
+    V[k][0] = rt[k];
+    V[k][1] = up[k];
+    V[k][2] = -fw[k];
+  }
+  V[3][0] = -(eye[0] * rt[0] + eye[1] * rt[1] + eye[2] * rt[2]);
+  V[3][1] = -(eye[0] * up[0] + eye[1] * up[1] + eye[2] * up[2]);
+  V[3][2] = eye[0] * fw[0] + eye[1] * fw[1] + eye[2] * fw[2];
+  V[3][3] = 1.0;
+  if (cam->roll_rad != 0.0f) {  // Mat4::from_rotation_z(roll) * view
+    const double cr = std::cos((double)cam->roll_rad), sr = std::sin((double)cam->roll_rad);
+    double Rm[4][4] = {{cr, sr, 0, 0}, {-sr, cr, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+    double T[4][4];
+    for (int col = 0; col < 4; ++col)
+      for (int row = 0; row < 4; ++row) {
+        double s = 0;
+        for (int k = 0; k < 4; ++k) s += Rm[k][row] * V[col][k];
+        T[col][row] = s;
+      }
+    std::memcpy(V, T, sizeof(V));
+  }
+  const double f = 1.0 / std::tan(0.5 * (double)cam->fov_y_rad);
+  double P[4][4] = {};
+  P[0][0] = f / ((double)width / (double)height);
+  P[1][1] = f;
+  P[2][3] = -1.0;
+  P[3][2] = cam->near_m;
+  double VP[4][4];
+  for (int col = 0; col < 4; ++col)
+    for (int row = 0; row < 4; ++row) {
+      double s = 0;
+      for (int k = 0; k < 4; ++k) s += P[k][row] * V[col][k];
+      VP[col][row] = s;
+    }
+  // inverse via the adjugate (cofactor expansion in 2x2 minors)
+  const double* m = &VP[0][0];  // m[col*4+row]
+  auto a = [&](int row, int col) { return m[col * 4 + row]; };
+  double s0 = a(0, 0) * a(1, 1) - a(1, 0) * a(0, 1), s1 = a(0, 0) * a(1, 2) - a(1, 0) * a(0, 2);
+  double s2 = a(0, 0) * a(1, 3) - a(1, 0) * a(0, 3), s3 = a(0, 1) * a(1, 2) - a(1, 1) * a(0, 2);
+  double s4 = a(0, 1) * a(1, 3) - a(1, 1) * a(0, 3), s5 = a(0, 2) * a(1, 3) - a(1, 2) * a(0, 3);
+  double c5 = a(2, 2) * a(3, 3) - a(3, 2) * a(2, 3), c4 = a(2, 1) * a(3, 3) - a(3, 1) * a(2, 3);
+  double c3 = a(2, 1) * a(3, 2) - a(3, 1) * a(2, 2), c2 = a(2, 0) * a(3, 3) - a(3, 0) * a(2, 3);
+  double c1 = a(2, 0) * a(3, 2) - a(3, 0) * a(2, 2), c0 = a(2, 0) * a(3, 1) - a(3, 0) * a(2, 1);
+  const double det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+  if (det == 0.0 || !std::isfinite(det)) return fail(PSC_ERR_INVALID_ARGUMENT, "singular view-projection");
+  const double id = 1.0 / det;
+  double inv[4][4];  // inv[row][col]
+  inv[0][0] = (a(1, 1) * c5 - a(1, 2) * c4 + a(1, 3) * c3) * id;
+  inv[0][1] = (-a(0, 1) * c5 + a(0, 2) * c4 - a(0, 3) * c3) * id;
+  inv[0][2] = (a(3, 1) * s5 - a(3, 2) * s4 + a(3, 3) * s3) * id;
+  inv[0][3] = (-a(2, 1) * s5 + a(2, 2) * s4 - a(2, 3) * s3) * id;
+  inv[1][0] = (-a(1, 0) * c5 + a(1, 2) * c2 - a(1, 3) * c1) * id;
+  inv[1][1] = (a(0, 0) * c5 - a(0, 2) * c2 + a(0, 3) * c1) * id;
+  inv[1][2] = (-a(3, 0) * s5 + a(3, 2) * s2 - a(3, 3) * s1) * id;
+  inv[1][3] = (a(2, 0) * s5 - a(2, 2) * s2 + a(2, 3) * s1) * id;
+  inv[2][0] = (a(1, 0) * c4 - a(1, 1) * c2 + a(1, 3) * c0) * id;
+  inv[2][1] = (-a(0, 0) * c4 + a(0, 1) * c2 - a(0, 3) * c0) * id;
+  inv[2][2] = (a(3, 0) * s4 - a(3, 1) * s2 + a(3, 3) * s0) * id;
+  inv[2][3] = (-a(2, 0) * s4 + a(2, 1) * s2 - a(2, 3) * s0) * id;
+  inv[3][0] = (-a(1, 0) * c3 + a(1, 1) * c1 - a(1, 2) * c0) * id;
+  inv[3][1] = (a(0, 0) * c3 - a(0, 1) * c1 + a(0, 2) * c0) * id;
+  inv[3][2] = (-a(3, 0) * s3 + a(3, 1) * s1 - a(3, 2) * s0) * id;
+  inv[3][3] = (a(2, 0) * s3 - a(2, 1) * s1 + a(2, 2) * s0) * id;
+  for (int col = 0; col < 4; ++col)
+    for (int row = 0; row < 4; ++row) {
+      o->view[col][row] = (float)V[col][row];
+      o->proj[col][row] = (float)P[col][row];
+      o->view_proj[col][row] = (float)VP[col][row];
+      o->prev_view_proj[col][row] = (float)VP[col][row];
+      o->inv_view_proj[col][row] = (float)inv[row][col];
+    }
+  o->camera_position_world[0] = cam->position[0];
+  o->camera_position_world[1] = std::fmax(cam->position[1], 0.1f);  // test_harness.rs:356
+  o->camera_position_world[2] = cam->position[2];
+  o->viewport_size[0] = (float)width;
+  o->viewport_size[1] = (float)height;
+  o->viewport_size[2] = 1.0f / (float)width;
+  o->viewport_size[3] = 1.0f / (float)height;
+  // altaz_to_world, world.rs:110-114
+  const double sa = std::sin((double)sun_alt), ca = std::cos((double)sun_alt);
+  const double sz = std::sin((double)sun_az), cz = std::cos((double)sun_az);
+  o->sun_direction[0] = (float)(ca * sz);
+  o->sun_direction[1] = (float)sa;
+  o->sun_direction[2] = (float)(-ca * cz);
+  o->sun_direction[3] = sun_ang;
+  for (int k = 0; k < 4; ++k) o->sun_illuminance[k] = lux;
+  return PSC_OK;
+}
+
+// Void-and-cluster blue noise (crates/ps-clouds/src/noise.rs:646-704).
+int psc_generate_blue_noise(uint8_t* out) {
+  if (!out) return fail(PSC_ERR_INVALID_ARGUMENT, "null output");
+  const int S = 64, N = S * S, rad = 6;
+  const float sigma = 1.9f;
+  const float k = 1.0f / ((2.0f * sigma) * sigma);
+  // splat kernel, row-major over (dy, dx) in [-6, 6]^2
+  float kern[13 * 13];
+  for (int dy = -rad; dy <= rad; ++dy)
+    for (int dx = -rad; dx <= rad; ++dx)
+      kern[(dy + rad) * 13 + (dx + rad)] = std::exp(-(float)(dx * dx + dy * dy) * k) * 1.0f;
+  std::vector<float> energy(N, 0.0f);
+  std::vector<uint32_t> rank(N, 0);
+  std::vector<uint8_t> placed(N, 0);
+  for (int step = 0; step < N; ++step) {
+    int best = 0;
+    float be = INFINITY;
+    for (int i = 0; i < N; ++i)
+      if (!placed[i] && energy[i] < be) {
+        be = energy[i];
+        best = i;
+      }
+    placed[best] = 1;
+    rank[best] = (uint32_t)step;
+    const int cx = best % S, cy = best / S;
+    for (int dy = -rad; dy <= rad; ++dy) {
+      const int yy = ((cy + dy) % S + S) % S;
+      for (int dx = -rad; dx <= rad; ++dx) {
+        const int xx = ((cx + dx) % S + S) % S;
+        energy[yy * S + xx] += kern[(dy + rad) * 13 + (dx + rad)];
+      }
+    }
+  }
+  const float maxr = (float)(N - 1);
+  for (int i = 0; i < N; ++i) {
+    const float v = std::round(((float)rank[i] / maxr) * 255.0f);
+    out[i] = (uint8_t)std::fmin(std::fmax(v, 0.0f), 255.0f);
+  }
+  return PSC_OK;
+}
+
+// weather_map.rs:160-183
+static float wm_hash2(int32_t x, int32_t y) {
+  uint32_t h = (uint32_t)x * 2654435761u;
+  h ^= (uint32_t)y * 2246822519u;
+  h ^= h >> 16;
+  h *= 2654435761u;
+  h ^= h >> 13;
+  return std::fmin(std::fmax((float)h / 4294967296.0f, 0.0f), 1.0f);
+}
+static float wm_value_noise(float x, float y) {
+  const float xi = std::floor(x), yi = std::floor(y);
+  const float xf = x - xi, yf = y - yi;
+  const int32_t ix = (int32_t)xi, iy = (int32_t)yi;
+  const float h00 = wm_hash2(ix, iy), h10 = wm_hash2(ix + 1, iy);
+  const float h01 = wm_hash2(ix, iy + 1), h11 = wm_hash2(ix + 1, iy + 1);
+  const float sx = xf * xf * (3.0f - 2.0f * xf), sy = yf * yf * (3.0f - 2.0f * yf);
+  const float b = h00 + (h10 - h00) * sx, t = h01 + (h11 - h01) * sx;
+  return b + (t - b) * sy;
+}
+
+int psc_synthesise_weather_map(uint32_t n_layers, float precip, float wet, const float* grid,
+                               uint32_t gw, uint32_t gh, float gext, uint16_t* out) {
+  if (!out) return fail(PSC_ERR_INVALID_ARGUMENT, "null output");
+  if (grid && (gw < 1 || gh < 1 || !(gext > 0.0f)))
+    return fail(PSC_ERR_INVALID_ARGUMENT, "coverage grid needs w,h >= 1 and extent > 0");
+  const float gate = n_layers ? 1.0f : 0.0f;
+  const float alpha = std::fmax(std::fmin(std::fmax(precip / 50.0f, 0.0f), 1.0f),
+                                std::fmin(std::fmax(wet, 0.0f), 1.0f));
+  for (uint32_t y = 0; y < 128; ++y)
+    for (uint32_t x = 0; x < 128; ++x) {
+      float cov = gate;
+      if (grid) {  // coverage_grid.rs:34-60, sample_world
+        const float gx = (((float)x + 0.5f) / 128.0f) * 32000.0f - 16000.0f;
+        const float gy = (((float)y + 0.5f) / 128.0f) * 32000.0f - 16000.0f;
+        const float half = gext * 0.5f;
+        const float u = std::fmin(std::fmax((gx + half) / gext, 0.0f), 1.0f);
+        const float v = std::fmin(std::fmax((gy + half) / gext, 0.0f), 1.0f);
+        const float fx = u * ((float)gw - 1.0f), fy = v * ((float)gh - 1.0f);
+        const uint32_t x0 = (uint32_t)std::floor(fx), y0 = (uint32_t)std::floor(fy);
+        const uint32_t x1 = std::min(x0 + 1, gw - 1), y1 = std::min(y0 + 1, gh - 1);
+        const float tx = fx - (float)x0, ty = fy - (float)y0;
+        const float b = grid[y0 * gw + x0] + (grid[y0 * gw + x1] - grid[y0 * gw + x0]) * tx;
+        const float t = grid[y1 * gw + x0] + (grid[y1 * gw + x1] - grid[y1 * gw + x0]) * tx;
+        cov = std::fmin(std::fmax(b + (t - b) * ty, 0.0f), 1.0f);
+      }
+      const float bias = wm_value_noise((float)x * 0.05f, (float)y * 0.05f) * 2.0f - 1.0f;
+      uint16_t* t = out + (y * 128 + x) * 4;
+      t[0] = float_to_half_bits(cov);
+      t[1] = float_to_half_bits(0.0f);
+      t[2] = float_to_half_bits(bias);
+      t[3] = float_to_half_bits(alpha);
+    }
+  return PSC_OK;
+}
+
+int psc_synthesise_wind_field(float speed, float dir_deg, uint16_t* out) {  // wind_field.rs:150-170
+  if (!out) return fail(PSC_ERR_INVALID_ARGUMENT, "null output");
+  if (!std::isfinite(speed) || !std::isfinite(dir_deg)) return fail(PSC_ERR_NOT_FINITE, "non-finite wind");
+  const float pi = 3.14159265358979323846f;
+  const float to_rad = (dir_deg + 180.0f) * (pi / 180.0f);
+  const float ekman = 30.0f * pi / 180.0f;
+  for (uint32_t z = 0; z < 32; ++z)
+    for (uint32_t y = 0; y < 16; ++y)
+      for (uint32_t x = 0; x < 32; ++x) {
+        const float alt = ((float)y + 0.5f) / 16.0f * 12000.0f;
+        const float sp = speed * std::pow(std::fmax(alt, 10.0f) / 10.0f, 0.143f);
+        const float veer = std::pow(std::fmin(std::fmax(alt / 12000.0f, 0.0f), 1.0f), 0.7f);
+        const float ang = to_rad + veer * ekman;
+        uint16_t* t = out + ((z * 16 + y) * 32 + x) * 4;
+        t[0] = float_to_half_bits(sp * std::sin(ang));
+        t[1] = float_to_half_bits(sp * -std::cos(ang));
+        t[2] = 0;
+        t[3] = 0;
+      }
+  return PSC_OK;
+}
+
+int psc_create(int device, psc_ctx** out) {
+  if (!out) return fail(PSC_ERR_INVALID_ARGUMENT, "null output");
+  *out = nullptr;
+  // The device is bound lazily: host-side state and validation work without
+  // a GPU, and the first call that touches the device checks the ordinal.
+  if (device < 0) return fail(PSC_ERR_INVALID_ARGUMENT, "device %d is negative", device);
+  psc_ctx* c = new (std::nothrow) psc_ctx();
+  if (!c) return fail(PSC_ERR_OUT_OF_MEMORY, "context allocation");
+  c->device = device;
+  psc_params_default(&c->params);
+  c->params.cloud_layer_count = 0;
+  psc_world_default(&c->world);
+  psc_options_default(&c->opts);
+  *out = c;
+  return PSC_OK;
+}
+
+int psc_destroy(psc_ctx* c) {
+  if (!c) return PSC_OK;
+  const bool touched = c->d_base_u8 || c->d_detail_u8 || c->d_curl || c->d_blue || c->d_weather ||
+                       c->d_type || c->d_lut[0] || c->d_lut_h[0] || c->d_lut[2] || c->d_lut_h[3];
+  if (!touched) {
+    delete c;
+    return PSC_OK;
+  }
+  cudaSetDevice(c->device);
+  destroy_textures(c);
+  dfree(c->d_base_u8);
+  dfree(c->d_detail_u8);
+  dfree(c->d_base_store);
+  dfree(c->d_detail_store);
+  dfree(c->d_curl);
+  dfree(c->d_blue);
+  dfree(c->d_weather);
+  dfree(c->d_type);
+  for (int k = 0; k < 4; ++k) {
+    dfree(c->d_lut[k]);
+    dfree(c->d_lut_h[k]);
+  }
+  delete c;
+  return PSC_OK;
+}
+
+int psc_set_march_steps(psc_ctx* c, uint32_t cloud, uint32_t light) {  // lib.rs:709-712
+  if (!c) return fail(PSC_ERR_INVALID_ARGUMENT, "null context");
+  c->params.cloud_steps = std::min(std::max(cloud, 8u), 256u);
+  c->params.light_steps = std::min(std::max(light, 1u), 16u);
+  return PSC_OK;
+}
+
+int psc_set_params(psc_ctx* c, const PscCloudParamsGpu* p) {
+  if (!c || !p) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  PscCloudParamsGpu q = *p;
+  q.cloud_layer_count = c->n_layers;  // owned by psc_set_layers
+  const int rc = validate_params(q);
+  if (rc) return rc;
+  c->params = q;
+  return PSC_OK;
+}
+
+int psc_get_params(psc_ctx* c, PscCloudParamsGpu* out) {
+  if (!c || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  *out = c->params;
+  return PSC_OK;
+}
+
+int psc_set_layers(psc_ctx* c, const PscCloudLayerGpu* l, uint32_t n) {
+  if (!c || (n && !l)) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  const int rc = validate_layers(l, n);
+  if (rc) return rc;
+  std::memset(c->layers, 0, sizeof(c->layers));
+  for (uint32_t i = 0; i < n; ++i) c->layers[i] = l[i];
+  c->n_layers = n;
+  c->params.cloud_layer_count = n;
+  return PSC_OK;
+}
+
+int psc_set_frame(psc_ctx* c, const PscFrameUniformsGpu* f, const PscWorldUniformsGpu* w) {
+  if (!c || !f || !w) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  const float* ff = reinterpret_cast<const float*>(f);
+  for (size_t i = 0; i < sizeof(*f) / 4; ++i)
+    if (i != 94 && !std::isfinite(ff[i]))  // word 94 = frame_index (u32)
+      return fail(PSC_ERR_NOT_FINITE, "FrameUniforms word %zu is not finite", i);
+  if (!all_finite(reinterpret_cast<const float*>(w), sizeof(*w) / 4))
+    return fail(PSC_ERR_NOT_FINITE, "WorldUniforms has a non-finite field");
+  if (!(w->planet_radius_m > 0.0f) || !(w->atmosphere_top_m > w->planet_radius_m))
+    return fail(PSC_ERR_INVALID_ARGUMENT, "need 0 < planet_radius_m < atmosphere_top_m");
+  c->frame = *f;
+  c->world = *w;
+  c->have_frame = true;
+  return PSC_OK;
+}
+
+int psc_set_options(psc_ctx* c, const PscMarchOptions* o) {
+  if (!c || !o) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (o->phase_mode > PSC_PHASE_DUAL_LOBE_HG) return fail(PSC_ERR_INVALID_ARGUMENT, "bad phase_mode");
+  if (o->storage > PSC_STORAGE_FP8) return fail(PSC_ERR_INVALID_ARGUMENT, "bad storage");
+  if (o->filter > PSC_FILTER_TEXTURE) return fail(PSC_ERR_INVALID_ARGUMENT, "bad filter");
+  if (o->schedule > PSC_SCHED_FAST) return fail(PSC_ERR_INVALID_ARGUMENT, "bad schedule");
+  if (o->filter == PSC_FILTER_TEXTURE && o->storage != PSC_STORAGE_U8)
+    return fail(PSC_ERR_UNSUPPORTED, "texture filtering reads the RGBA8 volumes (storage U8 only)");
+  const float hv[] = {o->hg_g_forward, o->hg_g_backward, o->hg_blend};
+  if (!all_finite(hv, 3)) return fail(PSC_ERR_NOT_FINITE, "non-finite HG lobe");
+  c->opts = *o;
+  return PSC_OK;
+}
+
+int psc_bake_noise(psc_ctx* c) {
+  if (!c) return fail(PSC_ERR_INVALID_ARGUMENT, "null context");
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  if (!c->d_base_u8) PSC_CUDA(cudaMalloc(&c->d_base_u8, 128u * 128u * 128u * 4u), "cudaMalloc base");
+  if (!c->d_detail_u8) PSC_CUDA(cudaMalloc(&c->d_detail_u8, 32u * 32u * 32u * 4u), "cudaMalloc detail");
+  if (!c->d_curl) PSC_CUDA(cudaMalloc(&c->d_curl, 128u * 128u * 2u), "cudaMalloc curl");
+  if (psc::launch_noise_bakes(c->d_base_u8, c->d_detail_u8, c->d_curl, 0))
+    return fail(PSC_ERR_CUDA, "noise bake failed: %s", cudaGetErrorString(cudaGetLastError()));
+  c->have_base = c->have_detail = c->have_curl = true;
+  std::vector<uint8_t> blue(64 * 64);
+  psc_generate_blue_noise(blue.data());
+  rc = psc_upload_noise(c, PSC_NOISE_BLUE, blue.data(), blue.size());
+  if (rc) return rc;
+  c->store_form = -1;
+  c->tex_dirty = true;
+  return build_storage(c);
+}
+
+int psc_upload_noise(psc_ctx* c, int kind, const void* texels, size_t bytes) {
+  if (!c || !texels) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  const size_t need[] = {128u * 128u * 128u * 4u, 32u * 32u * 32u * 4u, 128u * 128u * 2u, 64u * 64u};
+  if (kind < 0 || kind > 3) return fail(PSC_ERR_INVALID_ARGUMENT, "bad noise kind %d", kind);
+  if (bytes != need[kind]) return fail(PSC_ERR_INVALID_ARGUMENT, "noise kind %d needs %zu bytes, got %zu", kind, need[kind], bytes);
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  if (kind == PSC_NOISE_BLUE) {
+    std::vector<float> f(64 * 64);
+    const uint8_t* b = static_cast<const uint8_t*>(texels);
+    for (int i = 0; i < 64 * 64; ++i) f[i] = (float)b[i] / 255.0f;
+    if (!c->d_blue) PSC_CUDA(cudaMalloc(&c->d_blue, f.size() * 4), "cudaMalloc blue");
+    PSC_CUDA(cudaMemcpy(c->d_blue, f.data(), f.size() * 4, cudaMemcpyHostToDevice), "blue upload");
+    c->h_blue.assign(b, b + 64 * 64);
+    c->have_blue = true;
+    return PSC_OK;
+  }
+  uint8_t** dst = kind == PSC_NOISE_BASE ? &c->d_base_u8 : kind == PSC_NOISE_DETAIL ? &c->d_detail_u8 : &c->d_curl;
+  if (!*dst) PSC_CUDA(cudaMalloc(dst, bytes), "cudaMalloc noise");
+  PSC_CUDA(cudaMemcpy(*dst, texels, bytes, cudaMemcpyHostToDevice), "noise upload");
+  if (kind == PSC_NOISE_BASE) c->have_base = true;
+  if (kind == PSC_NOISE_DETAIL) c->have_detail = true;
+  if (kind == PSC_NOISE_CURL) c->have_curl = true;
+  c->store_form = -1;
+  c->tex_dirty = true;
+  return build_storage(c);
+}
+
+int psc_download_noise(psc_ctx* c, int kind, void* texels, size_t bytes) {
+  if (!c || !texels) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  const size_t need[] = {128u * 128u * 128u * 4u, 32u * 32u * 32u * 4u, 128u * 128u * 2u, 64u * 64u};
+  if (kind < 0 || kind > 3) return fail(PSC_ERR_INVALID_ARGUMENT, "bad noise kind %d", kind);
+  if (bytes != need[kind]) return fail(PSC_ERR_INVALID_ARGUMENT, "noise kind %d needs %zu bytes", kind, need[kind]);
+  if (kind == PSC_NOISE_BLUE) {
+    if (!c->have_blue) return fail(PSC_ERR_MISSING_INPUT, "no blue noise");
+    std::memcpy(texels, c->h_blue.data(), bytes);
+    return PSC_OK;
+  }
+  const uint8_t* src = kind == PSC_NOISE_BASE ? c->d_base_u8 : kind == PSC_NOISE_DETAIL ? c->d_detail_u8 : c->d_curl;
+  if (!src) return fail(PSC_ERR_MISSING_INPUT, "noise kind %d not present", kind);
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  PSC_CUDA(cudaMemcpy(texels, src, bytes, cudaMemcpyDeviceToHost), "noise download");
+  return PSC_OK;
+}
+
+int psc_upload_weather(psc_ctx* c, const void* texels, uint32_t w, uint32_t h, int format) {
+  if (!c || !texels) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (!w || !h || w > 16384 || h > 16384) return fail(PSC_ERR_INVALID_ARGUMENT, "weather size %ux%u out of range", w, h);
+  std::vector<float> r((size_t)w * h);
+  for (size_t i = 0; i < r.size(); ++i) {
+    switch (format) {
+      case PSC_WEATHER_RGBA16F: r[i] = half_bits_to_float(static_cast<const uint16_t*>(texels)[i * 4]); break;
+      case PSC_WEATHER_RG8: r[i] = (float)static_cast<const uint8_t*>(texels)[i * 2] / 255.0f; break;
+      case PSC_WEATHER_R32F: r[i] = static_cast<const float*>(texels)[i]; break;
+      default: return fail(PSC_ERR_INVALID_ARGUMENT, "bad weather format %d", format);
+    }
+    if (!std::isfinite(r[i])) return fail(PSC_ERR_NOT_FINITE, "weather texel %zu is not finite", i);
+  }
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  if (c->d_weather && (c->weather_w != w || c->weather_h != h)) dfree(c->d_weather);
+  if (!c->d_weather) PSC_CUDA(cudaMalloc(&c->d_weather, r.size() * 4), "cudaMalloc weather");
+  PSC_CUDA(cudaMemcpy(c->d_weather, r.data(), r.size() * 4, cudaMemcpyHostToDevice), "weather upload");
+  c->weather_w = w;
+  c->weather_h = h;
+  return PSC_OK;
+}
+
+int psc_upload_type_grid(psc_ctx* c, const uint8_t* texels, uint32_t w, uint32_t h) {
+  if (!c) return fail(PSC_ERR_INVALID_ARGUMENT, "null context");
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  if (!texels) {  // no grid: every sample uses its layer's type
+    dfree(c->d_type);
+    c->type_w = c->type_h = 0;
+    return PSC_OK;
+  }
+  if (!w || !h || w > 16384 || h > 16384) return fail(PSC_ERR_INVALID_ARGUMENT, "type grid size %ux%u out of range", w, h);
+  for (size_t i = 0; i < (size_t)w * h; ++i)
+    if (texels[i] > 7 && texels[i] != PSC_TYPE_SENTINEL)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "type grid texel %zu = %u is neither 0..7 nor 255", i, texels[i]);
+  if (c->d_type && (c->type_w != w || c->type_h != h)) dfree(c->d_type);
+  if (!c->d_type) PSC_CUDA(cudaMalloc(&c->d_type, (size_t)w * h), "cudaMalloc type grid");
+  PSC_CUDA(cudaMemcpy(c->d_type, texels, (size_t)w * h, cudaMemcpyHostToDevice), "type grid upload");
+  c->type_w = w;
+  c->type_h = h;
+  return PSC_OK;
+}
+
+int psc_upload_wind(psc_ctx* c, const uint16_t* rgba16f, size_t count) {
+  if (!c || !rgba16f) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (count != 32u * 16u * 32u * 4u) return fail(PSC_ERR_INVALID_ARGUMENT, "wind field needs 32x16x32x4 halves");
+  c->h_wind.assign(rgba16f, rgba16f + count);
+  return PSC_OK;
+}
+
+int psc_upload_lut(psc_ctx* c, int kind, const uint16_t* rgba16f, size_t count) {
+  if (!c || !rgba16f) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (kind < 0 || kind > 3) return fail(PSC_ERR_INVALID_ARGUMENT, "bad LUT kind %d", kind);
+  if (count != lut_texels(kind) * 4) return fail(PSC_ERR_INVALID_ARGUMENT, "LUT %d needs %zu halves", kind, lut_texels(kind) * 4);
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  if (!c->d_lut_h[kind]) PSC_CUDA(cudaMalloc(&c->d_lut_h[kind], count * 2), "cudaMalloc LUT");
+  PSC_CUDA(cudaMemcpy(c->d_lut_h[kind], rgba16f, count * 2, cudaMemcpyHostToDevice), "LUT upload");
+  return upload_lut_float4(c, kind, rgba16f);
+}
+
+int psc_bake_luts(psc_ctx* c, void* stream) {
+  if (!c) return fail(PSC_ERR_INVALID_ARGUMENT, "null context");
+  if (!c->have_frame) return fail(PSC_ERR_MISSING_INPUT, "psc_set_frame must precede psc_bake_luts");
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  for (int k = 0; k < 4; ++k)
+    if (!c->d_lut_h[k]) PSC_CUDA(cudaMalloc(&c->d_lut_h[k], lut_texels(k) * 8), "cudaMalloc LUT");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (psc::launch_lut_bakes(c->world, c->frame, c->d_lut_h[0], c->d_lut_h[1], c->d_lut_h[2], c->d_lut_h[3], s))
+    return fail(PSC_ERR_CUDA, "LUT bake launch failed");
+  PSC_CUDA(cudaStreamSynchronize(s), "LUT bake");
+  std::vector<uint16_t> h;
+  for (int k = 0; k < 4; ++k) {
+    h.resize(lut_texels(k) * 4);
+    PSC_CUDA(cudaMemcpy(h.data(), c->d_lut_h[k], h.size() * 2, cudaMemcpyDeviceToHost), "LUT readback");
+    rc = upload_lut_float4(c, k, h.data());
+    if (rc) return rc;
+  }
+  return PSC_OK;
+}
+
+int psc_download_lut(psc_ctx* c, int kind, uint16_t* out, size_t count) {
+  if (!c || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (kind < 0 || kind > 3) return fail(PSC_ERR_INVALID_ARGUMENT, "bad LUT kind %d", kind);
+  if (count != lut_texels(kind) * 4) return fail(PSC_ERR_INVALID_ARGUMENT, "LUT %d needs %zu halves", kind, lut_texels(kind) * 4);
+  if (!c->d_lut_h[kind]) return fail(PSC_ERR_MISSING_INPUT, "LUT %d not present", kind);
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  PSC_CUDA(cudaMemcpy(out, c->d_lut_h[kind], count * 2, cudaMemcpyDeviceToHost), "LUT download");
+  return PSC_OK;
+}
+
+int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
+  if (!c || (n && !views)) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (!c->have_frame) return fail(PSC_ERR_MISSING_INPUT, "psc_set_frame was not called");
+  if (!c->have_base || !c->have_detail || !c->have_curl || !c->have_blue)
+    return fail(PSC_ERR_MISSING_INPUT, "noise volumes missing (psc_bake_noise or psc_upload_noise)");
+  if (!c->d_weather) return fail(PSC_ERR_MISSING_INPUT, "weather map missing (psc_upload_weather)");
+  if (!c->have_lut[PSC_LUT_TRANSMITTANCE] || !c->have_lut[PSC_LUT_SKYVIEW] || !c->have_lut[PSC_LUT_AERIAL])
+    return fail(PSC_ERR_MISSING_INPUT, "atmosphere LUTs missing (psc_upload_lut or psc_bake_luts)");
+  int rc = validate_params(c->params);
+  if (rc) return rc;
+  rc = ensure_device(c);
+  if (rc) return rc;
+  rc = build_storage(c);
+  if (rc) return rc;
+  rc = build_textures(c);
+  if (rc) return rc;
+  if (c->opts.filter == PSC_FILTER_TEXTURE && (!c->tex_base || !c->tex_detail))
+    return fail(PSC_ERR_MISSING_INPUT, "texture objects for the noise volumes were not created");
+  for (uint32_t i = 0; i < n; ++i) {
+    const PscView& v = views[i];
+    if (!v.width || !v.height || v.width > 32768 || v.height > 32768)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: size %ux%u out of range", i, v.width, v.height);
+    if (!v.out_luminance && !v.out_transmittance && !(c->opts.composite && v.hdr))
+      return fail(PSC_ERR_INVALID_ARGUMENT, "view %u has no output buffer", i);
+    if (c->opts.composite && !v.hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: composite needs hdr", i);
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  psc::MarchUniforms u;
+  for (uint32_t i = 0; i < n; ++i) {
+    const PscView& v = views[i];
+    build_uniforms(c, v.width, v.height, u);
+    psc::ViewDev vd{v.width, v.height, v.depth, reinterpret_cast<float4*>(v.out_luminance),
+                    reinterpret_cast<float4*>(v.out_transmittance), reinterpret_cast<float4*>(v.hdr)};
+    rc = psc::launch_march(u, vd, c->opts, s);
+    if (rc) return fail(rc, "march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    ++c->launches;
+  }
+  return PSC_OK;
+}
+
+int psc_composite(const float* l, const float* t, float* hdr, uint32_t w, uint32_t h, void* stream) {
+  if (!l || !t || !hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "null buffer");
+  if (!w || !h) return fail(PSC_ERR_INVALID_ARGUMENT, "zero-size composite");
+  if (psc::launch_composite(reinterpret_cast<const float4*>(l), reinterpret_cast<const float4*>(t),
+                            reinterpret_cast<float4*>(hdr), w * h, static_cast<cudaStream_t>(stream)))
+    return fail(PSC_ERR_CUDA, "composite launch failed");
+  return PSC_OK;
+}
+
+int psc_launch_count(psc_ctx* c, uint64_t* out) {
+  if (!c || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  *out = c->launches;
+  return PSC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,120 @@
+// Internal layout shared by the host library and the CUDA kernels.
+//
+// The host flattens the reference's uniforms (CloudParams, FrameUniforms,
+// WorldUniforms, the 8-entry layer array) plus everything that is constant
+// per layer or per frame into one `MarchUniforms` block, passed to the march
+// kernel by value as a __grid_constant__ parameter (it lives in the constant
+// bank; every lane reads the same address, so these loads broadcast).
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/psclouds.h"
+
+#ifndef __CUDACC__
+#include <cuda_runtime_api.h>
+#else
+#include <cuda_runtime.h>
+#endif
+
+namespace psc {
+
+constexpr float kPi = 3.14159265358979f;  // HG_PI, cloud_march.wgsl:71
+
+// Per-layer constants.  Everything here is a pure function of the layer,
+// CloudParams, the wind field and the sun direction, so the host computes
+// it once per frame instead of every pixel re-deriving it.
+struct LayerConst {
+  float base_m, top_m;
+  float inv_thickness;     // 1 / max(top - base, 1)
+  float coverage;
+  float density_scale;
+  uint32_t cloud_type;
+  float lf_bias;           // shape_bias * diurnal(layer.type) * 0.5
+  float layer_detail;      // clamp(detail_strength + detail_bias * diurnal, 0, 1)
+  float anvil_bias;
+  float droplet_um;
+  float sigma_t[3];        // (sigma_s + sigma_a) * chromatic_mie_modulation(d)
+  float wind_off_x, wind_off_z;   // LayerWindCache.wind_offset
+  float skew_x, skew_z, skew_thickness;
+  // Approx-Mie constants (cloud_phase_constants); exact for every layer
+  // type except Cumulonimbus, whose diameter depends on height.
+  float g_hg, g_d, alpha, w_d, ice;
+  float _pad;
+  double r_bottom, r_top;  // planet_radius + base/top, FP64
+};
+
+struct MarchUniforms {
+  // frame
+  float inv_vp[4][4];      // inv_view_proj, [col][row]
+  double inv_vp_d[4][4];   // the same matrix widened to double
+  float cam[3];
+  float sun[3];
+  float sun_illum[3];
+  float lightning_rgb[3];
+  float lightning_radius;
+  float lightning_origin_x, lightning_origin_z;
+  float vp_w, vp_h;        // viewport used for NDC and AP uv
+  uint32_t temporal_jitter;
+  uint32_t frame_index;
+  float fwd_factor_unused;
+  // world
+  float planet_r, atmo_top;
+  double planet_r_d;
+  // params
+  float sigma_s[3];
+  float droplet_bias;
+  float forward_bias;
+  float detail_strength, curl_strength, powder;
+  float ms_a, ms_b, ms_c;
+  float ambient;
+  float base_scale, detail_scale, weather_scale;  // already max(., 1)
+  uint32_t light_steps, cloud_steps, octaves, layer_count;
+  uint32_t cone;
+  // options
+  uint32_t phase_mode;
+  float hg_f, hg_b, hg_w;
+  uint32_t kahan;
+  uint32_t composite;
+  uint32_t debug_checks;
+  LayerConst layers[8];
+
+  // inputs (device pointers)
+  const void* noise_base;      // layout depends on storage
+  const void* noise_detail;
+  float noise_scale;           // value = stored * scale (F16/BF16/FP8)
+  const uint8_t* curl;         // 128^2 RG8
+  const float* blue;           // 64^2, already v/255
+  const float* weather;        // R channel as float, weather_w x weather_h
+  uint32_t weather_w, weather_h;
+  const uint8_t* type_grid;    // may be null (all sentinel)
+  uint32_t type_w, type_h;
+  const float4* lut_trans;     // 256x64
+  const float4* lut_sky;       // 192x108
+  const float4* lut_ap;        // 32x32x64
+  cudaTextureObject_t tex_base, tex_detail;  // PSC_FILTER_TEXTURE only
+  int* error_word;             // device, debug checks
+};
+
+// One view of a launch.
+struct ViewDev {
+  uint32_t width, height;
+  const float* depth;
+  float4* out_l;
+  float4* out_t;
+  float4* hdr;
+};
+
+// Launchers (march.cu).
+int launch_march(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
+                 cudaStream_t stream);
+int launch_composite(const float4* l, const float4* t, float4* hdr, uint32_t n,
+                     cudaStream_t stream);
+// Noise bakes (noise_bake.cu), synchronous on `stream`.
+int launch_noise_bakes(uint8_t* base, uint8_t* detail, uint8_t* curl, cudaStream_t stream);
+// Atmosphere LUT bakes (atmosphere.cu).
+int launch_lut_bakes(const PscWorldUniformsGpu& world, const PscFrameUniformsGpu& frame,
+                     uint16_t* trans_f16, uint16_t* ms_f16, uint16_t* sky_f16,
+                     uint16_t* ap_f16, cudaStream_t stream);
+
+}  // namespace psc

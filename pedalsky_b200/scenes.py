@@ -1,0 +1,283 @@
+"""Seeded synthetic scenes for the cloud-march workloads.
+
+Every scene is assembled the way the reference's headless render assembles
+one (crates/ps-app/src/test_harness.rs:335-390): `CloudParamsGpu::default()`
+overridden by the `[render.clouds]` tuning defaults
+(crates/ps-core/src/config.rs:469-488 via crates/ps-clouds/src/lib.rs:561-600),
+layers through `synthesise_cloud_layers`, the reference weather map and wind
+field, frame uniforms from a `FlyCamera`, and determinism switches as the
+golden harness sets them (wind drift 0, diurnal 0, simulated_seconds 0;
+crates/ps-app/tests/golden.rs:112,119).
+
+All host arithmetic goes through the C ABI helpers of libpsclouds.so.
+Workloads:
+  plain_320x180   one Cumulus layer 1500-2300 m, coverage 0.5, 320x180,
+                  64/6 steps, 3 octaves, dual-lobe HG 0.8/-0.2 w=0.5
+  plain_literal   the same with the 512^2 RG8 weather map 0.5+0.15*noise
+  precision_1080p Cumulus 1500-2300 (0.5), Altostratus 4000-5000 (0.7),
+                  Cirrus 8000-9000 (0.3), 1920x1080, 128/6 steps
+  stress_2160p    Cumulonimbus 600-12000 m, coverage 0.8, 2048^2 f32
+                  coverage grid, 3840x2160, 256/8 steps, 15 m/s wind
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi
+from .capi import call
+
+CLOUD_TYPES = ("Cumulus", "Stratus", "Stratocumulus", "Altocumulus", "Altostratus",
+               "Cirrus", "Cirrostratus", "Cumulonimbus")
+TOA_LUX = 127500.0          # crates/ps-core/src/world.rs:139-146
+SUN_ANGULAR_RADIUS = math.radians(0.27)  # config.rs:343
+
+
+@dataclass
+class Scene:
+    name: str
+    width: int
+    height: int
+    params: capi.CloudParamsGpu
+    layers: object                      # CloudLayerGpu * 8
+    n_layers: int
+    frame: capi.FrameUniformsGpu
+    world: capi.WorldUniformsGpu
+    options: capi.MarchOptions
+    weather: np.ndarray
+    weather_w: int
+    weather_h: int
+    weather_format: int
+    wind: np.ndarray                    # 32x16x32x4 float16 bits (uint16)
+    type_grid: np.ndarray | None = None
+    depth: np.ndarray | None = None     # (h, w) float32 reverse-Z, 0 = sky
+    background: np.ndarray | None = None  # (h, w, 4) float32 HDR backdrop
+    extra: dict = field(default_factory=dict)
+
+
+def default_params() -> capi.CloudParamsGpu:
+    """CloudParamsGpu::default() + CloudsTuning::default() as CloudsSubsystem::new applies it."""
+    p = capi.CloudParamsGpu()
+    call("psc_params_default", C.byref(p))
+    p.cloud_steps, p.light_steps, p.multi_scatter_octaves = 192, 6, 4
+    p.detail_strength = 0.35       # CloudsTuning::default (config.rs:484)
+    p.powder_strength = 1.0
+    p.wind_drift_strength = 0.0    # golden determinism
+    p.diurnal_strength = 0.0
+    p.wind_skew_strength = 0.5
+    return p
+
+
+def world_default() -> capi.WorldUniformsGpu:
+    w = capi.WorldUniformsGpu()
+    call("psc_world_default", C.byref(w))
+    return w
+
+
+def options(phase=capi.PHASE_APPROX_MIE, storage=capi.STORAGE_U8, filt=capi.FILTER_EXACT,
+            schedule=capi.SCHED_PLAIN, kahan=0, composite=0) -> capi.MarchOptions:
+    o = capi.MarchOptions()
+    call("psc_options_default", C.byref(o))
+    o.phase_mode, o.storage, o.filter, o.schedule = phase, storage, filt, schedule
+    o.kahan, o.composite = kahan, composite
+    return o
+
+
+def synth_layers(descs: list[tuple]) -> tuple[object, int]:
+    """descs: (type, base, top, coverage[, density_scale]); returns (CloudLayerGpu*8, n)."""
+    n = len(descs)
+    arr = (capi.CloudLayerDesc * max(n, 1))()
+    for i, d in enumerate(descs):
+        t, base, top, cov = d[:4]
+        dens = d[4] if len(d) > 4 else -1.0
+        arr[i] = capi.CloudLayerDesc(t, base, top, cov, dens, 0.0, 0.0, -1.0, -1.0)
+    out = (capi.CloudLayerGpu * 8)()
+    call("psc_synthesise_layers", arr, n, out)
+    return out, n
+
+
+def frame_for(width, height, cam_pos=(0.0, 100.0, 0.0), pitch_deg=10.0, yaw_deg=0.0,
+              fov_deg=90.0, sun_alt_deg=35.0, sun_az_deg=240.0, sim_seconds=0.0):
+    cam = capi.FlyCamera((C.c_float * 3)(*cam_pos), math.radians(pitch_deg), math.radians(yaw_deg),
+                         0.0, math.radians(fov_deg), 0.1)
+    f = capi.FrameUniformsGpu()
+    call("psc_frame_from_camera", C.byref(cam), width, height, math.radians(sun_alt_deg),
+         math.radians(sun_az_deg), SUN_ANGULAR_RADIUS, TOA_LUX, C.byref(f))
+    f.simulated_seconds = sim_seconds
+    return f
+
+
+def reference_weather(n_layers: int, grid: np.ndarray | None = None, grid_extent=32000.0):
+    out = np.zeros(128 * 128 * 4, np.uint16)
+    if grid is None:
+        call("psc_synthesise_weather_map", n_layers, 0.0, 0.0, None, 0, 0, 0.0, capi.ptr(out))
+    else:
+        g = np.ascontiguousarray(grid, np.float32)
+        call("psc_synthesise_weather_map", n_layers, 0.0, 0.0, capi.ptr(g), g.shape[1],
+             g.shape[0], grid_extent, capi.ptr(out))
+    return out
+
+
+def wind_field(speed=5.0, dir_deg=240.0):
+    """Surface::default() wind (scene.rs:217-218) unless given."""
+    out = np.zeros(32 * 16 * 32 * 4, np.uint16)
+    call("psc_synthesise_wind_field", speed, dir_deg, capi.ptr(out))
+    return out
+
+
+def _hash2(x, y):
+    """weather_map.rs:178-183 on int32 arrays (u32 wrap)."""
+    h = (x.astype(np.uint32) * np.uint32(2654435761)).astype(np.uint32)
+    h ^= (y.astype(np.uint32) * np.uint32(2246822519)).astype(np.uint32)
+    h ^= h >> np.uint32(16)
+    h = (h * np.uint32(2654435761)).astype(np.uint32)
+    h ^= h >> np.uint32(13)
+    return np.clip(h.astype(np.float32) / np.float32(4294967296.0), 0, 1)
+
+
+def value_noise(x, y):
+    """value_noise_2d, weather_map.rs:160-176 (float32)."""
+    x = np.asarray(x, np.float32)
+    y = np.asarray(y, np.float32)
+    xi, yi = np.floor(x), np.floor(y)
+    xf, yf = x - xi, y - yi
+    ix, iy = xi.astype(np.int32), yi.astype(np.int32)
+    h00, h10 = _hash2(ix, iy), _hash2(ix + 1, iy)
+    h01, h11 = _hash2(ix, iy + 1), _hash2(ix + 1, iy + 1)
+    sx = xf * xf * (np.float32(3) - np.float32(2) * xf)
+    sy = yf * yf * (np.float32(3) - np.float32(2) * yf)
+    b = h00 + (h10 - h00) * sx
+    t = h01 + (h11 - h01) * sx
+    return (b + (t - b) * sy).astype(np.float32)
+
+
+def literal_weather_rg8(size=512):
+    """512^2 RG8: R = 0.5 + 0.15 * value_noise at the reference map's spatial
+    frequency (0.05 per 250 m texel), G = cloud type 0."""
+    yy, xx = np.mgrid[0:size, 0:size].astype(np.float32)
+    s = np.float32(0.05 * 128.0 / size)
+    vn = value_noise(xx * s, yy * s)
+    r = np.clip(np.rint((np.float32(0.5) + np.float32(0.15) * vn) * 255.0), 0, 255).astype(np.uint8)
+    rg = np.zeros((size, size, 2), np.uint8)
+    rg[..., 0] = r
+    return rg.reshape(-1)
+
+
+def view_rays(frame: capi.FrameUniformsGpu, width: int, height: int):
+    """Per-pixel world directions (float64) as compute_view_ray builds them."""
+    inv = np.array(frame.inv_view_proj, np.float64)  # [col][row]
+    cam = np.array(frame.camera_position_world[:3], np.float64)
+    xs = (np.arange(width) + 0.5) / width * 2 - 1
+    ys = 1 - (np.arange(height) + 0.5) / height * 2
+    nx, ny = np.meshgrid(xs, ys)
+    h = (inv[0][None, None, :] * nx[..., None] + inv[1][None, None, :] * ny[..., None]
+         + inv[2][None, None, :] + inv[3][None, None, :])
+    p = h[..., :3] / h[..., 3:4]
+    d = p - cam
+    return d / np.linalg.norm(d, axis=-1, keepdims=True)
+
+
+def ground_depth(frame, world, width, height):
+    """Headless ground: reverse-Z depth of the planet sphere (0 where the ray sees sky)."""
+    d = view_rays(frame, width, height)
+    cam = np.array(frame.camera_position_world[:3], np.float64)
+    R = float(world.planet_radius_m)
+    oc = cam + np.array([0.0, R, 0.0])
+    b = d @ oc
+    c = oc @ oc - R * R
+    disc = b * b - c
+    hit = disc >= 0
+    t = -b - np.sqrt(np.where(hit, disc, 0))
+    hit &= t > 0
+    X = cam + d * t[..., None]
+    vp = np.array(frame.view_proj, np.float64)
+    clip = vp[0] * X[..., 0:1] + vp[1] * X[..., 1:2] + vp[2] * X[..., 2:3] + vp[3]
+    depth = np.where(hit, clip[..., 2] / clip[..., 3], 0.0)
+    return depth.astype(np.float32)
+
+
+def sky_background(frame, width, height):
+    """Smooth HDR backdrop the composite blends over (cd/m^2 scale)."""
+    d = view_rays(frame, width, height)
+    up = np.clip(d[..., 1], -1, 1)
+    sky = 2500.0 + 6000.0 * (1.0 - np.abs(up)) ** 2
+    tint = np.array([0.72, 0.86, 1.0])
+    bg = np.empty((height, width, 4), np.float32)
+    bg[..., :3] = (sky[..., None] * tint).astype(np.float32)
+    bg[..., :3] = np.where(up[..., None] < 0, 900.0 * np.array([0.55, 0.5, 0.45]), bg[..., :3])
+    bg[..., 3] = 1.0
+    return bg
+
+
+def _finish(name, width, height, params, layers_n, frame, opts, weather, ww, wh, wfmt,
+            type_grid=None, with_ground=True, wind=None):
+    layers, n = layers_n
+    world = world_default()
+    params.cloud_layer_count = n
+    depth = ground_depth(frame, world, width, height) if with_ground else None
+    return Scene(name, width, height, params, layers, n, frame, world, opts, weather, ww, wh, wfmt,
+                 wind if wind is not None else wind_field(), type_grid, depth,
+                 sky_background(frame, width, height))
+
+
+def plain_320x180(width=320, height=180, phase=capi.PHASE_DUAL_LOBE_HG, **kw) -> Scene:
+    p = default_params()
+    p.cloud_steps, p.light_steps, p.multi_scatter_octaves = 64, 6, 3
+    ln = synth_layers([(0, 1500.0, 2300.0, 0.5, 1.0)])
+    frame = frame_for(width, height)
+    return _finish("plain_320x180", width, height, p, ln, frame, options(phase=phase, **kw),
+                   reference_weather(ln[1]), 128, 128, capi.WEATHER_RGBA16F)
+
+
+def plain_literal(width=320, height=180, **kw) -> Scene:
+    s = plain_320x180(width, height, **kw)
+    s.name = "plain_literal"
+    s.weather, s.weather_w, s.weather_h = literal_weather_rg8(), 512, 512
+    s.weather_format = capi.WEATHER_RG8
+    s.type_grid = np.zeros(512 * 512, np.uint8)
+    return s
+
+
+def precision_1080p(width=1920, height=1080, steps=128, **kw) -> Scene:
+    p = default_params()
+    p.cloud_steps, p.light_steps = steps, 6
+    ln = synth_layers([(0, 1500.0, 2300.0, 0.5), (4, 4000.0, 5000.0, 0.7),
+                       (5, 8000.0, 9000.0, 0.3)])
+    frame = frame_for(width, height)
+    return _finish("precision_1080p", width, height, p, ln, frame, options(**kw),
+                   reference_weather(ln[1]), 128, 128, capi.WEATHER_RGBA16F)
+
+
+def mountain_wave_grid(size=2048, seed=0, wavelength_m=8000.0, amplitude=0.3, extent=32000.0):
+    """2048^2 f32 coverage grid: mountain-wave sinusoid + seeded value noise."""
+    rng = np.random.default_rng(seed)
+    off = rng.uniform(0, 1000, 2).astype(np.float32)
+    x = (np.arange(size, dtype=np.float32) + 0.5) / size * extent - extent / 2
+    X, Y = np.meshgrid(x, x)
+    wave = amplitude * np.sin(2 * np.pi * X / wavelength_m)
+    vn = value_noise(X / 1500.0 + off[0], Y / 1500.0 + off[1])
+    return np.clip(0.55 + wave + 0.35 * (vn - 0.5), 0, 1).astype(np.float32)
+
+
+def stress_2160p(width=3840, height=2160, frame_index=0, **kw) -> Scene:
+    p = default_params()
+    p.cloud_steps, p.light_steps = 256, 8
+    p.wind_drift_strength = 1.0
+    ln = synth_layers([(7, 600.0, 12000.0, 0.8)])
+    frame = frame_for(width, height, sim_seconds=float(frame_index))
+    grid = mountain_wave_grid()
+    s = _finish("stress_2160p", width, height, p, ln, frame, options(**kw), grid.reshape(-1),
+                2048, 2048, capi.WEATHER_R32F, wind=wind_field(15.0 / 1.0, 240.0))
+    s.extra["frame_index"] = frame_index
+    return s
+
+
+WORKLOADS = {
+    "plain_320x180": plain_320x180,
+    "plain_literal": plain_literal,
+    "precision_1080p": precision_1080p,
+    "stress_2160p": stress_2160p,
+}
