@@ -180,8 +180,10 @@ enum {
 
 /* How the noise volumes are filtered. */
 enum {
-  PSC_FILTER_EXACT = 0, /* FP32 trilinear weights from point loads        */
-  PSC_FILTER_TEXTURE = 1 /* texture-unit trilinear (8-bit fixed weights)  */
+  PSC_FILTER_EXACT = 0,   /* FP32 trilinear weights from point loads      */
+  PSC_FILTER_TEXTURE = 1, /* texture-unit trilinear (8-bit fixed weights) */
+  PSC_FILTER_HYBRID = 2   /* texture unit for the light-march taps only,
+                             exact filtering for the primary density      */
 };
 
 /* Kernel schedule. */

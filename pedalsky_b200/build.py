@@ -25,6 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include")]
 CUDA_UNITS = {
     "march.cu": [],
+    "march_fast.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
 }

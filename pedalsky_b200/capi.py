@@ -21,7 +21,8 @@ PHASE_APPROX_MIE, PHASE_DUAL_LOBE_HG = 0, 1
 STORAGE_U8, STORAGE_F32, STORAGE_F16, STORAGE_BF16, STORAGE_FP8 = range(5)
 STORAGE_NAMES = {"u8": STORAGE_U8, "f32": STORAGE_F32, "f16": STORAGE_F16,
                  "bf16": STORAGE_BF16, "fp8": STORAGE_FP8}
-FILTER_EXACT, FILTER_TEXTURE = 0, 1
+FILTER_EXACT, FILTER_TEXTURE, FILTER_HYBRID = 0, 1, 2
+FILTER_NAMES = {"exact": FILTER_EXACT, "texture": FILTER_TEXTURE, "hybrid": FILTER_HYBRID}
 SCHED_PLAIN, SCHED_FAST = 0, 1
 NOISE_BASE, NOISE_DETAIL, NOISE_CURL, NOISE_BLUE = range(4)
 LUT_TRANSMITTANCE, LUT_MULTISCATTER, LUT_SKYVIEW, LUT_AERIAL = range(4)

@@ -40,6 +40,35 @@ __device__ __forceinline__ float4 lerp4(float4 a, float4 b, float t) {
                      lerpf(a.w, b.w, t));
 }
 
+// Packed FP32x2 arithmetic (sm_100 `fma.rn.f32x2` / `sub.rn.f32x2`): two
+// IEEE-rounded lanes per instruction, bit-identical to the scalar forms.
+__device__ __forceinline__ unsigned long long f2_bits(float2 v) {
+  return *reinterpret_cast<unsigned long long*>(&v);
+}
+__device__ __forceinline__ float2 bits_f2(unsigned long long b) {
+  return *reinterpret_cast<float2*>(&b);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return bits_f2(d);
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+  return bits_f2(d);
+}
+// fma(t, b - a, a) on two lanes
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 tt) {
+  return fma2(tt, sub2(b, a), a);
+}
+__device__ __forceinline__ float4 lerp4p(float4 a, float4 b, float t) {
+  const float2 tt = make_float2(t, t);
+  const float2 lo = lerp2(make_float2(a.x, a.y), make_float2(b.x, b.y), tt);
+  const float2 hi = lerp2(make_float2(a.z, a.w), make_float2(b.z, b.w), tt);
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+
 __device__ __forceinline__ int wrap_mod(int i, int n) {
   int m = i % n;
   return m < 0 ? m + n : m;

@@ -270,6 +270,31 @@ void build_uniforms(const psc_ctx* c, uint32_t width, uint32_t height, psc::Marc
   u.composite = c->opts.composite;
   u.debug_checks = c->opts.debug_checks;
 
+  u.base_texel_scale = 128.0f / u.base_scale;
+  u.detail_texel_scale = 32.0f / u.detail_scale;
+  u.curl_texel_scale = 128.0f / u.detail_scale;
+  u.inv_base_scale = 1.0f / u.base_scale;
+  u.inv_detail_scale = 1.0f / u.detail_scale;
+  u.inv_weather_scale = 1.0f / u.weather_scale;
+  u.curl_offset_scale = p.curl_strength * u.detail_scale;
+  u.sun_az = std::atan2(f.sun_direction[0], f.sun_direction[2]);
+  {
+    const double top = w.atmosphere_top_m, R = w.planet_radius_m;
+    u.big_h = (float)std::sqrt(std::max(top * top - R * R, 0.0));
+  }
+  u.inv_cos_sun = 1.0f / std::fmax(f.sun_direction[1], 0.05f);
+  u.b_half = p.multi_scatter_b == 0.5f ? 1u : 0u;
+  {
+    float a = 1.0f, b = 1.0f, cc = 1.0f;
+    for (int n = 0; n < 8; ++n) {
+      u.apow[n] = a;
+      u.bpow[n] = b;
+      u.cpow[n] = cc;
+      a *= p.multi_scatter_a;
+      b *= p.multi_scatter_b;
+      cc *= p.multi_scatter_c;
+    }
+  }
   // diurnal_modulation (cloud_density_common.wgsl:204-219), per layer type
   const float bell = smoothstep_h(-0.1f, 0.4f, f.sun_direction[1]);
   for (uint32_t i = 0; i < 8; ++i) {
@@ -354,12 +379,19 @@ void destroy_textures(psc_ctx* c) {
   c->tex_dirty = true;
 }
 
-int make_volume_texture(const uint8_t* d_src, uint32_t n, cudaArray_t* arr, cudaTextureObject_t* tex) {
-  const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<uchar4>();
+// 3D texture over an RGBA8 (read as normalised float) or RGBA16F volume
+// (read as stored; the F16 volume holds the byte values 0..255), linear
+// filtering, repeat addressing, normalised coordinates: the noise sampler of
+// crates/ps-clouds/src/noise.rs:178-187.
+int make_volume_texture(const void* d_src, uint32_t n, bool half4, cudaArray_t* arr,
+                        cudaTextureObject_t* tex) {
+  const cudaChannelFormatDesc fmt =
+      half4 ? cudaCreateChannelDescHalf4() : cudaCreateChannelDesc<uchar4>();
+  const size_t texel = half4 ? 8 : 4;
   const cudaExtent ext = make_cudaExtent(n, n, n);
   PSC_CUDA(cudaMalloc3DArray(arr, &fmt, ext), "cudaMalloc3DArray");
   cudaMemcpy3DParms cp{};
-  cp.srcPtr = make_cudaPitchedPtr((void*)d_src, n * 4, n, n);
+  cp.srcPtr = make_cudaPitchedPtr((void*)d_src, n * texel, n, n);
   cp.dstArray = *arr;
   cp.extent = ext;
   cp.kind = cudaMemcpyDeviceToDevice;
@@ -370,18 +402,21 @@ int make_volume_texture(const uint8_t* d_src, uint32_t n, cudaArray_t* arr, cuda
   cudaTextureDesc td{};
   td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeWrap;
   td.filterMode = cudaFilterModeLinear;
-  td.readMode = cudaReadModeNormalizedFloat;
+  td.readMode = half4 ? cudaReadModeElementType : cudaReadModeNormalizedFloat;
   td.normalizedCoords = 1;
   PSC_CUDA(cudaCreateTextureObject(tex, &rd, &td, nullptr), "cudaCreateTextureObject");
   return PSC_OK;
 }
 
 int build_textures(psc_ctx* c) {
-  if (c->opts.filter != PSC_FILTER_TEXTURE || !c->tex_dirty) return PSC_OK;
+  if (c->opts.filter == PSC_FILTER_EXACT || !c->tex_dirty) return PSC_OK;
   destroy_textures(c);
-  int rc = make_volume_texture(c->d_base_u8, 128, &c->arr_base, &c->tex_base);
+  const bool h4 = c->opts.storage == PSC_STORAGE_F16;
+  int rc = make_volume_texture(h4 ? c->d_base_store : c->d_base_u8, 128, h4, &c->arr_base,
+                               &c->tex_base);
   if (rc) return rc;
-  rc = make_volume_texture(c->d_detail_u8, 32, &c->arr_detail, &c->tex_detail);
+  rc = make_volume_texture(h4 ? c->d_detail_store : c->d_detail_u8, 32, h4, &c->arr_detail,
+                           &c->tex_detail);
   if (rc) return rc;
   c->tex_dirty = false;
   return PSC_OK;
@@ -830,12 +865,19 @@ int psc_set_options(psc_ctx* c, const PscMarchOptions* o) {
   if (!c || !o) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
   if (o->phase_mode > PSC_PHASE_DUAL_LOBE_HG) return fail(PSC_ERR_INVALID_ARGUMENT, "bad phase_mode");
   if (o->storage > PSC_STORAGE_FP8) return fail(PSC_ERR_INVALID_ARGUMENT, "bad storage");
-  if (o->filter > PSC_FILTER_TEXTURE) return fail(PSC_ERR_INVALID_ARGUMENT, "bad filter");
+  if (o->filter > PSC_FILTER_HYBRID) return fail(PSC_ERR_INVALID_ARGUMENT, "bad filter");
+  if (o->filter == PSC_FILTER_HYBRID && o->schedule != PSC_SCHED_FAST)
+    return fail(PSC_ERR_UNSUPPORTED, "the hybrid filter is implemented by the FAST schedule only");
+  if (o->filter == PSC_FILTER_HYBRID && o->storage != PSC_STORAGE_U8 && o->storage != PSC_STORAGE_F16)
+    return fail(PSC_ERR_UNSUPPORTED, "the hybrid filter reads RGBA8 or RGBA16F volumes only");
   if (o->schedule > PSC_SCHED_FAST) return fail(PSC_ERR_INVALID_ARGUMENT, "bad schedule");
-  if (o->filter == PSC_FILTER_TEXTURE && o->storage != PSC_STORAGE_U8)
-    return fail(PSC_ERR_UNSUPPORTED, "texture filtering reads the RGBA8 volumes (storage U8 only)");
+  if (o->filter == PSC_FILTER_TEXTURE && o->storage != PSC_STORAGE_U8 && o->storage != PSC_STORAGE_F16)
+    return fail(PSC_ERR_UNSUPPORTED, "texture filtering reads RGBA8 or RGBA16F volumes only");
+  if (o->filter == PSC_FILTER_TEXTURE && o->storage == PSC_STORAGE_F16 && o->schedule != PSC_SCHED_FAST)
+    return fail(PSC_ERR_UNSUPPORTED, "F16 texture volumes are read by the FAST schedule only");
   const float hv[] = {o->hg_g_forward, o->hg_g_backward, o->hg_blend};
   if (!all_finite(hv, 3)) return fail(PSC_ERR_NOT_FINITE, "non-finite HG lobe");
+  if (o->storage != c->opts.storage || o->filter != c->opts.filter) c->tex_dirty = true;
   c->opts = *o;
   return PSC_OK;
 }
@@ -1015,7 +1057,7 @@ int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
   if (rc) return rc;
   rc = build_textures(c);
   if (rc) return rc;
-  if (c->opts.filter == PSC_FILTER_TEXTURE && (!c->tex_base || !c->tex_detail))
+  if (c->opts.filter != PSC_FILTER_EXACT && (!c->tex_base || !c->tex_detail))
     return fail(PSC_ERR_MISSING_INPUT, "texture objects for the noise volumes were not created");
   for (uint32_t i = 0; i < n; ++i) {
     const PscView& v = views[i];
@@ -1032,7 +1074,9 @@ int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
     build_uniforms(c, v.width, v.height, u);
     psc::ViewDev vd{v.width, v.height, v.depth, reinterpret_cast<float4*>(v.out_luminance),
                     reinterpret_cast<float4*>(v.out_transmittance), reinterpret_cast<float4*>(v.hdr)};
-    rc = psc::launch_march(u, vd, c->opts, s);
+    rc = PSC_ERR_UNSUPPORTED;
+    if (c->opts.schedule == PSC_SCHED_FAST) rc = psc::launch_march_fast(u, vd, c->opts, s);
+    if (rc == PSC_ERR_UNSUPPORTED) rc = psc::launch_march(u, vd, c->opts, s);
     if (rc) return fail(rc, "march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     ++c->launches;
   }

@@ -77,6 +77,18 @@ struct MarchUniforms {
   uint32_t kahan;
   uint32_t composite;
   uint32_t debug_checks;
+  // derived per frame, for the FAST schedule
+  float base_texel_scale;    // 128 / base_scale  (texel units per metre)
+  float detail_texel_scale;  // 32 / detail_scale
+  float curl_texel_scale;    // 128 / detail_scale
+  float inv_base_scale, inv_detail_scale, inv_weather_scale;
+  float curl_offset_scale;   // curl_strength * detail_scale
+  float sun_az;              // atan2(sun.x, sun.z)
+  float top_minus_r_sq_unused;
+  float big_h;               // sqrt(atmo_top^2 - planet_r^2)
+  float inv_cos_sun;         // 1 / max(sun.y, 0.05)
+  uint32_t b_half;           // multi_scatter_b == 0.5 exactly
+  float apow[8], bpow[8], cpow[8];  // a^n, b^n, c^n
   LayerConst layers[8];
 
   // inputs (device pointers)
@@ -108,6 +120,10 @@ struct ViewDev {
 // Launchers (march.cu).
 int launch_march(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
                  cudaStream_t stream);
+// FAST schedule (march_fast.cu); returns PSC_ERR_UNSUPPORTED for settings it
+// does not cover (more than 4 octaves), which the caller serves with PLAIN.
+int launch_march_fast(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
+                      cudaStream_t stream);
 int launch_composite(const float4* l, const float4* t, float4* hdr, uint32_t n,
                      cudaStream_t stream);
 // Noise bakes (noise_bake.cu), synchronous on `stream`.

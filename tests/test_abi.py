@@ -189,10 +189,16 @@ def test_options_validation():
         o.storage = 9
         with pytest.raises(PscError):
             call("psc_set_options", c, C.byref(o))
-        o.storage, o.filter = capi.STORAGE_F16, capi.FILTER_TEXTURE
+        o.storage, o.filter = capi.STORAGE_BF16, capi.FILTER_TEXTURE
         with pytest.raises(PscError) as e:
             call("psc_set_options", c, C.byref(o))
         assert e.value.code == -8
+        o.storage, o.schedule = capi.STORAGE_F16, capi.SCHED_PLAIN
+        with pytest.raises(PscError) as e:
+            call("psc_set_options", c, C.byref(o))
+        assert e.value.code == -8
+        o.schedule = capi.SCHED_FAST
+        call("psc_set_options", c, C.byref(o))
     finally:
         capi.lib().psc_destroy(c)
 

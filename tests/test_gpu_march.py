@@ -86,11 +86,16 @@ def test_lut_bake_matches_oracle(oracle):
         sub.close()
 
 
-def test_plain_u8_matches_fp64_oracle(c1, oracle_noise):
+SCHEDULES = {"plain": capi.SCHED_PLAIN, "fast": capi.SCHED_FAST}
+
+
+@pytest.mark.parametrize("sched", sorted(SCHEDULES))
+def test_u8_matches_fp64_oracle(c1, oracle_noise, sched):
     s, luts, ref = c1
-    L, T, hdr = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
+    s2 = scenes.plain_320x180(schedule=SCHEDULES[sched])
+    L, T, hdr = _gpu.render(s2, oracle_noise, luts, composite_bg=s.background)
     assert np.isfinite(L).all() and np.isfinite(T).all()
-    _check("plain_320x180/u8/exact", hdr, ref)
+    _check(f"plain_320x180/{sched}/u8/exact", hdr, ref)
 
 
 def test_gpu_baked_inputs_match_oracle_inputs(c1, oracle_noise):
@@ -100,65 +105,92 @@ def test_gpu_baked_inputs_match_oracle_inputs(c1, oracle_noise):
     _check("plain_320x180/gpu-noise", hdr, ref)
 
 
+@pytest.mark.parametrize("sched", sorted(SCHEDULES))
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
-def test_exact_storage_forms(c1, oracle_noise, storage):
+def test_exact_storage_forms(c1, oracle_noise, storage, sched):
     s, luts, ref = c1
-    s2 = scenes.plain_320x180(storage=capi.STORAGE_NAMES[storage])
+    s2 = scenes.plain_320x180(storage=capi.STORAGE_NAMES[storage], schedule=SCHEDULES[sched])
     L, T, hdr = _gpu.render(s2, oracle_noise, luts, composite_bg=s.background)
-    _check(f"plain_320x180/{storage}/exact", hdr, ref)
+    _check(f"plain_320x180/{sched}/{storage}/exact", hdr, ref)
 
 
-def test_fp8_storage_reports_error(c1, oracle_noise):
+@pytest.mark.parametrize("sched", sorted(SCHEDULES))
+def test_fp8_storage_reports_error(c1, oracle_noise, sched):
     s, luts, ref = c1
-    s2 = scenes.plain_320x180(storage=capi.STORAGE_FP8)
+    s2 = scenes.plain_320x180(storage=capi.STORAGE_FP8, schedule=SCHEDULES[sched])
     L, T, hdr = _gpu.render(s2, oracle_noise, luts, composite_bg=s.background)
     st = rel_stats(hdr, ref)
     st["ssim"] = ssim(tonemap(hdr), tonemap(ref))
-    _report("plain_320x180/fp8/exact", st)
+    _report(f"plain_320x180/{sched}/fp8/exact", st)
     assert np.isfinite(hdr).all()
 
 
-def test_texture_filter_path(c1, oracle_noise):
+@pytest.mark.parametrize("sched,storage,filt", [
+    ("plain", "u8", "texture"), ("fast", "u8", "texture"), ("fast", "f16", "texture"),
+    ("fast", "u8", "hybrid"), ("fast", "f16", "hybrid")])
+def test_texture_filter_path(c1, oracle_noise, sched, storage, filt):
     s, luts, ref = c1
-    s2 = scenes.plain_320x180(filt=capi.FILTER_TEXTURE)
+    s2 = scenes.plain_320x180(filt=capi.FILTER_NAMES[filt], schedule=SCHEDULES[sched],
+                              storage=capi.STORAGE_NAMES[storage])
     L, T, hdr = _gpu.render(s2, oracle_noise, luts, composite_bg=s.background)
     st = rel_stats(hdr, ref)
     st["ssim"] = ssim(tonemap(hdr), tonemap(ref))
-    _report("plain_320x180/u8/texture", st)
+    _report(f"plain_320x180/{sched}/{storage}/{filt}", st)
     # texture units interpolate with 8-bit fixed-point weights; the error is
     # reported, and bounded loosely here
     assert st["ssim"] >= 0.99 and st["mean"] < 5e-2 and np.isfinite(hdr).all()
 
 
-def test_fused_composite_equals_two_pass(c1, oracle_noise):
+@pytest.mark.parametrize("sched", sorted(SCHEDULES))
+def test_fused_composite_equals_two_pass(c1, oracle_noise, sched):
     s, luts, ref = c1
-    _, _, two = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
-    _, _, fused = _gpu.render(s, oracle_noise, luts, composite_bg=s.background, fused=True)
-    assert np.array_equal(two, fused)
+    s2 = scenes.plain_320x180(schedule=SCHEDULES[sched])
+    _, _, two = _gpu.render(s2, oracle_noise, luts, composite_bg=s.background)
+    _, _, fused = _gpu.render(s2, oracle_noise, luts, composite_bg=s.background, fused=True)
+    assert np.allclose(two, fused, rtol=2e-7, atol=0)
 
 
-def test_approx_mie_phase(oracle, oracle_noise):
-    s = scenes.plain_320x180(phase=capi.PHASE_APPROX_MIE)
+@pytest.mark.parametrize("sched", sorted(SCHEDULES))
+def test_approx_mie_phase(oracle, oracle_noise, sched):
+    s = scenes.plain_320x180(phase=capi.PHASE_APPROX_MIE, schedule=SCHEDULES[sched])
     luts = oracle.bake_luts(s.frame, s.world)
     L, T = oracle.render(s, oracle_noise, luts)
     _, _, hdr = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
-    _check("plain_320x180/approx-mie", hdr, composite(L, T, s.background))
+    _check(f"plain_320x180/{sched}/approx-mie", hdr, composite(L, T, s.background))
 
 
-def test_three_layer_precision_scene(oracle, oracle_noise):
+@pytest.fixture(scope="module")
+def precision_ref(oracle, oracle_noise):
     s = scenes.precision_1080p(480, 270)
     luts = oracle.bake_luts(s.frame, s.world)
     L, T = oracle.render(s, oracle_noise, luts)
+    return luts, composite(L, T, s.background)
+
+
+@pytest.mark.parametrize("sched,storage,filt", [
+    ("plain", "u8", "exact"), ("plain", "f32", "exact"), ("fast", "f16", "exact"),
+    ("fast", "u8", "exact"), ("fast", "f16", "hybrid"), ("fast", "f16", "texture")])
+def test_three_layer_precision_scene(precision_ref, oracle_noise, sched, storage, filt):
+    luts, ref = precision_ref
+    s = scenes.precision_1080p(480, 270, schedule=SCHEDULES[sched],
+                               storage=capi.STORAGE_NAMES[storage], filt=capi.FILTER_NAMES[filt])
     _, _, hdr = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
-    _check("precision_480x270", hdr, composite(L, T, s.background))
+    if filt == "texture":
+        # 8-bit texture-unit weights sit at the edge of the 1e-3 bar; recorded,
+        # bounded at 2e-3 here (the exact and hybrid forms carry the bar)
+        _check(f"precision_480x270/{sched}/{storage}/{filt}", hdr, ref, p999=2e-3, frac=3e-3)
+        return
+    _check(f"precision_480x270/{sched}/{storage}/{filt}", hdr, ref)
 
 
 def test_literal_weather_map_scene(oracle, oracle_noise):
     s = scenes.plain_literal()
     luts = oracle.bake_luts(s.frame, s.world)
     L, T = oracle.render(s, oracle_noise, luts)
-    _, _, hdr = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
-    _check("plain_literal", hdr, composite(L, T, s.background))
+    for sched in sorted(SCHEDULES):
+        s.options.schedule = SCHEDULES[sched]
+        _, _, hdr = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
+        _check(f"plain_literal/{sched}", hdr, composite(L, T, s.background))
 
 
 def _variant(name, mutate, oracle, oracle_noise, size=(96, 54), **check):
@@ -166,8 +198,13 @@ def _variant(name, mutate, oracle, oracle_noise, size=(96, 54), **check):
     mutate(s)
     luts = oracle.bake_luts(s.frame, s.world)
     L, T = oracle.render(s, oracle_noise, luts)
-    _, _, hdr = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
-    return _check(name, hdr, composite(L, T, s.background), **check)
+    ref = composite(L, T, s.background)
+    out = None
+    for sched in sorted(SCHEDULES):
+        s.options.schedule = SCHEDULES[sched]
+        _, _, hdr = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
+        out = _check(f"{name}/{sched}", hdr, ref, **check)
+    return out
 
 
 def _cam(s, y, pitch=10.0, sun_alt=35.0, **kw):
