@@ -211,9 +211,13 @@ typedef struct PscMarchOptions {
   uint32_t _reserved[4];
 } PscMarchOptions;
 
-/* One view to render.  `depth` is an optional D32F reverse-Z buffer
- * (width*height floats, device, 0 = sky); NULL means "sky everywhere",
- * matching a headless render with no opaque geometry. */
+/* One view to render: a width x height rectangle of pixels.  By default
+ * the rectangle is the whole image; a non-zero `viewport_w/h` makes it the
+ * sub-rectangle at (`x_offset`, `y_offset`) of a viewport_w x viewport_h
+ * image (row bands of one frame rendered on several GPUs).  `depth` is an
+ * optional D32F reverse-Z buffer of the rectangle (width*height floats,
+ * device, 0 = sky); NULL means "sky everywhere", a headless render with no
+ * opaque geometry.  Outputs are indexed within the rectangle. */
 typedef struct PscView {
   uint32_t width;
   uint32_t height;
@@ -222,6 +226,10 @@ typedef struct PscView {
   float* out_transmittance;    /* device, width*height*4 floats (RGBA)   */
   float* hdr;                  /* device, RGBA, read-modify-write when
                                   options.composite = 1; else unused     */
+  uint32_t viewport_w;         /* 0 = width                              */
+  uint32_t viewport_h;         /* 0 = height                             */
+  uint32_t x_offset;
+  uint32_t y_offset;
 } PscView;
 
 /* Noise volume kinds for upload/download. */

@@ -104,6 +104,7 @@ class View(C.Structure):
     _fields_ = [
         ("width", u32), ("height", u32), ("depth", C.c_void_p),
         ("out_luminance", C.c_void_p), ("out_transmittance", C.c_void_p), ("hdr", C.c_void_p),
+        ("viewport_w", u32), ("viewport_h", u32), ("x_offset", u32), ("y_offset", u32),
     ]
 
 

@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant_
   const float sun_az = atan2f(u.sun[0], u.sun[2]);
 
   // blue-noise jitter (cloud_march.wgsl:745-756)
-  uint32_t sx = px & 63u, sy = py & 63u;
+  uint32_t sx = (px + v.x_off) & 63u, sy = (py + v.y_off) & 63u;
   if (u.temporal_jitter) {
     const uint32_t ph = u.frame_index & 15u;
     sx = (sx ^ ((ph * 11u + 7u) & 63u)) & 63u;
@@ -327,7 +327,8 @@ __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant_
   if (opacity > 1e-4f) {
     const float ds = fmaxf(t_cloud, 50.0f);
     const float az = clamp01(logf(ds / 50.0f) / logf(100000.0f / 50.0f));
-    const float4 ap = lut_ap(u.lut_ap, ((float)px + 0.5f) / u.vp_w, ((float)py + 0.5f) / u.vp_h, az);
+    const float4 ap = lut_ap(u.lut_ap, ((float)(px + v.x_off) + 0.5f) / u.vp_w,
+                             ((float)(py + v.y_off) + 0.5f) / u.vp_h, az);
     Or = Lr * ap.w + ap.x * opacity;
     Og = Lg * ap.w + ap.y * opacity;
     Ob = Lb * ap.w + ap.z * opacity;

@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_march_fast(const __grid_constan
   const float fwd_gain =
       u.forward_bias > 0.0f ? 1.0f + u.forward_bias * smoothstepf(0.0f, 1.0f, fmaxf(cos_theta, 0.0f))
                             : 1.0f;
-  uint32_t sx = px & 63u, sy = py & 63u;
+  uint32_t sx = (px + v.x_off) & 63u, sy = (py + v.y_off) & 63u;
   if (u.temporal_jitter) {
     const uint32_t ph = u.frame_index & 15u;
     sx = (sx ^ ((ph * 11u + 7u) & 63u)) & 63u;
@@ -532,7 +532,8 @@ __global__ void __launch_bounds__(kThreads, 6) k_march_fast(const __grid_constan
     const float t_cloud = __fdividef(tw, fmaxf(twn, 1e-6f));
     const float ds = fmaxf(t_cloud, 50.0f);
     const float az = clamp01(__logf(ds * (1.0f / 50.0f)) * (1.0f / 7.6009024595f));  // ln 2000
-    const float4 ap = lut_ap(u.lut_ap, ((float)px + 0.5f) / u.vp_w, ((float)py + 0.5f) / u.vp_h, az);
+    const float4 ap = lut_ap(u.lut_ap, ((float)(px + v.x_off) + 0.5f) / u.vp_w,
+                             ((float)(py + v.y_off) + 0.5f) / u.vp_h, az);
     Or = fmaf(Lr, ap.w, ap.x * opacity);
     Og = fmaf(Lg, ap.w, ap.y * opacity);
     Ob = fmaf(Lb, ap.w, ap.z * opacity);

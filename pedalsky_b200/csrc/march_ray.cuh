@@ -38,7 +38,7 @@ __device__ __forceinline__ bool sphere_hit(const double oc[3], const double d[3]
 
 __device__ void setup_ray(const MarchUniforms& u, const ViewDev& v, uint32_t px, uint32_t py,
                           RaySetup& rs) {
-  const double fx = (double)px + 0.5, fy = (double)py + 0.5;
+  const double fx = (double)(px + v.x_off) + 0.5, fy = (double)(py + v.y_off) + 0.5;
   const double nx = (fx / (double)u.vp_w) * 2.0 - 1.0;
   const double ny = 1.0 - (fy / (double)u.vp_h) * 2.0;
   double nh[4];

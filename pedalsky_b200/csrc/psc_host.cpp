@@ -1063,6 +1063,11 @@ int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
     const PscView& v = views[i];
     if (!v.width || !v.height || v.width > 32768 || v.height > 32768)
       return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: size %ux%u out of range", i, v.width, v.height);
+    const uint32_t vw = v.viewport_w ? v.viewport_w : v.width, vh = v.viewport_h ? v.viewport_h : v.height;
+    if ((!v.viewport_w && v.x_offset) || (!v.viewport_h && v.y_offset) || vw > 32768 || vh > 32768 ||
+        (uint64_t)v.x_offset + v.width > vw || (uint64_t)v.y_offset + v.height > vh)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: rectangle %ux%u at (%u,%u) exceeds viewport %ux%u",
+                  i, v.width, v.height, v.x_offset, v.y_offset, vw, vh);
     if (!v.out_luminance && !v.out_transmittance && !(c->opts.composite && v.hdr))
       return fail(PSC_ERR_INVALID_ARGUMENT, "view %u has no output buffer", i);
     if (c->opts.composite && !v.hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: composite needs hdr", i);
@@ -1071,8 +1076,10 @@ int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
   psc::MarchUniforms u;
   for (uint32_t i = 0; i < n; ++i) {
     const PscView& v = views[i];
-    build_uniforms(c, v.width, v.height, u);
-    psc::ViewDev vd{v.width, v.height, v.depth, reinterpret_cast<float4*>(v.out_luminance),
+    const uint32_t vw = v.viewport_w ? v.viewport_w : v.width, vh = v.viewport_h ? v.viewport_h : v.height;
+    build_uniforms(c, vw, vh, u);
+    psc::ViewDev vd{v.width, v.height, v.x_offset, v.y_offset, v.depth,
+                    reinterpret_cast<float4*>(v.out_luminance),
                     reinterpret_cast<float4*>(v.out_transmittance), reinterpret_cast<float4*>(v.hdr)};
     rc = PSC_ERR_UNSUPPORTED;
     if (c->opts.schedule == PSC_SCHED_FAST) rc = psc::launch_march_fast(u, vd, c->opts, s);

@@ -111,6 +111,7 @@ struct MarchUniforms {
 // One view of a launch.
 struct ViewDev {
   uint32_t width, height;
+  uint32_t x_off, y_off;   // rectangle origin in the viewport
   const float* depth;
   float4* out_l;
   float4* out_t;

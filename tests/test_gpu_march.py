@@ -294,3 +294,39 @@ def test_render_errors_are_reported(oracle_noise):
             sub.dispatch_pass(99, None)
     finally:
         sub.close()
+
+
+@pytest.mark.parametrize("sched", sorted(SCHEDULES))
+def test_row_bands_reassemble_the_full_frame(oracle_noise, sched):
+    """A frame split into row bands (the multi-GPU split of one large view)
+    is bit-identical to the frame rendered whole."""
+    import ctypes as C
+    from pedalsky_b200 import sharding
+    from pedalsky_b200.subsystem import subsystem_for_scene
+    torch = _gpu.torch_cuda()
+    s = scenes.precision_1080p(160, 90, schedule=SCHEDULES[sched])
+    from oracle import pyoracle
+    luts = pyoracle.bake_luts(s.frame, s.world)
+    whole_L, whole_T = _gpu.render(s, oracle_noise, luts)
+    sub = subsystem_for_scene(s, luts=luts, noise=oracle_noise)
+    dev = torch.device("cuda", 0)
+    depth = torch.from_numpy(s.depth).to(dev)
+    out_L = np.zeros_like(whole_L)
+    out_T = np.zeros_like(whole_T)
+    for band in sharding.row_bands(s.height, 3, np.linspace(3, 1, s.height)):
+        h = band.y1 - band.y0
+        L = torch.zeros((h, s.width, 4), device=dev)
+        T = torch.zeros((h, s.width, 4), device=dev)
+        d = depth[band.y0:band.y1].contiguous()
+        v = capi.View(s.width, h, d.data_ptr(), L.data_ptr(), T.data_ptr(), None,
+                      s.width, s.height, 0, band.y0)
+        call("psc_render", sub.handle, C.byref(v), 1, None)
+        torch.cuda.synchronize()
+        out_L[band.y0:band.y1] = L.cpu().numpy()
+        out_T[band.y0:band.y1] = T.cpu().numpy()
+    bad = capi.View(s.width, 10, None, L.data_ptr(), T.data_ptr(), None, s.width, s.height, 0,
+                    s.height - 5)
+    with pytest.raises(PscError):
+        call("psc_render", sub.handle, C.byref(bad), 1, None)
+    sub.close()
+    assert np.array_equal(out_L, whole_L) and np.array_equal(out_T, whole_T)
