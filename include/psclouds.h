@@ -394,10 +394,60 @@ int psc_composite(const float* luminance, const float* transmittance,
 /* Number of march-kernel launches issued by this context so far. */
 int psc_launch_count(psc_ctx* ctx, uint64_t* out);
 
+/* --------------------------------------------------------- batching */
+
+#define PSC_MAX_BATCH_VIEWS 256u
+
+/* One view of a batch: its own scene (CloudParams, layers, frame uniforms,
+ * i.e. camera and sun) and its own outputs.  World uniforms, noise, weather,
+ * wind and the transmittance/multi-scatter LUTs are the context's.  The
+ * sky-view and aerial-perspective LUTs are baked per view.  New in this
+ * library: the reference draws one view per pass
+ * (crates/ps-clouds/src/lib.rs:714-724). */
+typedef struct PscBatchView {
+  PscFrameUniformsGpu frame;
+  PscCloudParamsGpu params;     /* cloud_layer_count is taken from n_layers */
+  PscCloudLayerGpu layers[8];
+  uint32_t n_layers;
+  uint32_t width;
+  uint32_t height;
+  uint32_t _pad0;
+  const float* depth;           /* device, nullable                        */
+  float* out_luminance;         /* device, nullable                        */
+  float* out_transmittance;     /* device, nullable                        */
+  float* hdr;                   /* device; composited when options.composite */
+} PscBatchView;
+
+/* Launch shape of the persistent batched kernel. */
+typedef struct PscBatchTuning {
+  uint32_t threads;    /* CTA size: 64, 128 or 256                          */
+  uint32_t tile_w;     /* tile width in pixels, a multiple of 8 dividing
+                          threads/4; tile height = threads/32/(tile_w/8)*4 */
+  uint32_t use_graph;  /* 1: capture the batch once as a CUDA graph and
+                          relaunch it while the batch shape is unchanged    */
+  uint32_t _reserved;
+} PscBatchTuning;
+
+int psc_set_batch_tuning(psc_ctx* ctx, const PscBatchTuning* tuning);
+int psc_get_batch_tuning(psc_ctx* ctx, PscBatchTuning* out);
+
+/* March every view of the batch in one persistent kernel (FAST schedule;
+ * storage/filter from the context's options: F16, U8 or F32 exact, F16 or
+ * U8 hybrid, U8 texture).  Requires the transmittance and multi-scatter LUTs
+ * (psc_bake_luts or psc_upload_lut).  Enqueued on `stream`. */
+int psc_render_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, void* stream);
+
+/* Time every candidate launch shape on this batch (`reps` timed runs each,
+ * after one warm-up), keep the fastest in the context and return it with
+ * its median time in milliseconds.  Synchronous. */
+int psc_autotune_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, uint32_t reps,
+                       PscBatchTuning* best, float* best_ms, void* stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 
 static_assert(sizeof(PscCloudParamsGpu) == 112, "CloudParamsGpu is 112 B");
+static_assert(sizeof(PscBatchView) == 448 + 112 + 384 + 16 + 32, "PscBatchView layout");
 static_assert(sizeof(PscCloudLayerGpu) == 48, "CloudLayerGpu is 48 B");
 static_assert(sizeof(PscFrameUniformsGpu) == 448, "FrameUniformsGpu is 448 B");
 static_assert(sizeof(PscWorldUniformsGpu) == 144, "WorldUniformsGpu is 144 B");

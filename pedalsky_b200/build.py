@@ -26,6 +26,7 @@ NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", st
 CUDA_UNITS = {
     "march.cu": [],
     "march_fast.cu": ["-prec-div=false", "-prec-sqrt=false"],
+    "march_batch.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
 }
@@ -75,21 +76,24 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     BUILD_DIR.mkdir(exist_ok=True)
     nvcc, cxx = _nvcc(), _host_cxx()
     env_ccbin = ["-ccbin", cxx]
-    objs = []
+    cmds, objs = [], []
     for unit, extra in CUDA_UNITS.items():
         obj = BUILD_DIR / (unit + ".o")
         cmd = [nvcc, *env_ccbin, *ARCH, *NVCC_COMMON, *extra, "-c", str(CSRC / unit), "-o", str(obj)]
         if ptxas_info:
             cmd += ["-Xptxas", "-v"]
-        _run(cmd, verbose or ptxas_info)
+        cmds.append(cmd)
         objs.append(obj)
     cuda_inc = Path(nvcc).resolve().parent.parent / "include"
     for unit in CXX_UNITS:
         obj = BUILD_DIR / (unit + ".o")
-        cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-I", str(ROOT / "include"),
-               "-I", str(cuda_inc), "-c", str(CSRC / unit), "-o", str(obj)]
-        _run(cmd, verbose)
+        cmds.append([cxx, "-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-I", str(ROOT / "include"),
+                     "-I", str(cuda_inc), "-c", str(CSRC / unit), "-o", str(obj)])
         objs.append(obj)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(_run, cmd, verbose or ptxas_info) for cmd in cmds]:
+            f.result()
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc, *env_ccbin, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static"]
     _run(cmd, verbose)

@@ -125,6 +125,20 @@ class FlyCamera(C.Structure):
     ]
 
 
+class BatchView(C.Structure):
+    """`PscBatchView`: one view of a batch with its own scene and outputs."""
+    _fields_ = [
+        ("frame", FrameUniformsGpu), ("params", CloudParamsGpu), ("layers", CloudLayerGpu * 8),
+        ("n_layers", u32), ("width", u32), ("height", u32), ("_pad0", u32),
+        ("depth", C.c_void_p), ("out_luminance", C.c_void_p), ("out_transmittance", C.c_void_p),
+        ("hdr", C.c_void_p),
+    ]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("threads", u32), ("tile_w", u32), ("use_graph", u32), ("_reserved", u32)]
+
+
 class PscError(RuntimeError):
     def __init__(self, code: int, func: str, msg: str):
         super().__init__(f"{func}: {PSC_ERR.get(code, code)} ({code}): {msg}")
@@ -166,6 +180,10 @@ _PROTOS = {
     "psc_render": [_vp, P(View), u32, _vp],
     "psc_composite": [_vp, _vp, _vp, u32, u32, _vp],
     "psc_launch_count": [_vp, P(C.c_uint64)],
+    "psc_set_batch_tuning": [_vp, P(BatchTuning)],
+    "psc_get_batch_tuning": [_vp, P(BatchTuning)],
+    "psc_render_batch": [_vp, P(BatchView), u32, _vp],
+    "psc_autotune_batch": [_vp, P(BatchView), u32, u32, P(BatchTuning), P(C.c_float), _vp],
 }
 _RESTYPES = {
     "psc_last_error": C.c_char_p, "psc_abi_version": u32, "psc_sizeof_params": C.c_size_t,

@@ -311,7 +311,125 @@ __global__ void k_aerial(const Atmo A, const FrameLite F, const uint16_t* T, con
   store_h4(out + ((gz * 32 + gy) * 32 + gx) * 4, lum, tl);
 }
 
+__device__ __forceinline__ float4 f16_rounded(float3 v, float a) {
+  return make_float4(__half2float(__float2half_rn(v.x)), __half2float(__float2half_rn(v.y)),
+                     __half2float(__float2half_rn(v.z)), __half2float(__float2half_rn(a)));
+}
+
+// Per-view sky-view LUTs for a batch (blockIdx.z = view).  Output float4
+// holding the RGBA16F-rounded values the single-view path reads.
+__global__ void k_skyview_batch(const Atmo A, const FrameLite* __restrict__ frames,
+                                const uint16_t* T, const uint16_t* MS, float4* out) {
+  const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (gx >= 192 || gy >= 108) return;
+  const FrameLite& F = frames[blockIdx.z];
+  const float u = ((float)gx + 0.5f) / 192.0f, v = ((float)gy + 0.5f) / 108.0f;
+  float3 p = f3(F.cam.x, F.cam.y + A.R, F.cam.z);
+  float r = len3(p);
+  if (r < A.R + 1.0f) {
+    p = p * ((A.R + 1.0f) / r);
+    r = A.R + 1.0f;
+  }
+  const float zha = kPi - asinf(clampf(A.R / r, 0.0f, 1.0f));
+  float vza;
+  if (v < 0.5f) {
+    const float c = v * 2.0f;
+    vza = c * c * zha;
+  } else {
+    const float c = (v - 0.5f) * 2.0f;
+    vza = zha + c * c * (kPi - zha);
+  }
+  const float az = atan2f(F.sun.x, F.sun.z) + u * 2.0f * kPi;
+  const float3 vd = f3(sinf(vza) * sinf(az), cosf(vza), sinf(vza) * cosf(az));
+  const float ct = dot3(vd, F.sun);
+  const float tmax = dist_boundary(A, p, vd);
+  float4* o = out + (size_t)blockIdx.z * (192 * 108) + gy * 192 + gx;
+  if (tmax <= 0.0f) {
+    *o = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    return;
+  }
+  float3 tr;
+  float3 lum = inscatter(A, T, MS, p, r, vd, F.sun, phase_r(ct), phase_m(ct, A.mie_g), tmax / 32.0f,
+                         32, false, f3(1, 1, 1), tr);
+  float tp0, tp1;
+  if (sphere0(p, vd, A.R, tp0, tp1) && tp0 > 0.0f) {
+    const float3 pg = p + vd * tp0;
+    const float3 ng = pg * (1.0f / len3(pg));
+    const float3 vis = trans_lut(A, T, pg, F.sun);
+    const float ndl = fmaxf(dot3(ng, F.sun), 0.0f);
+    lum = lum + tr * (A.albedo * (1.0f / 3.14159265f) * ndl * vis);
+  }
+  *o = f16_rounded(lum, 1.0f);
+}
+
+// Per-view aerial-perspective LUTs (blockIdx.z = view * 16 + z block).
+__global__ void k_aerial_batch(const Atmo A, const FrameLite* __restrict__ frames, const uint16_t* T,
+                               const uint16_t* MS, float4* out) {
+  const int view = blockIdx.z / 16;
+  const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int gz = (blockIdx.z % 16) * blockDim.z + threadIdx.z;
+  if (gx >= 32 || gy >= 32 || gz >= 64) return;
+  const FrameLite& F = frames[view];
+  const float nx = (((float)gx + 0.5f) / 32.0f) * 2.0f - 1.0f;
+  const float ny = -((((float)gy + 0.5f) / 32.0f) * 2.0f - 1.0f);
+  float h[4];
+#pragma unroll
+  for (int rr = 0; rr < 4; ++rr)
+    h[rr] = ((F.inv_vp[0][rr] * nx + F.inv_vp[1][rr] * ny) + F.inv_vp[2][rr]) + F.inv_vp[3][rr];
+  float3 vd = f3(h[0] / h[3] - F.cam.x, h[1] / h[3] - F.cam.y, h[2] / h[3] - F.cam.z);
+  vd = vd * (1.0f / len3(vd));
+  const float zn = ((float)gz + 0.5f) / 64.0f;
+  const float t_target = 50.0f * powf(100000.0f / 50.0f, zn);
+  const float3 p0 = f3(F.cam.x, F.cam.y + A.R, F.cam.z);
+  const float r0 = len3(p0);
+  const float ct = dot3(vd, F.sun);
+  float3 tr;
+  const float3 lum = inscatter(A, T, MS, p0, r0, vd, F.sun, phase_r(ct), phase_m(ct, A.mie_g),
+                               t_target / 16.0f, 16, true, F.illum, tr);
+  const float tl = (tr.x * 0.2126f + tr.y * 0.7152f) + tr.z * 0.0722f;
+  out[(size_t)view * (32 * 32 * 64) + (gz * 32 + gy) * 32 + gx] = f16_rounded(lum, tl);
+}
+
+Atmo atmo_from(const PscWorldUniformsGpu& w) {
+  Atmo A;
+  A.R = w.planet_radius_m;
+  A.top = w.atmosphere_top_m;
+  A.hr = w.rayleigh_scale_height_m;
+  A.hm = w.mie_scale_height_m;
+  A.ray_s = make_float3(w.rayleigh_scattering[0], w.rayleigh_scattering[1], w.rayleigh_scattering[2]);
+  A.mie_s = make_float3(w.mie_scattering[0], w.mie_scattering[1], w.mie_scattering[2]);
+  A.mie_a = make_float3(w.mie_absorption[0], w.mie_absorption[1], w.mie_absorption[2]);
+  A.ozone = make_float3(w.ozone_absorption[0], w.ozone_absorption[1], w.ozone_absorption[2]);
+  A.oz_c = w.ozone_center_m;
+  A.oz_t = w.ozone_thickness_m;
+  A.mie_g = w.mie_g;
+  A.albedo = make_float3(w.ground_albedo[0], w.ground_albedo[1], w.ground_albedo[2]);
+  return A;
+}
+
 }  // namespace
+
+void frame_lite_from(const PscFrameUniformsGpu& f, void* out) {
+  FrameLite F;
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) F.inv_vp[c][r] = f.inv_view_proj[c][r];
+  F.cam = make_float3(f.camera_position_world[0], f.camera_position_world[1], f.camera_position_world[2]);
+  F.sun = make_float3(f.sun_direction[0], f.sun_direction[1], f.sun_direction[2]);
+  F.illum = make_float3(f.sun_illuminance[0], f.sun_illuminance[1], f.sun_illuminance[2]);
+  *static_cast<FrameLite*>(out) = F;
+}
+size_t frame_lite_size() { return sizeof(FrameLite); }
+
+int launch_view_lut_bakes(const PscWorldUniformsGpu& w, const void* d_frames, uint32_t n,
+                          const uint16_t* trans, const uint16_t* ms, float4* sky, float4* ap,
+                          cudaStream_t s) {
+  if (n == 0) return PSC_OK;
+  const Atmo A = atmo_from(w);
+  const FrameLite* F = static_cast<const FrameLite*>(d_frames);
+  k_skyview_batch<<<dim3(24, 14, n), dim3(8, 8), 0, s>>>(A, F, trans, ms, sky);
+  k_aerial_batch<<<dim3(8, 8, 16 * n), dim3(4, 4, 4), 0, s>>>(A, F, trans, ms, ap);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
 
 int launch_lut_bakes(const PscWorldUniformsGpu& w, const PscFrameUniformsGpu& f, uint16_t* trans,
                      uint16_t* ms, uint16_t* sky, uint16_t* ap, cudaStream_t s) {

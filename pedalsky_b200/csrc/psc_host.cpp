@@ -111,6 +111,26 @@ struct psc_ctx {
   bool tex_dirty = true;
 
   uint64_t launches = 0;
+
+  // batching (psc_render_batch)
+  PscBatchTuning batch_tuning{128, 16, 0, 0};
+  uint32_t batch_cap_views = 0, batch_cap_tiles = 0;
+  psc::MarchUniforms* d_bu = nullptr;   // per-view uniform blocks
+  psc::ViewDev* d_bv = nullptr;
+  void* d_bframes = nullptr;            // per-view frame records for the LUT bakes
+  float4* d_bsky = nullptr;             // per-view sky-view LUTs
+  float4* d_bap = nullptr;              // per-view aerial-perspective LUTs
+  uint32_t* d_btiles = nullptr;
+  uint32_t* d_bcounter = nullptr;
+  psc::MarchUniforms* h_bu = nullptr;   // pinned staging
+  psc::ViewDev* h_bv = nullptr;
+  void* h_bframes = nullptr;
+  uint32_t* h_btiles = nullptr;
+  cudaEvent_t batch_staged = nullptr;   // staging consumed by the last enqueue
+  cudaStream_t batch_stream = nullptr;  // capture stream
+  cudaGraphExec_t batch_exec = nullptr;
+  std::vector<uint64_t> batch_key;
+  int sms = 0;
 };
 
 namespace {
@@ -171,7 +191,8 @@ float smoothstep_h(float e0, float e1, float x) {
 
 // LayerWindCache (cloud_density_common.wgsl:154-183): one trilinear, repeat
 // sample of the wind field at (0.5, mid_alt / 12 km, 0.5).
-void wind_cache(const psc_ctx* c, const PscCloudLayerGpu& L, psc::LayerConst& o) {
+void wind_cache(const psc_ctx* c, const PscCloudParamsGpu& p, const PscFrameUniformsGpu& f,
+                const PscCloudLayerGpu& L, psc::LayerConst& o) {
   float wx = 0.0f, wz = 0.0f;
   if (c->h_wind.size() == 32u * 16u * 32u * 4u) {
     const float mid = (L.base_m + L.top_m) * 0.5f;
@@ -204,25 +225,27 @@ void wind_cache(const psc_ctx* c, const PscCloudLayerGpu& L, psc::LayerConst& o)
     wx = r[0];
     wz = r[1];
   }
-  const float drift = c->params.wind_drift_strength * c->frame.simulated_seconds;
+  const float drift = p.wind_drift_strength * f.simulated_seconds;
   o.wind_off_x = wx * drift;
   o.wind_off_z = wz * drift;
   o.skew_x = o.skew_z = o.skew_thickness = 0.0f;
-  if (c->params.wind_skew_strength != 0.0f) {
+  if (p.wind_skew_strength != 0.0f) {
     const float sp = std::sqrt(wx * wx + wz * wz);
     if (sp >= 0.1f) {
       o.skew_x = wx / sp;
       o.skew_z = wz / sp;
-      o.skew_thickness = std::fmax(L.top_m - L.base_m, 1.0f) * c->params.wind_skew_strength;
+      o.skew_thickness = std::fmax(L.top_m - L.base_m, 1.0f) * p.wind_skew_strength;
     }
   }
 }
 
-void build_uniforms(const psc_ctx* c, uint32_t width, uint32_t height, psc::MarchUniforms& u) {
+// Flatten one view's scene (params, layers, frame) plus the context's world,
+// options and inputs into the kernel's uniform block.
+void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscCloudLayerGpu* layers,
+                        const PscFrameUniformsGpu& f, uint32_t width, uint32_t height,
+                        psc::MarchUniforms& u) {
   std::memset(&u, 0, sizeof(u));
-  const PscFrameUniformsGpu& f = c->frame;
   const PscWorldUniformsGpu& w = c->world;
-  const PscCloudParamsGpu& p = c->params;
   for (int col = 0; col < 4; ++col)
     for (int row = 0; row < 4; ++row) {
       u.inv_vp[col][row] = f.inv_view_proj[col][row];
@@ -298,7 +321,7 @@ void build_uniforms(const psc_ctx* c, uint32_t width, uint32_t height, psc::Marc
   // diurnal_modulation (cloud_density_common.wgsl:204-219), per layer type
   const float bell = smoothstep_h(-0.1f, 0.4f, f.sun_direction[1]);
   for (uint32_t i = 0; i < 8; ++i) {
-    const PscCloudLayerGpu& L = c->layers[i];
+    const PscCloudLayerGpu& L = layers[i];
     psc::LayerConst& o = u.layers[i];
     o.base_m = L.base_m;
     o.top_m = L.top_m;
@@ -322,7 +345,7 @@ void build_uniforms(const psc_ctx* c, uint32_t width, uint32_t height, psc::Marc
       cm[2] = 1.0f + s;
     }
     for (int k = 0; k < 3; ++k) o.sigma_t[k] = (p.sigma_s[k] + p.sigma_a[k]) * cm[k];
-    wind_cache(c, L, o);
+    wind_cache(c, p, f, L, o);
     // cloud_phase_constants (cloud_march.wgsl:256-272) for non-Cb layers
     const float d = std::fmin(std::fmax(L.droplet_diameter_um * p.droplet_diameter_bias, 5.0f), 50.0f);
     o.g_hg = std::exp(-0.0990567f / (d - 1.67154f));
@@ -350,6 +373,10 @@ void build_uniforms(const psc_ctx* c, uint32_t width, uint32_t height, psc::Marc
   u.lut_ap = c->d_lut[PSC_LUT_AERIAL];
   u.tex_base = c->tex_base;
   u.tex_detail = c->tex_detail;
+}
+
+void build_uniforms(const psc_ctx* c, uint32_t width, uint32_t height, psc::MarchUniforms& u) {
+  build_uniforms_for(c, c->params, c->layers, c->frame, width, height, u);
 }
 
 int build_storage(psc_ctx* c) {
@@ -419,6 +446,164 @@ int build_textures(psc_ctx* c) {
                            &c->tex_detail);
   if (rc) return rc;
   c->tex_dirty = false;
+  return PSC_OK;
+}
+
+void release_batch(psc_ctx* c) {
+  if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+  c->batch_exec = nullptr;
+  c->batch_key.clear();
+  if (c->batch_stream) cudaStreamDestroy(c->batch_stream);
+  if (c->batch_staged) cudaEventDestroy(c->batch_staged);
+  c->batch_stream = nullptr;
+  c->batch_staged = nullptr;
+  dfree(c->d_bu);
+  dfree(c->d_bv);
+  dfree(c->d_bframes);
+  dfree(c->d_bsky);
+  dfree(c->d_bap);
+  dfree(c->d_btiles);
+  dfree(c->d_bcounter);
+  if (c->h_bu) cudaFreeHost(c->h_bu);
+  if (c->h_bv) cudaFreeHost(c->h_bv);
+  if (c->h_bframes) cudaFreeHost(c->h_bframes);
+  if (c->h_btiles) cudaFreeHost(c->h_btiles);
+  c->h_bu = nullptr;
+  c->h_bv = nullptr;
+  c->h_bframes = nullptr;
+  c->h_btiles = nullptr;
+  c->batch_cap_views = c->batch_cap_tiles = 0;
+}
+
+// Grow the batch buffers; a growth invalidates any captured graph.
+int reserve_batch(psc_ctx* c, uint32_t views, uint32_t tiles) {
+  if (!c->batch_stream) {
+    PSC_CUDA(cudaStreamCreateWithFlags(&c->batch_stream, cudaStreamNonBlocking), "batch stream");
+    PSC_CUDA(cudaEventCreateWithFlags(&c->batch_staged, cudaEventDisableTiming), "batch event");
+    PSC_CUDA(cudaMalloc(&c->d_bcounter, sizeof(uint32_t)), "cudaMalloc batch counter");
+  }
+  const size_t fl = psc::frame_lite_size();
+  if (views > c->batch_cap_views) {
+    cudaEventSynchronize(c->batch_staged);
+    if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+    c->batch_exec = nullptr;
+    dfree(c->d_bu);
+    dfree(c->d_bv);
+    dfree(c->d_bframes);
+    dfree(c->d_bsky);
+    dfree(c->d_bap);
+    if (c->h_bu) cudaFreeHost(c->h_bu);
+    if (c->h_bv) cudaFreeHost(c->h_bv);
+    if (c->h_bframes) cudaFreeHost(c->h_bframes);
+    c->h_bu = nullptr;
+    c->h_bv = nullptr;
+    c->h_bframes = nullptr;
+    PSC_CUDA(cudaMalloc(&c->d_bu, views * sizeof(psc::MarchUniforms)), "cudaMalloc batch uniforms");
+    PSC_CUDA(cudaMalloc(&c->d_bv, views * sizeof(psc::ViewDev)), "cudaMalloc batch views");
+    PSC_CUDA(cudaMalloc(&c->d_bframes, views * fl), "cudaMalloc batch frames");
+    PSC_CUDA(cudaMalloc(&c->d_bsky, (size_t)views * 192 * 108 * sizeof(float4)), "cudaMalloc batch sky LUTs");
+    PSC_CUDA(cudaMalloc(&c->d_bap, (size_t)views * 32 * 32 * 64 * sizeof(float4)), "cudaMalloc batch AP LUTs");
+    PSC_CUDA(cudaMallocHost(&c->h_bu, views * sizeof(psc::MarchUniforms)), "pinned batch uniforms");
+    PSC_CUDA(cudaMallocHost(&c->h_bv, views * sizeof(psc::ViewDev)), "pinned batch views");
+    PSC_CUDA(cudaMallocHost(&c->h_bframes, views * fl), "pinned batch frames");
+    c->batch_cap_views = views;
+  }
+  if (tiles > c->batch_cap_tiles) {
+    cudaEventSynchronize(c->batch_staged);
+    if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+    c->batch_exec = nullptr;
+    dfree(c->d_btiles);
+    if (c->h_btiles) cudaFreeHost(c->h_btiles);
+    c->h_btiles = nullptr;
+    PSC_CUDA(cudaMalloc(&c->d_btiles, tiles * sizeof(uint32_t)), "cudaMalloc batch tiles");
+    PSC_CUDA(cudaMallocHost(&c->h_btiles, tiles * sizeof(uint32_t)), "pinned batch tiles");
+    c->batch_cap_tiles = tiles;
+  }
+  return PSC_OK;
+}
+
+int validate_tuning(const PscBatchTuning& t) {
+  if (t.threads != 64 && t.threads != 128 && t.threads != 256)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "batch threads must be 64, 128 or 256 (got %u)", t.threads);
+  const uint32_t warps = t.threads / 32;
+  if (t.tile_w < 8 || t.tile_w % 8 || warps % (t.tile_w / 8))
+    return fail(PSC_ERR_INVALID_ARGUMENT, "tile_w %u must be 8*k with k dividing %u", t.tile_w, warps);
+  return PSC_OK;
+}
+
+// Host staging of one batch: per-view uniform blocks, view records, frame
+// records for the LUT bakes and the cost-sorted tile list.
+int stage_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32_t* n_tiles_out) {
+  const PscBatchTuning& tu = c->batch_tuning;
+  const uint32_t tile_w = tu.tile_w, tile_h = (tu.threads / 32 / (tu.tile_w / 8)) * 4;
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint64_t tx = (views[i].width + tile_w - 1) / tile_w, ty = (views[i].height + tile_h - 1) / tile_h;
+    if (tx > 4096 || ty > 4096) return fail(PSC_ERR_INVALID_ARGUMENT, "view %u has too many tiles", i);
+    total += tx * ty;
+  }
+  if (total > (1u << 26)) return fail(PSC_ERR_INVALID_ARGUMENT, "batch of %llu tiles is too large", (unsigned long long)total);
+  int rc = reserve_batch(c, n, (uint32_t)total);
+  if (rc) return rc;
+  // the previous enqueue must have consumed the pinned staging
+  PSC_CUDA(cudaEventSynchronize(c->batch_staged), "batch staging wait");
+  const size_t fl = psc::frame_lite_size();
+  for (uint32_t i = 0; i < n; ++i) {
+    const PscBatchView& bv = views[i];
+    PscCloudParamsGpu p = bv.params;
+    p.cloud_layer_count = bv.n_layers;
+    PscCloudLayerGpu layers[8];
+    std::memset(layers, 0, sizeof(layers));
+    for (uint32_t l = 0; l < bv.n_layers; ++l) layers[l] = bv.layers[l];
+    psc::MarchUniforms& u = c->h_bu[i];
+    build_uniforms_for(c, p, layers, bv.frame, bv.width, bv.height, u);
+    u.lut_sky = c->d_bsky + (size_t)i * 192 * 108;
+    u.lut_ap = c->d_bap + (size_t)i * 32 * 32 * 64;
+    c->h_bv[i] = psc::ViewDev{bv.width, bv.height, 0, 0, bv.depth, reinterpret_cast<float4*>(bv.out_luminance),
+                              reinterpret_cast<float4*>(bv.out_transmittance), reinterpret_cast<float4*>(bv.hdr)};
+    psc::frame_lite_from(bv.frame, static_cast<char*>(c->h_bframes) + i * fl);
+  }
+  // views in descending estimated cost (primary steps x layers, then pixels)
+  std::vector<uint32_t> order(n);
+  for (uint32_t i = 0; i < n; ++i) order[i] = i;
+  auto cost = [&](uint32_t i) {
+    return (double)views[i].params.cloud_steps * (double)std::max<uint32_t>(views[i].n_layers, 1);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    const double ca = cost(a), cb = cost(b);
+    if (ca != cb) return ca > cb;
+    return (uint64_t)views[a].width * views[a].height > (uint64_t)views[b].width * views[b].height;
+  });
+  uint32_t k = 0;
+  for (uint32_t i : order) {
+    const uint32_t tx = (views[i].width + tile_w - 1) / tile_w, ty = (views[i].height + tile_h - 1) / tile_h;
+    for (uint32_t y = 0; y < ty; ++y)
+      for (uint32_t x = 0; x < tx; ++x) c->h_btiles[k++] = (i << 24) | (x << 12) | y;
+  }
+  *n_tiles_out = k;
+  return PSC_OK;
+}
+
+// Copies, per-view LUT bakes, counter reset and the persistent march on `s`.
+int enqueue_batch(psc_ctx* c, uint32_t n, uint32_t n_tiles, cudaStream_t s, bool capturing) {
+  const size_t fl = psc::frame_lite_size();
+  PSC_CUDA(cudaMemcpyAsync(c->d_bu, c->h_bu, n * sizeof(psc::MarchUniforms), cudaMemcpyHostToDevice, s), "batch uniforms H2D");
+  PSC_CUDA(cudaMemcpyAsync(c->d_bv, c->h_bv, n * sizeof(psc::ViewDev), cudaMemcpyHostToDevice, s), "batch views H2D");
+  PSC_CUDA(cudaMemcpyAsync(c->d_bframes, c->h_bframes, n * fl, cudaMemcpyHostToDevice, s), "batch frames H2D");
+  PSC_CUDA(cudaMemcpyAsync(c->d_btiles, c->h_btiles, n_tiles * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "batch tiles H2D");
+  // Under capture the record must become an external event node so that the
+  // next call can wait on it after a graph launch.
+  PSC_CUDA(cudaEventRecordWithFlags(c->batch_staged, s, capturing ? cudaEventRecordExternal : 0),
+           "batch event");
+  if (psc::launch_view_lut_bakes(c->world, c->d_bframes, n, c->d_lut_h[PSC_LUT_TRANSMITTANCE],
+                                 c->d_lut_h[PSC_LUT_MULTISCATTER], c->d_bsky, c->d_bap, s))
+    return fail(PSC_ERR_CUDA, "per-view LUT bake launch failed");
+  PSC_CUDA(cudaMemsetAsync(c->d_bcounter, 0, sizeof(uint32_t), s), "batch counter reset");
+  const int rc = psc::launch_march_batch(c->opts, (int)c->batch_tuning.threads, c->batch_tuning.tile_w,
+                                         c->d_bu, c->d_bv, c->d_btiles, n_tiles, c->d_bcounter, c->sms, s);
+  if (rc == PSC_ERR_UNSUPPORTED)
+    return fail(rc, "batched march supports F16/U8/F32 exact, F16/U8 hybrid and U8 texture storage");
+  if (rc) return fail(rc, "batched march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   return PSC_OK;
 }
 
@@ -788,7 +973,8 @@ int psc_create(int device, psc_ctx** out) {
 int psc_destroy(psc_ctx* c) {
   if (!c) return PSC_OK;
   const bool touched = c->d_base_u8 || c->d_detail_u8 || c->d_curl || c->d_blue || c->d_weather ||
-                       c->d_type || c->d_lut[0] || c->d_lut_h[0] || c->d_lut[2] || c->d_lut_h[3];
+                       c->d_type || c->d_lut[0] || c->d_lut_h[0] || c->d_lut[2] || c->d_lut_h[3] ||
+                       c->d_bu || c->batch_stream;
   if (!touched) {
     delete c;
     return PSC_OK;
@@ -807,6 +993,7 @@ int psc_destroy(psc_ctx* c) {
     dfree(c->d_lut[k]);
     dfree(c->d_lut_h[k]);
   }
+  release_batch(c);
   delete c;
   return PSC_OK;
 }
@@ -1096,6 +1283,144 @@ int psc_composite(const float* l, const float* t, float* hdr, uint32_t w, uint32
   if (psc::launch_composite(reinterpret_cast<const float4*>(l), reinterpret_cast<const float4*>(t),
                             reinterpret_cast<float4*>(hdr), w * h, static_cast<cudaStream_t>(stream)))
     return fail(PSC_ERR_CUDA, "composite launch failed");
+  return PSC_OK;
+}
+
+int psc_set_batch_tuning(psc_ctx* c, const PscBatchTuning* t) {
+  if (!c || !t) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  const int rc = validate_tuning(*t);
+  if (rc) return rc;
+  c->batch_tuning = *t;
+  return PSC_OK;
+}
+
+int psc_get_batch_tuning(psc_ctx* c, PscBatchTuning* out) {
+  if (!c || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  *out = c->batch_tuning;
+  return PSC_OK;
+}
+
+int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* stream) {
+  if (!c || (n && !views)) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (n == 0) return PSC_OK;
+  if (n > PSC_MAX_BATCH_VIEWS) return fail(PSC_ERR_INVALID_ARGUMENT, "%u views exceeds %u", n, PSC_MAX_BATCH_VIEWS);
+  if (!c->have_base || !c->have_detail || !c->have_curl || !c->have_blue)
+    return fail(PSC_ERR_MISSING_INPUT, "noise volumes missing (psc_bake_noise or psc_upload_noise)");
+  if (!c->d_weather) return fail(PSC_ERR_MISSING_INPUT, "weather map missing (psc_upload_weather)");
+  if (!c->d_lut_h[PSC_LUT_TRANSMITTANCE] || !c->d_lut_h[PSC_LUT_MULTISCATTER] || !c->have_lut[PSC_LUT_TRANSMITTANCE])
+    return fail(PSC_ERR_MISSING_INPUT, "transmittance/multi-scatter LUTs missing (psc_bake_luts or psc_upload_lut)");
+  if (c->opts.schedule != PSC_SCHED_FAST)
+    return fail(PSC_ERR_UNSUPPORTED, "the batched kernel implements the FAST schedule (options.schedule)");
+  for (uint32_t i = 0; i < n; ++i) {
+    const PscBatchView& v = views[i];
+    if (!v.width || !v.height || v.width > 32768 || v.height > 32768)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "batch view %u: size %ux%u out of range", i, v.width, v.height);
+    if (!v.out_luminance && !v.out_transmittance && !(c->opts.composite && v.hdr))
+      return fail(PSC_ERR_INVALID_ARGUMENT, "batch view %u has no output buffer", i);
+    if (c->opts.composite && !v.hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "batch view %u: composite needs hdr", i);
+    int rc = validate_layers(v.layers, v.n_layers);
+    if (rc) return fail(rc, "batch view %u: %s", i, g_last_error.c_str());
+    PscCloudParamsGpu p = v.params;
+    p.cloud_layer_count = v.n_layers;
+    rc = validate_params(p);
+    if (rc) return fail(rc, "batch view %u: %s", i, g_last_error.c_str());
+    if (p.multi_scatter_octaves == 0 || p.multi_scatter_octaves > 4)
+      return fail(PSC_ERR_UNSUPPORTED, "batch view %u: the batched kernel handles 1..4 octaves", i);
+    const float* ff = reinterpret_cast<const float*>(&v.frame);
+    for (size_t k = 0; k < sizeof(v.frame) / 4; ++k)
+      if (k != 94 && !std::isfinite(ff[k])) return fail(PSC_ERR_NOT_FINITE, "batch view %u: frame word %zu", i, k);
+  }
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  if (!c->sms) PSC_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device), "SM count");
+  rc = build_storage(c);
+  if (rc) return rc;
+  rc = build_textures(c);
+  if (rc) return rc;
+  if (c->opts.filter != PSC_FILTER_EXACT && (!c->tex_base || !c->tex_detail))
+    return fail(PSC_ERR_MISSING_INPUT, "texture objects for the noise volumes were not created");
+  uint32_t n_tiles = 0;
+  rc = stage_batch(c, views, n, &n_tiles);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!c->batch_tuning.use_graph) {
+    rc = enqueue_batch(c, n, n_tiles, s, false);
+    if (rc) return rc;
+    ++c->launches;
+    return PSC_OK;
+  }
+  // Graph path: the key is everything the captured nodes bake in (buffer
+  // pointers, sizes, options, launch shape); uniforms are read from the
+  // pinned staging at launch time and may change freely.
+  std::vector<uint64_t> key = {n, n_tiles, c->batch_tuning.threads, c->batch_tuning.tile_w,
+                               c->opts.storage, c->opts.filter, c->opts.composite,
+                               (uint64_t)(uintptr_t)c->d_bu, (uint64_t)(uintptr_t)c->d_btiles,
+                               (uint64_t)(uintptr_t)c->d_base_store, (uint64_t)c->tex_base};
+  if (!c->batch_exec || key != c->batch_key) {
+    if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+    c->batch_exec = nullptr;
+    cudaGraph_t g = nullptr;
+    PSC_CUDA(cudaStreamBeginCapture(c->batch_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    rc = enqueue_batch(c, n, n_tiles, c->batch_stream, true);
+    const cudaError_t ce = cudaStreamEndCapture(c->batch_stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "end capture");
+    const cudaError_t ie = cudaGraphInstantiate(&c->batch_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return cuda_fail(ie, "graph instantiate");
+    c->batch_key = key;
+  }
+  PSC_CUDA(cudaGraphLaunch(c->batch_exec, s), "graph launch");
+  ++c->launches;
+  return PSC_OK;
+}
+
+int psc_autotune_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32_t reps,
+                       PscBatchTuning* best, float* best_ms, void* stream) {
+  if (!c || !views || !n) return fail(PSC_ERR_INVALID_ARGUMENT, "null or empty batch");
+  if (reps == 0 || reps > 100) return fail(PSC_ERR_INVALID_ARGUMENT, "reps must be 1..100");
+  const PscBatchTuning saved = c->batch_tuning;
+  static const uint32_t cand[][2] = {{128, 16}, {128, 32}, {128, 8}, {256, 16}, {256, 32},
+                                     {256, 64}, {64, 8}, {64, 16}};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaEvent_t a = nullptr, b = nullptr;
+  PSC_CUDA(cudaEventCreate(&a), "event");
+  PSC_CUDA(cudaEventCreate(&b), "event");
+  float best_t = INFINITY;
+  PscBatchTuning best_tu = saved;
+  int rc = PSC_OK;
+  for (const auto& cd : cand) {
+    c->batch_tuning = PscBatchTuning{cd[0], cd[1], 0, 0};
+    rc = psc_render_batch(c, views, n, stream);  // warm-up
+    if (rc) break;
+    std::vector<float> ts;
+    for (uint32_t r = 0; r < reps && !rc; ++r) {
+      cudaEventRecord(a, s);
+      rc = psc_render_batch(c, views, n, stream);
+      cudaEventRecord(b, s);
+      if (cudaEventSynchronize(b) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "autotune sync");
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, a, b);
+      ts.push_back(ms);
+    }
+    if (rc) break;
+    std::sort(ts.begin(), ts.end());
+    const float med = ts[ts.size() / 2];
+    if (med < best_t) {
+      best_t = med;
+      best_tu = c->batch_tuning;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  best_tu.use_graph = saved.use_graph;
+  c->batch_tuning = rc ? saved : best_tu;
+  if (rc) return rc;
+  if (best) *best = best_tu;
+  if (best_ms) *best_ms = best_t;
   return PSC_OK;
 }
 

@@ -44,7 +44,7 @@ struct LayerConst {
   double r_bottom, r_top;  // planet_radius + base/top, FP64
 };
 
-struct MarchUniforms {
+struct alignas(16) MarchUniforms {
   // frame
   float inv_vp[4][4];      // inv_view_proj, [col][row]
   double inv_vp_d[4][4];   // the same matrix widened to double
@@ -129,6 +129,18 @@ int launch_composite(const float4* l, const float4* t, float4* hdr, uint32_t n,
                      cudaStream_t stream);
 // Noise bakes (noise_bake.cu), synchronous on `stream`.
 int launch_noise_bakes(uint8_t* base, uint8_t* detail, uint8_t* curl, cudaStream_t stream);
+// Persistent batched march (march_batch.cu).
+int launch_march_batch(const PscMarchOptions& o, int threads, uint32_t tile_w,
+                       const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles,
+                       uint32_t n_tiles, uint32_t* counter, int sms, cudaStream_t stream);
+// Per-view sky-view + aerial-perspective LUTs for a batch (atmosphere.cu):
+// `d_frames` holds n frame records built by frame_lite_from; outputs are
+// float4 (RGBA16F-rounded), sky 192x108 and AP 32x32x64 per view.
+void frame_lite_from(const PscFrameUniformsGpu& f, void* out);
+size_t frame_lite_size();
+int launch_view_lut_bakes(const PscWorldUniformsGpu& world, const void* d_frames, uint32_t n,
+                          const uint16_t* trans_f16, const uint16_t* ms_f16, float4* sky,
+                          float4* ap, cudaStream_t stream);
 // Atmosphere LUT bakes (atmosphere.cu).
 int launch_lut_bakes(const PscWorldUniformsGpu& world, const PscFrameUniformsGpu& frame,
                      uint16_t* trans_f16, uint16_t* ms_f16, uint16_t* sky_f16,

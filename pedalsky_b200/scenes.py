@@ -195,7 +195,8 @@ def ground_depth(frame, world, width, height):
     X = cam + d * t[..., None]
     vp = np.array(frame.view_proj, np.float64)
     clip = vp[0] * X[..., 0:1] + vp[1] * X[..., 1:2] + vp[2] * X[..., 2:3] + vp[3]
-    depth = np.where(hit, clip[..., 2] / clip[..., 3], 0.0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        depth = np.where(hit, clip[..., 2] / clip[..., 3], 0.0)
     return depth.astype(np.float32)
 
 
@@ -212,15 +213,48 @@ def sky_background(frame, width, height):
     return bg
 
 
+def device_inputs(frame, world, width, height, device):
+    """(depth, background) of `ground_depth` / `sky_background` computed with
+    torch on `device` (float64 rays), for large batches."""
+    import torch
+    dt = torch.float64
+    inv = torch.tensor(np.array(frame.inv_view_proj, np.float64), dtype=dt, device=device)
+    vp = torch.tensor(np.array(frame.view_proj, np.float64), dtype=dt, device=device)
+    cam = torch.tensor(np.array(frame.camera_position_world[:3], np.float64), dtype=dt, device=device)
+    xs = (torch.arange(width, dtype=dt, device=device) + 0.5) / width * 2 - 1
+    ys = 1 - (torch.arange(height, dtype=dt, device=device) + 0.5) / height * 2
+    ny, nx = torch.meshgrid(ys, xs, indexing="ij")
+    h = inv[0] * nx[..., None] + inv[1] * ny[..., None] + inv[2] + inv[3]
+    d = h[..., :3] / h[..., 3:4] - cam
+    d = d / torch.linalg.norm(d, dim=-1, keepdim=True)
+    R = float(world.planet_radius_m)
+    oc = cam + torch.tensor([0.0, R, 0.0], dtype=dt, device=device)
+    b = d @ oc
+    c = oc @ oc - R * R
+    disc = b * b - c
+    t = -b - torch.sqrt(torch.clamp(disc, min=0))
+    hit = (disc >= 0) & (t > 0)
+    X = cam + d * t[..., None]
+    clip = vp[0] * X[..., 0:1] + vp[1] * X[..., 1:2] + vp[2] * X[..., 2:3] + vp[3]
+    depth = torch.where(hit, clip[..., 2] / clip[..., 3], torch.zeros_like(t)).float()
+    up = d[..., 1].clamp(-1, 1)
+    sky = 2500.0 + 6000.0 * (1.0 - up.abs()) ** 2
+    tint = torch.tensor([0.72, 0.86, 1.0], dtype=dt, device=device)
+    ground = torch.tensor([0.55, 0.5, 0.45], dtype=dt, device=device) * 900.0
+    rgb = torch.where(up[..., None] < 0, ground.expand(height, width, 3), sky[..., None] * tint)
+    bg = torch.cat([rgb, torch.ones_like(rgb[..., :1])], dim=-1).float().contiguous()
+    return depth.contiguous(), bg
+
+
 def _finish(name, width, height, params, layers_n, frame, opts, weather, ww, wh, wfmt,
-            type_grid=None, with_ground=True, wind=None):
+            type_grid=None, with_ground=True, wind=None, host_inputs=True):
     layers, n = layers_n
     world = world_default()
     params.cloud_layer_count = n
-    depth = ground_depth(frame, world, width, height) if with_ground else None
+    depth = ground_depth(frame, world, width, height) if (with_ground and host_inputs) else None
+    bg = sky_background(frame, width, height) if host_inputs else None
     return Scene(name, width, height, params, layers, n, frame, world, opts, weather, ww, wh, wfmt,
-                 wind if wind is not None else wind_field(), type_grid, depth,
-                 sky_background(frame, width, height))
+                 wind if wind is not None else wind_field(), type_grid, depth, bg)
 
 
 def plain_320x180(width=320, height=180, phase=capi.PHASE_DUAL_LOBE_HG, **kw) -> Scene:
@@ -275,9 +309,56 @@ def stress_2160p(width=3840, height=2160, frame_index=0, **kw) -> Scene:
     return s
 
 
+# Altitude bands that keep randomly typed layers disjoint: low, middle, high.
+_BANDS = ((600.0, 2600.0), (3000.0, 6000.0), (7000.0, 11000.0))
+CUBE_FACES = ((0.0, 0.0), (90.0, 0.0), (180.0, 0.0), (270.0, 0.0), (0.0, 89.9), (0.0, -89.9))
+FRAME_SIZES = ((640, 360), (1280, 720), (1920, 1080), (2560, 1440), (3840, 2160))
+CUBE_SIZES = (256, 512, 768, 1024)
+
+
+def batch_views(n=64, seed=0, size_scale=1.0, host_inputs=True, **kw) -> list[Scene]:
+    """Seeded batch of uneven views: half cube-map faces (256^2..1024^2,
+    fov 90), half 16:9 frames (640x360..3840x2160, fov 60); each with 1-3
+    disjoint layers of uniformly drawn type, coverage U[0.2, 0.9], sun
+    elevation U[5, 70] deg, azimuth U[0, 360), and 48..160 primary steps.
+    `size_scale` shrinks every view (tests)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        if i % 2 == 0:
+            side = int(CUBE_SIZES[rng.integers(len(CUBE_SIZES))])
+            w = h = side
+            yaw, pitch = CUBE_FACES[rng.integers(len(CUBE_FACES))]
+            fov = 90.0
+        else:
+            w, h = FRAME_SIZES[rng.integers(len(FRAME_SIZES))]
+            yaw, pitch, fov = float(rng.uniform(0, 360)), float(rng.uniform(-5, 30)), 60.0
+        w, h = max(8, int(w * size_scale)), max(8, int(h * size_scale))
+        nl = int(rng.integers(1, 4))
+        bands = sorted(rng.choice(3, size=nl, replace=False))
+        descs = []
+        for b in bands:
+            lo, hi = _BANDS[b]
+            t = int(rng.integers(0, 8))
+            thick = float(rng.uniform(400.0, 1800.0))
+            base = float(rng.uniform(lo, hi - thick))
+            descs.append((t, base, base + thick, float(rng.uniform(0.2, 0.9))))
+        p = default_params()
+        p.cloud_steps = int(rng.integers(48, 161))
+        ln = synth_layers(descs)
+        frame = frame_for(w, h, yaw_deg=yaw, pitch_deg=pitch, fov_deg=fov,
+                          sun_alt_deg=float(rng.uniform(5, 70)), sun_az_deg=float(rng.uniform(0, 360)))
+        sc = _finish(f"batch_{i}", w, h, p, ln, frame, options(schedule=capi.SCHED_FAST, **kw),
+                     reference_weather(ln[1]), 128, 128, capi.WEATHER_RGBA16F,
+                     host_inputs=host_inputs)
+        out.append(sc)
+    return out
+
+
 WORKLOADS = {
     "plain_320x180": plain_320x180,
     "plain_literal": plain_literal,
     "precision_1080p": precision_1080p,
     "stress_2160p": stress_2160p,
+    "batch_64": batch_views,
 }

@@ -1,0 +1,128 @@
+"""GPU tests of the persistent batched march: every view of a batch must
+equal the same view rendered on its own by the single-view FAST kernel
+(same per-ray body, per-view LUTs baked the same way), in eager and
+CUDA-graph mode, for every autotuner candidate shape."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from pedalsky_b200 import batch as B
+from pedalsky_b200 import capi, scenes
+from pedalsky_b200.capi import PscError, call
+from pedalsky_b200.subsystem import subsystem_for_scene
+
+from . import _gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _single(view, noise):
+    """One view through psc_render with LUTs baked for its own frame."""
+    torch = _gpu.torch_cuda()
+    sub = subsystem_for_scene(view, luts=None, noise=noise)
+    dev = torch.device("cuda", 0)
+    L = torch.zeros((view.height, view.width, 4), device=dev)
+    T = torch.zeros((view.height, view.width, 4), device=dev)
+    depth = torch.from_numpy(view.depth).to(dev)
+    v = capi.View(view.width, view.height, depth.data_ptr(), L.data_ptr(), T.data_ptr(), None)
+    call("psc_render", sub.handle, C.byref(v), 1, None)
+    torch.cuda.synchronize()
+    sub.close()
+    return L.cpu().numpy(), T.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def small_batch():
+    return scenes.batch_views(10, seed=7, size_scale=0.06, storage=capi.STORAGE_F16,
+                              filt=capi.FILTER_HYBRID)
+
+
+def _run_batch(views, noise, tuning=(128, 16, 0), reps=1):
+    torch = _gpu.torch_cuda()
+    sub = subsystem_for_scene(views[0], luts=None, noise=noise)
+    b = B.Batch(views, "cuda:0", outputs=("luminance", "transmittance"))
+    B.set_tuning(sub.handle, *tuning)
+    for _ in range(reps):
+        b.render(sub.handle)
+    torch.cuda.synchronize()
+    out = [(L.cpu().numpy(), T.cpu().numpy()) for L, T in zip(b.lum, b.trans)]
+    sub.close()
+    return out
+
+
+def _compare(views, got, noise, rtol=2e-6):
+    worst = 0.0
+    for s, (L, T) in zip(views, got):
+        L1, T1 = _single(s, noise)
+        d = np.abs(L - L1)[..., :3] / np.maximum(np.abs(L1[..., :3]), 1.0)
+        worst = max(worst, float(d.max()), float(np.abs(T - T1).max()))
+    assert worst <= rtol, worst
+    return worst
+
+
+def test_batch_matches_single_view_renders(small_batch, oracle_noise):
+    got = _run_batch(small_batch, oracle_noise)
+    _compare(small_batch, got, oracle_noise)
+
+
+@pytest.mark.parametrize("threads,tile_w", [(64, 8), (64, 16), (128, 8), (128, 32), (256, 16),
+                                            (256, 64)])
+def test_every_launch_shape_gives_the_same_image(small_batch, oracle_noise, threads, tile_w):
+    ref = _run_batch(small_batch, oracle_noise)
+    got = _run_batch(small_batch, oracle_noise, (threads, tile_w, 0))
+    for (a, b), (c, d) in zip(ref, got):
+        assert np.array_equal(a, c) and np.array_equal(b, d)
+
+
+def test_graph_replay_equals_eager_and_follows_camera_changes(small_batch, oracle_noise):
+    torch = _gpu.torch_cuda()
+    eager = _run_batch(small_batch, oracle_noise)
+    replayed = _run_batch(small_batch, oracle_noise, (128, 16, 1), reps=3)
+    for (a, b), (c, d) in zip(eager, replayed):
+        assert np.array_equal(a, c) and np.array_equal(b, d)
+    # the captured graph reads the uniforms from staging at each launch:
+    # moving the sun changes the image without re-capture
+    sub = subsystem_for_scene(small_batch[0], luts=None, noise=oracle_noise)
+    b = B.Batch(small_batch, "cuda:0", outputs=("luminance",))
+    B.set_tuning(sub.handle, 128, 16, 1)
+    b.render(sub.handle)
+    torch.cuda.synchronize()
+    first = b.lum[1].cpu().numpy().copy()
+    f = scenes.frame_for(small_batch[1].width, small_batch[1].height, sun_alt_deg=8.0)
+    b.arr[1].frame = f
+    b.render(sub.handle)
+    torch.cuda.synchronize()
+    assert not np.array_equal(first, b.lum[1].cpu().numpy())
+    sub.close()
+
+
+def test_autotuner_picks_a_valid_shape(small_batch, oracle_noise):
+    _gpu.torch_cuda()
+    sub = subsystem_for_scene(small_batch[0], luts=None, noise=oracle_noise)
+    b = B.Batch(small_batch, "cuda:0", outputs=("luminance",))
+    res = B.autotune(sub.handle, b, reps=1)
+    assert res["threads"] in (64, 128, 256) and res["ms"] > 0
+    t = capi.BatchTuning()
+    call("psc_get_batch_tuning", sub.handle, C.byref(t))
+    assert (t.threads, t.tile_w) == (res["threads"], res["tile_w"])
+    sub.close()
+
+
+def test_batch_argument_errors(small_batch, oracle_noise):
+    _gpu.torch_cuda()
+    sub = subsystem_for_scene(small_batch[0], luts=None, noise=oracle_noise)
+    b = B.Batch(small_batch[:2], "cuda:0", outputs=("luminance",))
+    with pytest.raises(PscError):
+        call("psc_set_batch_tuning", sub.handle, C.byref(capi.BatchTuning(96, 16, 0, 0)))
+    with pytest.raises(PscError):
+        call("psc_set_batch_tuning", sub.handle, C.byref(capi.BatchTuning(128, 24, 0, 0)))
+    b.arr[0].n_layers = 9
+    with pytest.raises(PscError):
+        b.render(sub.handle)
+    b.arr[0].n_layers = small_batch[0].n_layers
+    b.arr[1].params.multi_scatter_octaves = 6
+    with pytest.raises(PscError) as e:
+        b.render(sub.handle)
+    assert e.value.code == -8
+    sub.close()
