@@ -443,6 +443,47 @@ int psc_render_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, void* 
 int psc_autotune_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, uint32_t reps,
                        PscBatchTuning* best, float* best_ms, void* stream);
 
+/* ------------------------------------------------ allocation-free batch */
+
+#define PSC_NOALLOC_MAX_VIEWS 64u
+#define PSC_NOALLOC_MAX_TILES (1u << 20)
+
+/* No counterpart in the reference (which allocates its GPU resources through
+ * wgpu at set-up).  psc_render_batch with no allocation at call time, for
+ * callers that cannot call cudaMalloc while rendering: a real-time frame loop
+ * where an allocation or free would synchronise the device, an engine that
+ * owns a fixed device-memory budget and must not see it grow, or code that
+ * runs in a host callback where the CUDA allocator may not be called.
+ *
+ * The batch's work list (tile counter, tile list, per-view uniform and frame
+ * records) lives in one fixed array of device memory of about 4.1 MiB,
+ * reserved in every GPU that loads this library and held until the process
+ * exits.  Limits: at most PSC_NOALLOC_MAX_VIEWS views and
+ * PSC_NOALLOC_MAX_TILES tiles under the context's launch shape (a tile is
+ * tile_w x threads/32/(tile_w/8)*4 pixels, 16x8 by default, so about 134 M
+ * pixels); larger batches are rejected with PSC_ERR_INVALID_ARGUMENT.
+ *
+ * The caller passes the views (inputs and outputs as for psc_render_batch)
+ * and two device buffers, 16-byte aligned, that the call fills with each
+ * view's LUTs before marching: `sky_luts`, n x 192 x 108 RGBA32F texels, and
+ * `ap_luts`, n x 32 x 32 x 64 RGBA32F texels (view i at i x one LUT).
+ *
+ * Set-up: everything psc_render_batch needs, plus one psc_render or
+ * psc_render_batch call after the last change of noise inputs or storage /
+ * filter options, which builds the noise storage form and texture objects
+ * (those calls allocate); otherwise PSC_ERR_MISSING_INPUT.  The first call
+ * on each device looks up the array's device address (and may load the
+ * library's GPU code on that device); make that first call before any stream
+ * capture.
+ *
+ * Every call shares the one array, whose contents persist from the previous
+ * call (the counter is cleared on each call).  Calls whose work overlaps on
+ * the GPU, on different streams or from different contexts on the same
+ * device, race on it: order them on one stream or synchronise between them.
+ * Calls from several host threads are serialised while they stage. */
+int psc_render_batch_noalloc(psc_ctx* ctx, const PscBatchView* views, uint32_t n, float* sky_luts,
+                             float* ap_luts, void* stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 

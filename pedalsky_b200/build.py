@@ -27,6 +27,7 @@ CUDA_UNITS = {
     "march.cu": [],
     "march_fast.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "march_batch.cu": ["-prec-div=false", "-prec-sqrt=false"],
+    "march_noalloc.cu": [],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
 }

@@ -183,6 +183,7 @@ _PROTOS = {
     "psc_set_batch_tuning": [_vp, P(BatchTuning)],
     "psc_get_batch_tuning": [_vp, P(BatchTuning)],
     "psc_render_batch": [_vp, P(BatchView), u32, _vp],
+    "psc_render_batch_noalloc": [_vp, P(BatchView), u32, _vp, _vp, _vp],
     "psc_autotune_batch": [_vp, P(BatchView), u32, u32, P(BatchTuning), P(C.c_float), _vp],
 }
 _RESTYPES = {

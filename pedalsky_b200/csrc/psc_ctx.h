@@ -1,0 +1,100 @@
+// The context object behind the C ABI, shared by the host translation
+// units (psc_host.cpp and the allocation-free batch path in
+// march_noalloc.cu), and the host helpers both use.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/psclouds.h"
+#include "psc_internal.h"
+
+struct psc_ctx {
+  int device = 0;
+  PscCloudParamsGpu params{};
+  PscCloudLayerGpu layers[8]{};
+  uint32_t n_layers = 0;
+  PscFrameUniformsGpu frame{};
+  PscWorldUniformsGpu world{};
+  bool have_frame = false;
+  PscMarchOptions opts{};
+
+  uint8_t* d_base_u8 = nullptr;    // 128^3 RGBA8 (canonical)
+  uint8_t* d_detail_u8 = nullptr;  // 32^3 RGBA8
+  void* d_base_store = nullptr;    // storage form
+  void* d_detail_store = nullptr;
+  int store_form = -1;
+  float fp8_scale = 448.0f;
+  uint8_t* d_curl = nullptr;       // 128^2 RG8
+  float* d_blue = nullptr;         // 64^2 floats
+  std::vector<uint8_t> h_blue;
+  bool have_base = false, have_detail = false, have_curl = false, have_blue = false;
+
+  float* d_weather = nullptr;
+  uint32_t weather_w = 0, weather_h = 0;
+  uint8_t* d_type = nullptr;
+  uint32_t type_w = 0, type_h = 0;
+  std::vector<uint16_t> h_wind;    // 32x16x32 RGBA16F
+
+  float4* d_lut[4] = {nullptr, nullptr, nullptr, nullptr};  // float4 copies
+  uint16_t* d_lut_h[4] = {nullptr, nullptr, nullptr, nullptr};  // RGBA16F bake outputs
+  bool have_lut[4] = {false, false, false, false};
+
+  // texture-unit path
+  cudaArray_t arr_base = nullptr, arr_detail = nullptr;
+  cudaTextureObject_t tex_base = 0, tex_detail = 0;
+  bool tex_dirty = true;
+
+  uint64_t launches = 0;
+
+  // batching (psc_render_batch)
+  PscBatchTuning batch_tuning{128, 16, 0, 0};
+  uint32_t batch_cap_views = 0, batch_cap_tiles = 0;
+  psc::MarchUniforms* d_bu = nullptr;   // per-view uniform blocks
+  psc::ViewDev* d_bv = nullptr;
+  void* d_bframes = nullptr;            // per-view frame records for the LUT bakes
+  float4* d_bsky = nullptr;             // per-view sky-view LUTs
+  float4* d_bap = nullptr;              // per-view aerial-perspective LUTs
+  uint32_t* d_btiles = nullptr;
+  uint32_t* d_bcounter = nullptr;
+  psc::MarchUniforms* h_bu = nullptr;   // pinned staging
+  psc::ViewDev* h_bv = nullptr;
+  void* h_bframes = nullptr;
+  uint32_t* h_btiles = nullptr;
+  cudaEvent_t batch_staged = nullptr;   // staging consumed by the last enqueue
+  cudaStream_t batch_stream = nullptr;  // capture stream
+  cudaGraphExec_t batch_exec = nullptr;
+  std::vector<uint64_t> batch_key;
+  int sms = 0;
+};
+
+namespace psc {
+namespace host {
+
+// Thread-local error message + status code (psc_last_error).
+int fail(int code, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+// Bind the context's device (checks the ordinal).
+int ensure_device(psc_ctx* c);
+// Context inputs, options and per-view checks shared by the batch entry
+// points (the same rules as psc_render_batch).
+int validate_batch(psc_ctx* c, const PscBatchView* views, uint32_t n);
+// Tiles the batch needs under the launch shape `tu`; UINT64_MAX when a view
+// has more than 4096 tiles along one axis (the tile word's 12-bit fields).
+uint64_t count_batch_tiles(const PscBatchView* views, uint32_t n, const PscBatchTuning& tu);
+// Host records of one batch (per-view uniform blocks pointing at the
+// per-view LUTs `sky` + i*192*108 and `ap` + i*32*32*64, view records,
+// frame records for the LUT bakes) and the cost-sorted tile list.  Uses no
+// heap.  Fails if the tiles would exceed `max_tiles`.
+int fill_batch(const psc_ctx* c, const PscBatchView* views, uint32_t n, const PscBatchTuning& tu,
+               psc::MarchUniforms* hu, psc::ViewDev* hv, void* hframes, uint32_t* htiles, uint32_t max_tiles,
+               float4* sky, float4* ap, uint32_t* n_tiles_out);
+// True when the noise storage form (and, for texture filtering, the texture
+// objects) for the current options exist, i.e. rendering would not allocate.
+bool storage_ready(const psc_ctx* c);
+
+}  // namespace host
+}  // namespace psc

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/psclouds.h"
+#include "psc_ctx.h"
 #include "psc_internal.h"
 
 namespace psc {
@@ -26,8 +27,17 @@ int launch_convert_storage(const uint8_t* src, void* dst, uint32_t n_texels, int
 }
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
+
+#define PSC_CUDA(call, what)                    \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+namespace psc {
+namespace host {
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -44,11 +54,22 @@ int cuda_fail(cudaError_t e, const char* what) {
               cudaGetErrorString(e));
 }
 
-#define PSC_CUDA(call, what)                    \
-  do {                                          \
-    cudaError_t e_ = (call);                    \
-    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
-  } while (0)
+int ensure_device(psc_ctx* c) {
+  int n = 0;
+  PSC_CUDA(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+  if (c->device >= n) return fail(PSC_ERR_INVALID_ARGUMENT, "device %d not in [0,%d)", c->device, n);
+  PSC_CUDA(cudaSetDevice(c->device), "cudaSetDevice");
+  return PSC_OK;
+}
+
+}  // namespace host
+}  // namespace psc
+
+using psc::host::cuda_fail;
+using psc::host::ensure_device;
+using psc::host::fail;
+
+namespace {
 
 bool all_finite(const float* p, size_t n) {
   for (size_t i = 0; i < n; ++i)
@@ -74,64 +95,6 @@ void dfree(T*& p) {
 
 }  // namespace
 
-struct psc_ctx {
-  int device = 0;
-  PscCloudParamsGpu params{};
-  PscCloudLayerGpu layers[8]{};
-  uint32_t n_layers = 0;
-  PscFrameUniformsGpu frame{};
-  PscWorldUniformsGpu world{};
-  bool have_frame = false;
-  PscMarchOptions opts{};
-
-  uint8_t* d_base_u8 = nullptr;    // 128^3 RGBA8 (canonical)
-  uint8_t* d_detail_u8 = nullptr;  // 32^3 RGBA8
-  void* d_base_store = nullptr;    // storage form
-  void* d_detail_store = nullptr;
-  int store_form = -1;
-  float fp8_scale = 448.0f;
-  uint8_t* d_curl = nullptr;       // 128^2 RG8
-  float* d_blue = nullptr;         // 64^2 floats
-  std::vector<uint8_t> h_blue;
-  bool have_base = false, have_detail = false, have_curl = false, have_blue = false;
-
-  float* d_weather = nullptr;
-  uint32_t weather_w = 0, weather_h = 0;
-  uint8_t* d_type = nullptr;
-  uint32_t type_w = 0, type_h = 0;
-  std::vector<uint16_t> h_wind;    // 32x16x32 RGBA16F
-
-  float4* d_lut[4] = {nullptr, nullptr, nullptr, nullptr};  // float4 copies
-  uint16_t* d_lut_h[4] = {nullptr, nullptr, nullptr, nullptr};  // RGBA16F bake outputs
-  bool have_lut[4] = {false, false, false, false};
-
-  // texture-unit path
-  cudaArray_t arr_base = nullptr, arr_detail = nullptr;
-  cudaTextureObject_t tex_base = 0, tex_detail = 0;
-  bool tex_dirty = true;
-
-  uint64_t launches = 0;
-
-  // batching (psc_render_batch)
-  PscBatchTuning batch_tuning{128, 16, 0, 0};
-  uint32_t batch_cap_views = 0, batch_cap_tiles = 0;
-  psc::MarchUniforms* d_bu = nullptr;   // per-view uniform blocks
-  psc::ViewDev* d_bv = nullptr;
-  void* d_bframes = nullptr;            // per-view frame records for the LUT bakes
-  float4* d_bsky = nullptr;             // per-view sky-view LUTs
-  float4* d_bap = nullptr;              // per-view aerial-perspective LUTs
-  uint32_t* d_btiles = nullptr;
-  uint32_t* d_bcounter = nullptr;
-  psc::MarchUniforms* h_bu = nullptr;   // pinned staging
-  psc::ViewDev* h_bv = nullptr;
-  void* h_bframes = nullptr;
-  uint32_t* h_btiles = nullptr;
-  cudaEvent_t batch_staged = nullptr;   // staging consumed by the last enqueue
-  cudaStream_t batch_stream = nullptr;  // capture stream
-  cudaGraphExec_t batch_exec = nullptr;
-  std::vector<uint64_t> batch_key;
-  int sms = 0;
-};
 
 namespace {
 
@@ -140,14 +103,6 @@ const uint32_t kLutH[4] = {64, 32, 108, 32};
 const uint32_t kLutD[4] = {1, 1, 1, 64};
 
 size_t lut_texels(int k) { return (size_t)kLutW[k] * kLutH[k] * kLutD[k]; }
-
-int ensure_device(psc_ctx* c) {
-  int n = 0;
-  PSC_CUDA(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
-  if (c->device >= n) return fail(PSC_ERR_INVALID_ARGUMENT, "device %d not in [0,%d)", c->device, n);
-  PSC_CUDA(cudaSetDevice(c->device), "cudaSetDevice");
-  return PSC_OK;
-}
 
 int validate_params(const PscCloudParamsGpu& p) {
   const float* f = reinterpret_cast<const float*>(&p);
@@ -618,6 +573,108 @@ int upload_lut_float4(psc_ctx* c, int kind, const uint16_t* h16) {
 }
 
 }  // namespace
+
+namespace psc {
+namespace host {
+
+int validate_batch(psc_ctx* c, const PscBatchView* views, uint32_t n) {
+  if (!c->have_base || !c->have_detail || !c->have_curl || !c->have_blue)
+    return fail(PSC_ERR_MISSING_INPUT, "noise volumes missing (psc_bake_noise or psc_upload_noise)");
+  if (!c->d_weather) return fail(PSC_ERR_MISSING_INPUT, "weather map missing (psc_upload_weather)");
+  if (!c->d_lut_h[PSC_LUT_TRANSMITTANCE] || !c->d_lut_h[PSC_LUT_MULTISCATTER] || !c->have_lut[PSC_LUT_TRANSMITTANCE])
+    return fail(PSC_ERR_MISSING_INPUT, "transmittance/multi-scatter LUTs missing (psc_bake_luts or psc_upload_lut)");
+  if (c->opts.schedule != PSC_SCHED_FAST)
+    return fail(PSC_ERR_UNSUPPORTED, "the batched kernel implements the FAST schedule (options.schedule)");
+  for (uint32_t i = 0; i < n; ++i) {
+    const PscBatchView& v = views[i];
+    if (!v.width || !v.height || v.width > 32768 || v.height > 32768)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "batch view %u: size %ux%u out of range", i, v.width, v.height);
+    if (!v.out_luminance && !v.out_transmittance && !(c->opts.composite && v.hdr))
+      return fail(PSC_ERR_INVALID_ARGUMENT, "batch view %u has no output buffer", i);
+    if (c->opts.composite && !v.hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "batch view %u: composite needs hdr", i);
+    int rc = validate_layers(v.layers, v.n_layers);
+    if (rc) return fail(rc, "batch view %u: %s", i, g_last_error.c_str());
+    PscCloudParamsGpu p = v.params;
+    p.cloud_layer_count = v.n_layers;
+    rc = validate_params(p);
+    if (rc) return fail(rc, "batch view %u: %s", i, g_last_error.c_str());
+    if (p.multi_scatter_octaves == 0 || p.multi_scatter_octaves > 4)
+      return fail(PSC_ERR_UNSUPPORTED, "batch view %u: the batched kernel handles 1..4 octaves", i);
+    const float* ff = reinterpret_cast<const float*>(&v.frame);
+    for (size_t k = 0; k < sizeof(v.frame) / 4; ++k)
+      if (k != 94 && !std::isfinite(ff[k])) return fail(PSC_ERR_NOT_FINITE, "batch view %u: frame word %zu", i, k);
+  }
+  return PSC_OK;
+}
+
+uint64_t count_batch_tiles(const PscBatchView* views, uint32_t n, const PscBatchTuning& tu) {
+  const uint32_t tile_w = tu.tile_w, tile_h = (tu.threads / 32 / (tu.tile_w / 8)) * 4;
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint64_t tx = (views[i].width + tile_w - 1) / tile_w, ty = (views[i].height + tile_h - 1) / tile_h;
+    if (tx > 4096 || ty > 4096) return UINT64_MAX;
+    total += tx * ty;
+  }
+  return total;
+}
+
+// Same records and tile order as the allocating batch path, written into
+// caller-provided host arrays with no heap use (n <= PSC_MAX_BATCH_VIEWS;
+// the view order is a stable insertion sort).
+int fill_batch(const psc_ctx* c, const PscBatchView* views, uint32_t n, const PscBatchTuning& tu,
+               MarchUniforms* hu, ViewDev* hv, void* hframes, uint32_t* htiles, uint32_t max_tiles,
+               float4* sky, float4* ap, uint32_t* n_tiles_out) {
+  const uint32_t tile_w = tu.tile_w, tile_h = (tu.threads / 32 / (tu.tile_w / 8)) * 4;
+  const size_t fl = psc::frame_lite_size();
+  for (uint32_t i = 0; i < n; ++i) {
+    const PscBatchView& bv = views[i];
+    PscCloudParamsGpu p = bv.params;
+    p.cloud_layer_count = bv.n_layers;
+    PscCloudLayerGpu layers[8];
+    std::memset(layers, 0, sizeof(layers));
+    for (uint32_t l = 0; l < bv.n_layers; ++l) layers[l] = bv.layers[l];
+    build_uniforms_for(c, p, layers, bv.frame, bv.width, bv.height, hu[i]);
+    hu[i].lut_sky = sky + (size_t)i * PSC_SKYVIEW_W * PSC_SKYVIEW_H;
+    hu[i].lut_ap = ap + (size_t)i * PSC_AP_W * PSC_AP_H * PSC_AP_D;
+    hv[i] = psc::ViewDev{bv.width, bv.height, 0, 0, bv.depth, reinterpret_cast<float4*>(bv.out_luminance),
+                         reinterpret_cast<float4*>(bv.out_transmittance), reinterpret_cast<float4*>(bv.hdr)};
+    psc::frame_lite_from(bv.frame, static_cast<char*>(hframes) + i * fl);
+  }
+  auto cost = [&](uint32_t i) {
+    return (double)views[i].params.cloud_steps * (double)std::max<uint32_t>(views[i].n_layers, 1);
+  };
+  auto before = [&](uint32_t a, uint32_t b) {
+    const double ca = cost(a), cb = cost(b);
+    if (ca != cb) return ca > cb;
+    return (uint64_t)views[a].width * views[a].height > (uint64_t)views[b].width * views[b].height;
+  };
+  uint32_t order[PSC_MAX_BATCH_VIEWS];
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t j = i;
+    for (; j > 0 && before(i, order[j - 1]); --j) order[j] = order[j - 1];
+    order[j] = i;
+  }
+  uint32_t k = 0;
+  for (uint32_t oi = 0; oi < n; ++oi) {
+    const uint32_t i = order[oi];
+    const uint32_t tx = (views[i].width + tile_w - 1) / tile_w, ty = (views[i].height + tile_h - 1) / tile_h;
+    if ((uint64_t)k + (uint64_t)tx * ty > max_tiles)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "batch needs more than %u tiles", max_tiles);
+    for (uint32_t y = 0; y < ty; ++y)
+      for (uint32_t x = 0; x < tx; ++x) htiles[k++] = (i << 24) | (x << 12) | y;
+  }
+  *n_tiles_out = k;
+  return PSC_OK;
+}
+
+bool storage_ready(const psc_ctx* c) {
+  const bool store = c->d_base_store && c->d_detail_store && c->store_form == (int)c->opts.storage;
+  const bool tex = c->opts.filter == PSC_FILTER_EXACT || (!c->tex_dirty && c->tex_base && c->tex_detail);
+  return store && tex;
+}
+
+}  // namespace host
+}  // namespace psc
 
 extern "C" {
 
