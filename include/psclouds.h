@@ -443,6 +443,55 @@ int psc_render_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, void* 
 int psc_autotune_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, uint32_t reps,
                        PscBatchTuning* best, float* best_ms, void* stream);
 
+/* ------------------------------------------ voxel-grid density, adjoint */
+
+/* A voxel density source for the differentiable form of the march.  New in
+ * this library: the reference's clouds are procedural only (sample_density,
+ * shaders/clouds/cloud_march.wgsl:432-530).  The grid replaces the density of
+ * the context's single layer (layer 0 gives the altitude range base_m..top_m,
+ * droplet size and type; CloudParams give scattering, phase, octaves,
+ * powder, ambient and the step counts), and the march differs from the
+ * procedural one in three stated ways: every primary step contributes (no
+ * density > 1e-3 gate, so the image is a smooth function of the grid), the
+ * step integral is (1 - exp(-x)) / x without the 1e-6 floor, and no aerial
+ * perspective is applied.  Cells are trilinearly interpolated between cell
+ * centres and read as zero outside the grid.  Values are mean extinction
+ * coefficients in 1/m: density = density_scale * value * 3 / (sigma_t.r +
+ * sigma_t.g + sigma_t.b) with sigma_t the layer's (sigma_s + sigma_a) x
+ * chromatic modulation, so the RGB-mean extinction equals
+ * density_scale * value. */
+typedef struct PscDensityGrid {
+  const float* values;          /* ny x nz x nx FP32, x fastest, then z, then altitude */
+  uint32_t nx, ny, nz;          /* cells along world x (east), altitude, world z (south) */
+  uint32_t checkpoint_every;    /* psc_adjoint: transmittance checkpoint interval, 1..32 steps */
+  float min_x_m, min_z_m;       /* world x / z of the grid's low corner */
+  float size_x_m, size_z_m;     /* horizontal extent (altitude extent: layer 0 base..top) */
+  float density_scale;          /* multiplies every value */
+  float exit_transmittance;     /* stop once max(T) < this; 0.01 as the march, 0 = never */
+} PscDensityGrid;
+
+#define PSC_GRID_MAX_CHECKPOINTS 32u
+
+/* Forward march of the grid form for each view (device `values`);
+ * outputs as psc_render (luminance, transmittance, optional composite).
+ * Needs the frame, blue noise and the transmittance and sky-view LUTs. */
+int psc_render_grid(psc_ctx* ctx, const PscDensityGrid* grid, const PscView* view, void* stream);
+
+/* Gradient of an image loss with respect to the grid values and
+ * density_scale.  The image is I = L + background * T per pixel and channel
+ * (the composite over `background`), the loss is
+ * sum((I - target)^2) / (3 * viewport_w * viewport_h), summed over the
+ * view's rectangle, so row bands of one viewport add up to the whole
+ * image's loss and gradient.  `background` and `target` are device float4
+ * per pixel of the rectangle.  The march keeps transmittance at every
+ * `checkpoint_every`-th step and recomputes the steps between checkpoints
+ * in the reverse sweep.  Results are ADDED to `grad_values` (device, same
+ * shape as the grid), `*grad_density_scale` and `*loss` (device doubles),
+ * so callers zero them first; view outputs, if given, receive L and T. */
+int psc_adjoint(psc_ctx* ctx, const PscDensityGrid* grid, const PscView* view,
+                const float* background, const float* target, float* grad_values,
+                double* grad_density_scale, double* loss, void* stream);
+
 /* ------------------------------------------------ allocation-free batch */
 
 #define PSC_NOALLOC_MAX_VIEWS 64u
@@ -488,6 +537,7 @@ int psc_render_batch_noalloc(psc_ctx* ctx, const PscBatchView* views, uint32_t n
 } /* extern "C" */
 
 static_assert(sizeof(PscCloudParamsGpu) == 112, "CloudParamsGpu is 112 B");
+static_assert(sizeof(PscDensityGrid) == 48, "PscDensityGrid layout");
 static_assert(sizeof(PscBatchView) == 448 + 112 + 384 + 16 + 32, "PscBatchView layout");
 static_assert(sizeof(PscCloudLayerGpu) == 48, "CloudLayerGpu is 48 B");
 static_assert(sizeof(PscFrameUniformsGpu) == 448, "FrameUniformsGpu is 448 B");

@@ -123,6 +123,33 @@ int oracle_render_pixel(const OracleScene* scene, uint32_t width,
                         int precision, int filter, double* lum4,
                         double* trans4);
 
+/* ---- voxel-grid form (no reference counterpart; see oracle_grid.cpp) ----
+ * Images are width x height = the scene's viewport; bg / target are
+ * width*height*4 floats; the loss is sum((L + bg*T - target)^2) / (3*w*h). */
+int oracle_grid_render(const OracleScene* scene, const PscDensityGrid* grid,
+                       uint32_t width, uint32_t height, int precision,
+                       int threads, float* out_lum, float* out_trans);
+/* FP64 loss over the listed pixel indices (y*width + x); NULL = all. */
+int oracle_grid_loss(const OracleScene* scene, const PscDensityGrid* grid,
+                     uint32_t width, uint32_t height, const float* bg,
+                     const float* target, const uint32_t* pixels,
+                     uint32_t n_pixels, int threads, double* loss);
+/* FP64 reverse-mode gradient (all steps stored, no checkpoints) of the
+ * loss terms of rows [row0, row1) (row1 = 0: all rows); the normalisation
+ * stays the whole image's, so row bands add up. */
+int oracle_grid_adjoint(const OracleScene* scene, const PscDensityGrid* grid,
+                        uint32_t width, uint32_t height, const float* bg,
+                        const float* target, uint32_t row0, uint32_t row1,
+                        int threads, double* grad, double* grad_density_scale,
+                        double* loss);
+/* Central differences of the FP64 loss for each listed voxel index, over
+ * the pixels whose samples touch that voxel (their count per voxel goes to
+ * n_pixels_out if not NULL). */
+int oracle_grid_fd(const OracleScene* scene, const PscDensityGrid* grid,
+                   uint32_t width, uint32_t height, const float* bg,
+                   const float* target, const uint64_t* voxels, uint32_t n_vox,
+                   double eps, int threads, double* out, uint32_t* n_pixels_out);
+
 /* `dst = L + dst*T` per channel (cloud_composite.wgsl + blend One/Src1). */
 int oracle_composite(const float* lum, const float* trans, float* hdr,
                      uint32_t n_pixels);

@@ -75,6 +75,12 @@ def lib() -> C.CDLL:
             ("oracle_render", [vp, u32, u32, C.c_int, C.c_int, C.c_int, u32, u32, vp, vp, vp], C.c_int),
             ("oracle_render_pixel", [vp, u32, u32, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
             ("oracle_composite", [vp, vp, vp, u32], C.c_int),
+            ("oracle_grid_render", [vp, vp, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
+            ("oracle_grid_loss", [vp, vp, u32, u32, vp, vp, vp, u32, C.c_int, vp], C.c_int),
+            ("oracle_grid_adjoint", [vp, vp, u32, u32, vp, vp, u32, u32, C.c_int, vp, vp, vp],
+             C.c_int),
+            ("oracle_grid_fd", [vp, vp, u32, u32, vp, vp, vp, u32, C.c_double, C.c_int, vp, vp],
+             C.c_int),
         ]:
             fn = getattr(L, name)
             fn.argtypes, fn.restype = args, res
@@ -174,3 +180,86 @@ def composite(L, T, bg):
                                _p(np.ascontiguousarray(T, np.float32)), _p(out),
                                out.size // 4), "composite")
     return out
+
+
+# ---- voxel-grid form (oracle_grid.cpp) ----
+
+def grid_struct(values: np.ndarray, spec: dict) -> capi.DensityGrid:
+    """PscDensityGrid over a host (ny, nz, nx) float32 array; `spec` holds
+    min_x_m, min_z_m, size_x_m, size_z_m, density_scale, exit_transmittance,
+    checkpoint_every."""
+    ny, nz, nx = values.shape
+    return capi.DensityGrid(values.ctypes.data, nx, ny, nz, spec.get("checkpoint_every", 16),
+                            spec["min_x_m"], spec["min_z_m"], spec["size_x_m"], spec["size_z_m"],
+                            spec["density_scale"], spec["exit_transmittance"])
+
+
+def _grid_args(scene, noise, luts, values, spec):
+    s, keep = make_scene(scene, noise, luts)
+    v = np.ascontiguousarray(values, np.float32)
+    keep.append(v)
+    g = grid_struct(v, spec)
+    return s, g, keep
+
+
+def grid_render(scene, noise, luts, values, spec, precision=FP64, threads=0):
+    s, g, keep = _grid_args(scene, noise, luts, values, spec)
+    w, h = scene.width, scene.height
+    L = np.zeros((h, w, 4), np.float32)
+    T = np.zeros((h, w, 4), np.float32)
+    _ok(lib().oracle_grid_render(C.byref(s), C.byref(g), w, h, precision, threads, _p(L), _p(T)),
+        "oracle_grid_render")
+    del keep
+    return L, T
+
+
+def grid_loss(scene, noise, luts, values, spec, bg, target, pixels=None, threads=0) -> float:
+    s, g, keep = _grid_args(scene, noise, luts, values, spec)
+    bg = np.ascontiguousarray(bg, np.float32)
+    target = np.ascontiguousarray(target, np.float32)
+    px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    out = C.c_double()
+    _ok(lib().oracle_grid_loss(C.byref(s), C.byref(g), scene.width, scene.height, _p(bg),
+                               _p(target), _p(px), 0 if px is None else px.size, threads,
+                               C.byref(out)), "oracle_grid_loss")
+    del keep
+    return out.value
+
+
+def grid_adjoint(scene, noise, luts, values, spec, bg, target, threads=0, rows=None):
+    """FP64 reverse-mode gradient: (grad (ny, nz, nx) float64, d/d density_scale, loss),
+    of rows [r0, r1) if `rows` is given."""
+    s, g, keep = _grid_args(scene, noise, luts, values, spec)
+    bg = np.ascontiguousarray(bg, np.float32)
+    target = np.ascontiguousarray(target, np.float32)
+    grad = np.zeros(values.shape, np.float64)
+    gs, loss = C.c_double(), C.c_double()
+    r0, r1 = rows if rows else (0, 0)
+    _ok(lib().oracle_grid_adjoint(C.byref(s), C.byref(g), scene.width, scene.height, _p(bg),
+                                  _p(target), r0, r1, threads, _p(grad), C.byref(gs),
+                                  C.byref(loss)),
+        "oracle_grid_adjoint")
+    del keep
+    return grad, gs.value, loss.value
+
+
+def grid_fd(scene, noise, luts, values, spec, bg, target, voxels, eps=1e-3, threads=0):
+    """Central differences of the FP64 loss at flat voxel indices: (fd, pixels touched)."""
+    s, g, keep = _grid_args(scene, noise, luts, values, spec)
+    bg = np.ascontiguousarray(bg, np.float32)
+    target = np.ascontiguousarray(target, np.float32)
+    vox = np.ascontiguousarray(voxels, np.uint64)
+    out = np.zeros(vox.size, np.float64)
+    npx = np.zeros(vox.size, np.uint32)
+    _ok(lib().oracle_grid_fd(C.byref(s), C.byref(g), scene.width, scene.height, _p(bg), _p(target),
+                             _p(vox), vox.size, eps, threads, _p(out), _p(npx)), "oracle_grid_fd")
+    del keep
+    return out, npx
+
+
+def grid_fd_richardson(scene, noise, luts, values, spec, bg, target, voxels, eps, threads=0):
+    """Central differences at eps and eps/2 combined as (4 D(eps/2) - D(eps)) / 3,
+    which cancels the eps^2 truncation term: (extrapolated, D(eps), pixels touched)."""
+    d1, npx = grid_fd(scene, noise, luts, values, spec, bg, target, voxels, eps, threads)
+    d2, _ = grid_fd(scene, noise, luts, values, spec, bg, target, voxels, eps / 2, threads)
+    return (4.0 * d2 - d1) / 3.0, d1, npx

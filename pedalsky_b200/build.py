@@ -28,6 +28,7 @@ CUDA_UNITS = {
     "march_fast.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "march_batch.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "march_noalloc.cu": [],
+    "grid_march.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
 }

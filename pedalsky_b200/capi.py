@@ -139,6 +139,16 @@ class BatchTuning(C.Structure):
     _fields_ = [("threads", u32), ("tile_w", u32), ("use_graph", u32), ("_reserved", u32)]
 
 
+class DensityGrid(C.Structure):
+    _fields_ = [("values", C.c_void_p), ("nx", u32), ("ny", u32), ("nz", u32),
+                ("checkpoint_every", u32), ("min_x_m", C.c_float), ("min_z_m", C.c_float),
+                ("size_x_m", C.c_float), ("size_z_m", C.c_float), ("density_scale", C.c_float),
+                ("exit_transmittance", C.c_float)]
+
+
+assert C.sizeof(DensityGrid) == 48
+
+
 class PscError(RuntimeError):
     def __init__(self, code: int, func: str, msg: str):
         super().__init__(f"{func}: {PSC_ERR.get(code, code)} ({code}): {msg}")
@@ -185,6 +195,8 @@ _PROTOS = {
     "psc_render_batch": [_vp, P(BatchView), u32, _vp],
     "psc_render_batch_noalloc": [_vp, P(BatchView), u32, _vp, _vp, _vp],
     "psc_autotune_batch": [_vp, P(BatchView), u32, u32, P(BatchTuning), P(C.c_float), _vp],
+    "psc_render_grid": [_vp, P(DensityGrid), P(View), _vp],
+    "psc_adjoint": [_vp, P(DensityGrid), P(View), _vp, _vp, _vp, _vp, _vp, _vp],
 }
 _RESTYPES = {
     "psc_last_error": C.c_char_p, "psc_abi_version": u32, "psc_sizeof_params": C.c_size_t,

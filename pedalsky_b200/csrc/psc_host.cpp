@@ -1481,6 +1481,120 @@ int psc_autotune_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32
   return PSC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Inputs, grid description and view checks of the voxel-grid form; fills
+// the uniforms, view record and grid record for the launch.
+int prepare_grid(psc_ctx* c, const PscDensityGrid* g, const PscView* v, bool adjoint,
+                 psc::MarchUniforms& u, psc::ViewDev& vd, psc::GridDev& gd) {
+  if (!c || !g || !v) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (!c->have_frame) return fail(PSC_ERR_MISSING_INPUT, "psc_set_frame was not called");
+  if (!c->have_blue) return fail(PSC_ERR_MISSING_INPUT, "blue noise missing (psc_bake_noise or psc_upload_noise)");
+  if (!c->have_lut[PSC_LUT_TRANSMITTANCE] || !c->have_lut[PSC_LUT_SKYVIEW])
+    return fail(PSC_ERR_MISSING_INPUT, "transmittance/sky-view LUTs missing (psc_upload_lut or psc_bake_luts)");
+  int rc = validate_params(c->params);
+  if (rc) return rc;
+  if (c->n_layers != 1) return fail(PSC_ERR_LAYERS, "the grid form takes exactly one layer (got %u)", c->n_layers);
+  if (c->params.cone_light_sampling)
+    return fail(PSC_ERR_UNSUPPORTED, "the grid form marches the straight light path (cone sampling off)");
+  if (c->params.multi_scatter_octaves == 0 || c->params.multi_scatter_octaves > 4)
+    return fail(PSC_ERR_UNSUPPORTED, "the grid form handles 1..4 octaves");
+  if (!g->values) return fail(PSC_ERR_INVALID_ARGUMENT, "grid values are null");
+  if (!g->nx || !g->ny || !g->nz || (uint64_t)g->nx * g->ny * g->nz > 0x7fffffffull)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "grid of %ux%ux%u cells out of range", g->nx, g->ny, g->nz);
+  const float fields[] = {g->min_x_m, g->min_z_m, g->size_x_m, g->size_z_m, g->density_scale,
+                          g->exit_transmittance};
+  for (float f : fields)
+    if (!std::isfinite(f)) return fail(PSC_ERR_NOT_FINITE, "grid field is not finite");
+  if (g->size_x_m <= 0.0f || g->size_z_m <= 0.0f)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "grid extent must be positive");
+  if (g->exit_transmittance < 0.0f || g->exit_transmittance >= 1.0f)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "exit_transmittance must be in [0, 1)");
+  if (adjoint) {
+    const uint32_t k = g->checkpoint_every;
+    if (k == 0 || k > 32)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "checkpoint_every must be 1..32 (got %u)", k);
+    if ((c->params.cloud_steps + k - 1) / k > PSC_GRID_MAX_CHECKPOINTS)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "%u steps need more than %u checkpoints at interval %u",
+                  c->params.cloud_steps, PSC_GRID_MAX_CHECKPOINTS, k);
+  }
+  if (!v->width || !v->height || v->width > 32768 || v->height > 32768)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "view size %ux%u out of range", v->width, v->height);
+  const uint32_t vw = v->viewport_w ? v->viewport_w : v->width, vh = v->viewport_h ? v->viewport_h : v->height;
+  if ((!v->viewport_w && v->x_offset) || (!v->viewport_h && v->y_offset) || vw > 32768 || vh > 32768 ||
+      (uint64_t)v->x_offset + v->width > vw || (uint64_t)v->y_offset + v->height > vh)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "view rectangle %ux%u at (%u,%u) exceeds viewport %ux%u", v->width,
+                v->height, v->x_offset, v->y_offset, vw, vh);
+  if (!adjoint && !v->out_luminance && !v->out_transmittance && !(c->opts.composite && v->hdr))
+    return fail(PSC_ERR_INVALID_ARGUMENT, "view has no output buffer");
+  if (!adjoint && c->opts.composite && !v->hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "composite needs hdr");
+  rc = ensure_device(c);
+  if (rc) return rc;
+  build_uniforms(c, vw, vh, u);
+  vd = psc::ViewDev{v->width, v->height, v->x_offset, v->y_offset, v->depth,
+                    reinterpret_cast<float4*>(v->out_luminance), reinterpret_cast<float4*>(v->out_transmittance),
+                    reinterpret_cast<float4*>(v->hdr)};
+  const psc::LayerConst& L = u.layers[0];
+  const float sig = L.sigma_t[0] + L.sigma_t[1] + L.sigma_t[2];
+  if (!(sig > 0.0f)) return fail(PSC_ERR_INVALID_ARGUMENT, "layer extinction must be positive");
+  gd = psc::GridDev{};
+  gd.values = g->values;
+  gd.nx = g->nx;
+  gd.ny = g->ny;
+  gd.nz = g->nz;
+  gd.k_cp = g->checkpoint_every;
+  gd.min_x = g->min_x_m;
+  gd.min_z = g->min_z_m;
+  gd.base = L.base_m;
+  gd.inv_cell_x = (float)g->nx / g->size_x_m;
+  gd.inv_cell_z = (float)g->nz / g->size_z_m;
+  gd.inv_cell_y = (float)g->ny / std::max(L.top_m - L.base_m, 1.0f);
+  gd.inv_sigma_bar = 3.0f / sig;
+  gd.k = g->density_scale * gd.inv_sigma_bar;
+  gd.exit_t = g->exit_transmittance;
+  gd.inv_n = (float)(1.0 / (3.0 * (double)vw * (double)vh));
+  return PSC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psc_render_grid(psc_ctx* c, const PscDensityGrid* g, const PscView* v, void* stream) {
+  psc::MarchUniforms u;
+  psc::ViewDev vd;
+  psc::GridDev gd;
+  int rc = prepare_grid(c, g, v, false, u, vd, gd);
+  if (rc) return rc;
+  rc = psc::launch_grid_march(u, vd, gd, false, static_cast<cudaStream_t>(stream));
+  if (rc) return fail(rc, "grid march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  ++c->launches;
+  return PSC_OK;
+}
+
+int psc_adjoint(psc_ctx* c, const PscDensityGrid* g, const PscView* v, const float* background,
+                const float* target, float* grad_values, double* grad_density_scale, double* loss,
+                void* stream) {
+  if (!background || !target || !grad_values || !grad_density_scale || !loss)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "null adjoint buffer");
+  psc::MarchUniforms u;
+  psc::ViewDev vd;
+  psc::GridDev gd;
+  int rc = prepare_grid(c, g, v, true, u, vd, gd);
+  if (rc) return rc;
+  gd.grad = grad_values;
+  gd.bg = reinterpret_cast<const float4*>(background);
+  gd.target = reinterpret_cast<const float4*>(target);
+  gd.loss = loss;
+  gd.grad_scale = grad_density_scale;
+  rc = psc::launch_grid_march(u, vd, gd, true, static_cast<cudaStream_t>(stream));
+  if (rc) return fail(rc, "adjoint launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  ++c->launches;
+  return PSC_OK;
+}
+
 int psc_launch_count(psc_ctx* c, uint64_t* out) {
   if (!c || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
   *out = c->launches;

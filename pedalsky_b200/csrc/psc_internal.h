@@ -118,6 +118,26 @@ struct ViewDev {
   float4* hdr;
 };
 
+// Voxel-grid density source of the differentiable form (grid_march.cu).
+struct GridDev {
+  const float* values;     // ny x nz x nx, x fastest
+  float* grad;             // adjoint: d loss / d values (accumulated)
+  uint32_t nx, ny, nz;
+  uint32_t k_cp;           // adjoint checkpoint interval (steps)
+  float min_x, min_z, base;
+  float inv_cell_x, inv_cell_y, inv_cell_z;
+  float k;                 // density = k * value (density_scale * inv_sigma_bar)
+  float inv_sigma_bar;     // 3 / (sigma_t.r + sigma_t.g + sigma_t.b) of layer 0
+  float exit_t;            // early exit once max(T) < exit_t
+  float inv_n;             // 1 / (3 * viewport pixels)
+  const float4* bg;        // adjoint: background per pixel of the view
+  const float4* target;    // adjoint: target image per pixel of the view
+  double* loss;            // adjoint: accumulated loss
+  double* grad_scale;      // adjoint: accumulated d loss / d density_scale
+};
+int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g, bool adjoint,
+                      cudaStream_t stream);
+
 // Launchers (march.cu).
 int launch_march(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
                  cudaStream_t stream);

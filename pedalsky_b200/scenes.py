@@ -18,6 +18,8 @@ Workloads:
                   Cirrus 8000-9000 (0.3), 1920x1080, 128/6 steps
   stress_2160p    Cumulonimbus 600-12000 m, coverage 0.8, 2048^2 f32
                   coverage grid, 3840x2160, 256/8 steps, 15 m/s wind
+  grid_512        256x256x64 Worley voxel grid over 20x20x2 km from 1500 m,
+                  512x512, 96/6 steps (the differentiable form)
 """
 from __future__ import annotations
 
@@ -355,10 +357,55 @@ def batch_views(n=64, seed=0, size_scale=1.0, host_inputs=True, **kw) -> list[Sc
     return out
 
 
+def worley_grid(nx=256, ny=64, nz=256, extent=(20000.0, 2000.0, 20000.0), seed=0, n_points=48,
+                radius_m=1100.0, flatten=2.5, vmax=0.05):
+    """Seeded Worley-thresholded voxel density, shape (ny, nz, nx), values in
+    [0, vmax] 1/m: vmax * clamp(1 - F1 / radius, 0, 1), F1 the distance from
+    the cell centre to the nearest of `n_points` uniformly placed feature
+    points, with vertical distances scaled by `flatten` (flat-based blobs)."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed)
+    ex, ey, ez = extent
+    pts = rng.uniform((0.0, 0.0, 0.0), (ex, ey, ez), size=(n_points, 3))
+    pts[:, 1] *= flatten
+    xs = (np.arange(nx) + 0.5) * (ex / nx)
+    ys = (np.arange(ny) + 0.5) * (ey / ny) * flatten
+    zs = (np.arange(nz) + 0.5) * (ez / nz)
+    Y, Z, X = np.meshgrid(ys, zs, xs, indexing="ij")
+    f1, _ = cKDTree(pts).query(np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1))
+    v = vmax * np.clip(1.0 - f1 / radius_m, 0.0, 1.0)
+    return v.reshape(ny, nz, nx).astype(np.float32)
+
+
+def grid_target_values(values: np.ndarray, seed=1, rel=0.05) -> np.ndarray:
+    """The grid perturbed by `rel` relative Gaussian noise (the target's density)."""
+    rng = np.random.default_rng(seed)
+    return np.clip(values * (1.0 + rel * rng.standard_normal(values.shape)), 0.0, None).astype(np.float32)
+
+
+def grid_512(width=512, height=512, seed=0, grid_shape=(256, 64, 256), steps=96, **kw) -> Scene:
+    """Voxel-grid scene: (nx, ny, nz) cells over 20 x 20 km from -10 km, 1500-3500 m
+    altitude (one Cumulus layer supplies droplet size and type), camera at
+    100 m pitched up 55 deg with a 60 deg field of view, `steps` + 6 steps."""
+    p = default_params()
+    p.cloud_steps, p.light_steps = steps, 6
+    ln = synth_layers([(0, 1500.0, 3500.0, 0.5)])
+    frame = frame_for(width, height, pitch_deg=55.0, fov_deg=60.0)
+    s = _finish("grid_512", width, height, p, ln, frame, options(**kw), reference_weather(ln[1]),
+                128, 128, capi.WEATHER_RGBA16F, with_ground=False)
+    nx, ny, nz = grid_shape
+    s.extra["grid"] = worley_grid(nx, ny, nz, seed=seed)
+    s.extra["grid_spec"] = dict(min_x_m=-10000.0, min_z_m=-10000.0, size_x_m=20000.0,
+                                size_z_m=20000.0, density_scale=1.0, exit_transmittance=0.01,
+                                checkpoint_every=16)
+    return s
+
+
 WORKLOADS = {
     "plain_320x180": plain_320x180,
     "plain_literal": plain_literal,
     "precision_1080p": precision_1080p,
     "stress_2160p": stress_2160p,
     "batch_64": batch_views,
+    "grid_512": grid_512,
 }

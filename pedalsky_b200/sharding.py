@@ -89,3 +89,15 @@ def max_over_ranks(value: float, device=None, group=None) -> float:
     if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+def allreduce_gradient(grad, acc, group=None):
+    """The adjoint's exchange step: pixels are sharded by row bands, so each
+    rank holds a partial d loss / d grid (and its share of the loss and of
+    d loss / d density_scale in `acc`); one sum all-reduce of each gives
+    every rank the whole image's values.  In place; a no-op on one rank."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+        dist.all_reduce(acc, op=dist.ReduceOp.SUM, group=group)
+    return grad, acc
