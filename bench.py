@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="precision_1080p", choices=["precision_1080p", "batch_64"],
+    ap.add_argument("--workload", default="precision_1080p",
+                    choices=["precision_1080p", "batch_64", "grid_512"],
                     help="batch_64: the 64-view uneven batch in one persistent kernel")
     ap.add_argument("--batch-views", type=int, default=64)
     return ap.parse_args()
@@ -164,10 +165,45 @@ def cpu_baseline(scene, sample_rows: int, reps: int = 1):
     return rays / float(np.median(times)), rays, threads, float(np.median(times))
 
 
+def run_reference_grid(args):
+    """CPU reference arm of the grid workload: the FP64 restatement's forward +
+    reverse sweep on a bounded row sample per step, all host threads."""
+    from oracle import pyoracle
+    from pedalsky_b200 import scenes
+    sc = scenes.grid_512()
+    noise = pyoracle.bake_noise()
+    luts = pyoracle.bake_luts(sc.frame, sc.world)
+    for _ in range(args.warmup):
+        grid_cpu_baseline(sc, noise, luts, 32)
+    vals = []
+    for _ in range(args.steps):
+        v, rays, threads, secs = grid_cpu_baseline(sc, noise, luts, 64)
+        vals.append(v)
+    value = float(np.median(vals)) / 1e6
+    line = {
+        "metric": GRID_METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sc.width * sc.height / (value * 1e6), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Worley grid)", "impl": "reference",
+        "config": {"workload": "grid_512", "grid": [256, 256, 64], "view": [sc.width, sc.height],
+                   "primary_steps": 96, "light_steps": 6,
+                   "note": "the reference has no voxel-grid form or adjoint; this is the CPU "
+                           "restatement (FP64 reverse sweep) on a row sample"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{rays} rays per step (4 row bands)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    if args.workload == "grid_512":
+        return run_reference_grid(args)
     from pedalsky_b200 import scenes
     s = scenes.precision_1080p(args.width, args.height)
     sample = 64  # rows per step
@@ -418,12 +454,197 @@ def run_batch(args):
     return 0
 
 
+GRID_METRIC = ("Mrays/s of the adjoint (forward + checkpointed reverse + gradient all-reduce), "
+               "512^2 view of a 256x256x64 voxel grid, 96+6 steps")
+
+
+def grid_bytes_per_ray() -> dict:
+    """Algorithmic bytes per ray of the grid forward and adjoint kernels from
+    the executed work counted by the CPU restatement (fetch_counts.json):
+    FP32 texels read by primary and light taps, two bilinear RGBA32F LUT taps
+    (sun transmittance, sky view) per step, the blue-noise load and the L/T
+    writes; the adjoint adds the segment recompute (texels again), the
+    reverse sweep's LUT taps, one 4-byte atomic add per texel and the
+    background/target reads."""
+    p = ROOT / "tests" / "golden" / "fetch_counts.json"
+    if not p.exists():
+        return {}
+    d = json.loads(p.read_text()).get("grid_512")
+    if not d:
+        return {}
+    c = d["counts"]
+    px = c["pixels"]
+    tex = 4 * (c["primary_texels"] + c["light_texels"])
+    lut = c["steps"] * 2 * 4 * 16
+    fwd = (tex + lut) / px + 4 + 32
+    adj = (3 * tex + 2 * lut) / px + 4 + 32 + 32
+    return {"forward": fwd, "adjoint": adj, "steps_per_ray": c["steps"] / px}
+
+
+def grid_cpu_baseline(sc, noise, luts, rows: int):
+    """FP64 CPU restatement of forward + reverse sweep on `rows` rows spread
+    over the view; returns (rays/s, rays, threads, seconds)."""
+    from oracle import pyoracle
+    G = sc.extra["grid"]
+    spec = sc.extra["grid_spec"]
+    bg = sc.background
+    tgt = np.ascontiguousarray(bg, np.float32)  # the timing does not depend on the target values
+    threads = os.cpu_count() or 1
+    band = max(1, rows // 4)
+    starts = np.linspace(0, sc.height - band, 4).astype(int)
+    t0 = time.perf_counter()
+    for r0 in starts:
+        pyoracle.grid_adjoint(sc, noise, luts, G, spec, bg, tgt, threads=threads,
+                              rows=(int(r0), int(r0) + band))
+    secs = time.perf_counter() - t0
+    rays = 4 * band * sc.width
+    return rays / secs, rays, threads, secs
+
+
+def run_grid(args):
+    """The differentiable form: one 512^2 view's loss gradient per step.  Pixels
+    are sharded in row bands over the ranks (strong scaling); each rank runs
+    its band's adjoint and one sum all-reduce (NCCL) of the 16 MiB gradient
+    grid gives every rank the whole image's gradient."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from pedalsky_b200 import grid as GR
+    from pedalsky_b200 import scenes, sharding
+    from pedalsky_b200.subsystem import subsystem_for_scene
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sc = scenes.grid_512()
+    W, H = sc.width, sc.height
+    G = sc.extra["grid"]
+    sub = subsystem_for_scene(sc, device=local, luts=None)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream
+    P = GR.GridProblem(sc, G, device=dev)
+    Pt = GR.GridProblem(sc, scenes.grid_target_values(G), device=dev)
+    with torch.cuda.stream(stream):
+        Pt.render(sub.handle, stream=sh)
+        P.set_target(Pt.composite_image())
+    torch.cuda.synchronize()
+    del Pt
+    band = sharding.row_bands(H, world)[rank]
+    rows = (band.y0, band.y1) if world > 1 else None
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        P.zero_grad()
+        P.adjoint(sub.handle, rows=rows, stream=sh)
+        sharding.allreduce_gradient(P.grad, P.acc)
+
+    def timed(fn, n):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(n)]
+        with torch.cuda.stream(stream):
+            for i in range(n):
+                flush.zero_()
+                evs[i][0].record(stream)
+                fn()
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        return ms, sharding.max_over_ranks(float(np.mean(ms)), device=dev)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = sub.launch_count()
+    with ClockSampler(local) as clk:
+        step_ms, ms = timed(step, args.steps)
+    launches = sub.launch_count() - launches0
+    value = W * H / (ms * 1e-3) / 1e6
+    fwd_ms_list, fwd_ms = timed(lambda: P.render(sub.handle, rows=rows, stream=sh), args.steps)
+    adj_only_ms_list, adj_ms = timed(lambda: (P.zero_grad(), P.adjoint(sub.handle, rows=rows, stream=sh)),
+                                     args.steps)
+
+    # end to end: the grid values go up from pinned host memory, the loss
+    # and the gradient come back
+    h_vals = torch.from_numpy(np.ascontiguousarray(G)).pin_memory()
+    h_grad = torch.empty_like(h_vals).pin_memory()
+    h_acc = torch.empty(2, dtype=torch.float64).pin_memory()
+
+    def e2e():
+        P.values.copy_(h_vals, non_blocking=True)
+        step()
+        h_grad.copy_(P.grad, non_blocking=True)
+        h_acc.copy_(P.acc, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            e2e()
+    _, e2e_ms = timed(e2e, args.steps)
+    if rank == 0:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        hbm = peaks.get("hbm_gbs")
+        peak = hbm if hbm else 6650.0
+        bpr = grid_bytes_per_ray()
+        roof = None
+        if bpr:
+            rays_rank = W * (band.y1 - band.y0)
+            ach = bpr["adjoint"] * rays_rank / (adj_ms * 1e-3) / 1e9
+            roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "traffic": None, "peak_source": "measured" if hbm else "fallback",
+                    "bytes_per_ray": bpr["adjoint"], "kernel": "k_grid_march<adjoint>",
+                    "note": "algorithmic bytes (texels, LUT taps, atomic adds); the grid and "
+                            "gradient (16 MiB each) are L2-resident"}
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            from oracle import pyoracle
+            noise = pyoracle.bake_noise()
+            luts = pyoracle.bake_luts(sc.frame, sc.world)
+            v, rays, threads, secs = grid_cpu_baseline(sc, noise, luts, 128)
+            cpu = {"value": v / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{rays} rays (4 row bands), FP64 forward + reverse sweep, {secs:.1f} s"}
+        line = {
+            "metric": GRID_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Worley grid; target = render of the grid with 5% noise)",
+            "config": {"workload": "grid_512", "grid": [256, 256, 64], "view": [W, H],
+                       "primary_steps": 96, "light_steps": 6, "checkpoint_every": 16,
+                       "exit_transmittance": 0.01,
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"rowbands{world} + all-reduce"},
+            "forward_only": {"value": W * H / (fwd_ms * 1e-3) / 1e6, "ms_per_step": fwd_ms},
+            "adjoint_kernel_ms": adj_ms,
+            "e2e": {"value": W * H / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
+                    "h2d_bytes_per_step": h_vals.numel() * 4,
+                    "d2h_bytes_per_step": h_grad.numel() * 4 + 16},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "step_ms": [round(x, 4) for x in step_ms],
+        }
+        print(json.dumps(line), flush=True)
+    sub.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch_64":
         return run_batch(args)
+    if args.workload == "grid_512":
+        return run_grid(args)
     return run_ours(args)
 
 

@@ -142,6 +142,12 @@ int oracle_grid_adjoint(const OracleScene* scene, const PscDensityGrid* grid,
                         const float* target, uint32_t row0, uint32_t row1,
                         int threads, double* grad, double* grad_density_scale,
                         double* loss);
+/* Executed work of the forward march: out[0] pixels, [1] pixels whose ray
+ * meets the grid layer, [2] primary steps, [3] in-grid texels read by the
+ * primary samples, [4] in-grid texels read by the light taps. */
+int oracle_grid_counts(const OracleScene* scene, const PscDensityGrid* grid,
+                       uint32_t width, uint32_t height, int threads,
+                       uint64_t* out);
 /* Central differences of the FP64 loss for each listed voxel index, over
  * the pixels whose samples touch that voxel (their count per voxel goes to
  * n_pixels_out if not NULL). */

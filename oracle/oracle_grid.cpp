@@ -435,6 +435,43 @@ int oracle_grid_adjoint(const OracleScene* s, const PscDensityGrid* g, uint32_t 
   return 0;
 }
 
+int oracle_grid_counts(const OracleScene* s, const PscDensityGrid* g, uint32_t w, uint32_t h,
+                       int threads, uint64_t* out) {
+  if (!grid_ok(s, g) || !out) return -1;
+  GridMarch<double> gm;
+  gm.init(s, g, g->values);
+  uint64_t steps = 0, prim = 0, light = 0, hit = 0;
+  const int nt = set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt) reduction(+ : steps, prim, light, hit)
+  for (int64_t y = 0; y < (int64_t)h; ++y) {
+    std::vector<GridMarch<double>::Rec> recs;
+    for (uint32_t x = 0; x < w; ++x) {
+      const auto r = gm.ray(x, (uint32_t)y, w, s->depth);
+      double Lo[3], To[3];
+      gm.forward(r, Lo, To, &recs);
+      hit += recs.empty() ? 0 : 1;
+      steps += recs.size();
+      for (const auto& q : recs) {
+        const Corners<double> cp = gm.corners(q.p.x, q.alt, q.p.z);
+        for (int i = 0; i < 8; ++i) prim += cp.idx[i] >= 0;
+        const double delta = gm.light_delta(q.alt);
+        for (uint32_t j = 0; j < gm.m.light_steps; ++j) {
+          double qx, qa, qz;
+          gm.light_tap(q.p, q.alt, delta, j, &qx, &qa, &qz);
+          const Corners<double> cl = gm.corners(qx, qa, qz);
+          for (int i = 0; i < 8; ++i) light += cl.idx[i] >= 0;
+        }
+      }
+    }
+  }
+  out[0] = (uint64_t)w * h;
+  out[1] = hit;
+  out[2] = steps;
+  out[3] = prim;
+  out[4] = light;
+  return 0;
+}
+
 int oracle_grid_fd(const OracleScene* s, const PscDensityGrid* g, uint32_t w, uint32_t h,
                    const float* bg, const float* tgt, const uint64_t* voxels, uint32_t n_vox,
                    double eps, int threads, double* out, uint32_t* n_pixels_out) {

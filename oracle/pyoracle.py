@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
              C.c_int),
             ("oracle_grid_fd", [vp, vp, u32, u32, vp, vp, vp, u32, C.c_double, C.c_int, vp, vp],
              C.c_int),
+            ("oracle_grid_counts", [vp, vp, u32, u32, C.c_int, vp], C.c_int),
         ]:
             fn = getattr(L, name)
             fn.argtypes, fn.restype = args, res
@@ -263,3 +264,14 @@ def grid_fd_richardson(scene, noise, luts, values, spec, bg, target, voxels, eps
     d1, npx = grid_fd(scene, noise, luts, values, spec, bg, target, voxels, eps, threads)
     d2, _ = grid_fd(scene, noise, luts, values, spec, bg, target, voxels, eps / 2, threads)
     return (4.0 * d2 - d1) / 3.0, d1, npx
+
+
+def grid_counts(scene, noise, luts, values, spec, threads=0) -> dict:
+    """Executed work of the grid forward march (see oracle_grid_counts)."""
+    s, g, keep = _grid_args(scene, noise, luts, values, spec)
+    out = np.zeros(5, np.uint64)
+    _ok(lib().oracle_grid_counts(C.byref(s), C.byref(g), scene.width, scene.height, threads,
+                                 _p(out)), "oracle_grid_counts")
+    del keep
+    return dict(zip(("pixels", "hit_pixels", "steps", "primary_texels", "light_texels"),
+                    (int(x) for x in out)))

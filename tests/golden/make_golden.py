@@ -3,8 +3,9 @@
   python tests/golden/make_golden.py
 
 fetch_counts.json  executed-fetch counts per kind (instrumented FP64 CPU
-                   restatement) for each benchmark workload; bench.py turns
-                   them into algorithmic bytes per ray.
+                   restatement) for each benchmark workload, the voxel-grid
+                   one included; bench.py turns them into algorithmic bytes
+                   per ray.
 plain_96x54.npz    FP64-oracle L/T of the plain workload at 96x54 (float32),
 precision_96x54.npz  and of the three-layer workload; the GPU parity tests
                    compare against these (they pin the oracle as well).
@@ -36,6 +37,11 @@ def main():
         _, _, c = pyoracle.render(s, noise, luts, precision=pyoracle.FP64, counters=True)
         counts[name] = {"width": s.width, "height": s.height, "counts": c}
         print(name, c)
+    s = scenes.grid_512()
+    luts = pyoracle.bake_luts(s.frame, s.world)
+    c = pyoracle.grid_counts(s, noise, luts, s.extra["grid"], s.extra["grid_spec"])
+    counts["grid_512"] = {"width": s.width, "height": s.height, "counts": c}
+    print("grid_512", c)
     (HERE / "fetch_counts.json").write_text(json.dumps(counts, indent=1) + "\n")
     for name, make in (("plain_96x54", lambda: scenes.plain_320x180(96, 54)),
                        ("precision_96x54", lambda: scenes.precision_1080p(96, 54))):
