@@ -24,7 +24,7 @@ __device__ __forceinline__ void unpack_tile(uint32_t w, uint32_t& view, uint32_t
 }
 
 template <int ST, int FILT, int NT>
-__global__ void __launch_bounds__(NT, 768 / NT)
+__global__ void __launch_bounds__(NT, 1024 / NT)
     k_march_batch(const MarchUniforms* __restrict__ views_u, const ViewDev* __restrict__ views_v,
                   const uint32_t* __restrict__ tiles, uint32_t n_tiles, uint32_t* __restrict__ counter,
                   uint32_t tile_w) {

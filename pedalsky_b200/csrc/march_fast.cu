@@ -1,5 +1,6 @@
 // Single-view FAST march kernel: one thread per ray, CTA tile 16x8 pixels,
-// warps as 8x4 pixel tiles, 6 CTAs per SM (<= 85 registers).  The per-ray
+// warps as 8x4 pixel tiles, 8 CTAs per SM (64 registers: more resident warps
+// hide more fetch latency than the few spilled values cost).  The per-ray
 // body is march_fast_body.cuh.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -14,7 +15,7 @@ constexpr int kTileH = 8;
 constexpr int kThreads = 128;
 
 template <int ST, int FILT>
-__global__ void __launch_bounds__(kThreads, 6) k_march_fast(const __grid_constant__ MarchUniforms u,
+__global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constant__ MarchUniforms u,
                                                             const __grid_constant__ ViewDev v) {
   __shared__ float s_t0[8 * kThreads], s_t1[8 * kThreads];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;

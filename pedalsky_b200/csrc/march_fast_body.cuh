@@ -15,7 +15,23 @@
 //     returns zero density;
 //   * texel coordinates are formed with one FMA per axis.
 //   * smoothsteps multiply by precomputed reciprocals, and this translation
-//     unit is built with approximate division and square root (a few ulp).
+//     unit is built with approximate division and square root (a few ulp);
+//   * F16 storage reads the channel-folded volumes (noise_bake.cu:k_fold_*):
+//     the base volume as (R, 0.625G + 0.25B + 0.125A) and the detail volume
+//     as 0.625R + 0.25G + 0.125B, the only combinations the density uses, so
+//     an exact trilinear tap is two 16-byte (base) or 8-byte (detail) quad
+//     loads and a texture tap filters two channels (or one) instead of four;
+//   * the texture-unit light march reduces the tap geometry to per-sample
+//     constants (altitude from a quadratic in t, texture coordinates affine
+//     in t and h) and computes every tap position of a batch of up to four
+//     taps and issues their fetches before it combines any of them, so the
+//     fetches overlap instead of each waiting for the previous one;
+//   * in the primary step the weather, type and base-shape fetches are
+//     independent of each other and are issued together; the curl tile is
+//     read as 2x2 quads (one 16-byte load per tap);
+//   * in the filtered forms (HYBRID, TEXTURE) the transmittance and sky-view
+//     LUTs go through the texture unit, as the reference's linear sampler
+//     does; EXACT keeps FP32 weights for them.
 // Octave counts up to 4 are handled here; the host falls back to the plain
 // kernel beyond that.
 #pragma once
@@ -83,41 +99,108 @@ __device__ __forceinline__ float4 trilinear_texel(const void* vol, float x, floa
   return r;
 }
 
+__device__ __forceinline__ float2 h2f(uint32_t w) {
+  return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+
+// Exact trilinear tap of the folded base volume (128^3 quads, repeat),
+// coordinates in texel units: one 16-byte quad load per slab, FP32 weights.
+// Returns (R, 0.625G + 0.25B + 0.125A), both in [0, 1].
+__device__ __forceinline__ float2 base_quad_tap(const uint4* q, float x, float y, float z) {
+  const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+  const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+  const float wx = x - fx, wy = y - fy, wz = z - fz;
+  const uint32_t r = ((uint32_t)iy & 127u) * 128u + ((uint32_t)ix & 127u);
+  const uint32_t z0 = (uint32_t)iz & 127u, z1 = (uint32_t)(iz + 1) & 127u;
+  const uint4 a = __ldg(q + z0 * 16384u + r);
+  const uint4 b = __ldg(q + z1 * 16384u + r);
+  const float2 tx = make_float2(wx, wx), ty = make_float2(wy, wy);
+  const float2 sa = lerp2(lerp2(h2f(a.x), h2f(a.y), tx), lerp2(h2f(a.z), h2f(a.w), tx), ty);
+  const float2 sb = lerp2(lerp2(h2f(b.x), h2f(b.y), tx), lerp2(h2f(b.z), h2f(b.w), tx), ty);
+  const float2 v = lerp2(sa, sb, make_float2(wz, wz));
+  return make_float2(v.x * (1.0f / 255.0f), v.y * (1.0f / 2040.0f));
+}
+
+// Exact trilinear tap of the folded detail volume (32^3 quads, repeat):
+// one 8-byte quad load per slab; the two slabs ride the two FP32x2 lanes.
+// Returns 0.625R + 0.25G + 0.125B in [0, 1].
+__device__ __forceinline__ float detail_quad_tap(const uint2* q, float x, float y, float z) {
+  const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+  const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+  const float wx = x - fx, wy = y - fy, wz = z - fz;
+  const uint32_t r = ((uint32_t)iy & 31u) * 32u + ((uint32_t)ix & 31u);
+  const uint32_t z0 = (uint32_t)iz & 31u, z1 = (uint32_t)(iz + 1) & 31u;
+  const uint2 a = __ldg(q + z0 * 1024u + r);
+  const uint2 b = __ldg(q + z1 * 1024u + r);
+  const float2 a0 = h2f(a.x), a1 = h2f(a.y), b0 = h2f(b.x), b1 = h2f(b.y);
+  const float2 tx = make_float2(wx, wx), ty = make_float2(wy, wy);
+  const float2 s = lerp2(lerp2(make_float2(a0.x, b0.x), make_float2(a0.y, b0.y), tx),
+                         lerp2(make_float2(a1.x, b1.x), make_float2(a1.y, b1.y), tx), ty);
+  return lerpf(s.x, s.y, wz) * (1.0f / 2040.0f);
+}
+
+// Bilinear curl tap (128^2, repeat) from the quad form: one 16-byte load,
+// FP32 weights; returns (R, G) in [0, 1].
+__device__ __forceinline__ float2 curl_quad_tap(const uint4* q, float x, float y) {
+  const float fx = floorf(x), fy = floorf(y);
+  const int ix = (int)fx, iy = (int)fy;
+  const float wx = x - fx, wy = y - fy;
+  const uint4 c = __ldg(q + ((uint32_t)iy & 127u) * 128u + ((uint32_t)ix & 127u));
+  const float2 tx = make_float2(wx, wx);
+  const float2 v = lerp2(lerp2(h2f(c.x), h2f(c.y), tx), lerp2(h2f(c.z), h2f(c.w), tx), make_float2(wy, wy));
+  return make_float2(v.x * (1.0f / 255.0f), v.y * (1.0f / 255.0f));
+}
+
+// Base-noise tap: (R, 0.625G + 0.25B + 0.125A).  LIGHT taps use the texture
+// unit in the HYBRID form.
 template <int ST, int FILT, bool LIGHT>
-__device__ __forceinline__ float4 base_tap(const MarchUniforms& u, float ax, float ay, float az) {
-  if constexpr (FILT == PSC_FILTER_TEXTURE || (FILT == PSC_FILTER_HYBRID && LIGHT)) {
-    float4 r = tex3D<float4>(u.tex_base, ax * u.inv_base_scale, ay * u.inv_base_scale,
-                             az * u.inv_base_scale);
-    if constexpr (ST == PSC_STORAGE_F16) {
-      r.x *= (1.0f / 255.0f);
-      r.y *= (1.0f / 255.0f);
-      r.z *= (1.0f / 255.0f);
-      r.w *= (1.0f / 255.0f);
+__device__ __forceinline__ float2 base_tap(const MarchUniforms& u, float ax, float ay, float az) {
+  constexpr bool kTex = FILT == PSC_FILTER_TEXTURE || (FILT == PSC_FILTER_HYBRID && LIGHT);
+  if constexpr (ST == PSC_STORAGE_F16) {
+    if constexpr (kTex) {
+      const float2 r = tex3D<float2>(u.tex_base, ax * u.inv_base_scale, ay * u.inv_base_scale,
+                                     az * u.inv_base_scale);
+      return make_float2(r.x * (1.0f / 255.0f), r.y * (1.0f / 2040.0f));
+    } else {
+      const float k = u.base_texel_scale;
+      return base_quad_tap(u.base_quad, fmaf(ax, k, -0.5f), fmaf(ay, k, -0.5f), fmaf(az, k, -0.5f));
     }
-    return r;
   } else {
-    const float k = u.base_texel_scale;
-    return trilinear_texel<ST, 128>(u.noise_base, fmaf(ax, k, -0.5f), fmaf(ay, k, -0.5f),
-                                    fmaf(az, k, -0.5f), u.noise_scale);
+    float4 b;
+    if constexpr (kTex) {
+      b = tex3D<float4>(u.tex_base, ax * u.inv_base_scale, ay * u.inv_base_scale,
+                        az * u.inv_base_scale);
+    } else {
+      const float k = u.base_texel_scale;
+      b = trilinear_texel<ST, 128>(u.noise_base, fmaf(ax, k, -0.5f), fmaf(ay, k, -0.5f),
+                                   fmaf(az, k, -0.5f), u.noise_scale);
+    }
+    return make_float2(b.x, fmaf(b.w, 0.125f, fmaf(b.z, 0.25f, b.y * 0.625f)));
   }
 }
 
+// Detail-noise tap: 0.625R + 0.25G + 0.125B (cloud_march.wgsl:512-515).
 template <int ST, int FILT>
-__device__ __forceinline__ float4 detail_tap(const MarchUniforms& u, float dx, float dy, float dz) {
-  if constexpr (FILT == PSC_FILTER_TEXTURE) {
-    float4 r = tex3D<float4>(u.tex_detail, dx * u.inv_detail_scale, dy * u.inv_detail_scale,
-                             dz * u.inv_detail_scale);
-    if constexpr (ST == PSC_STORAGE_F16) {
-      r.x *= (1.0f / 255.0f);
-      r.y *= (1.0f / 255.0f);
-      r.z *= (1.0f / 255.0f);
-      r.w *= (1.0f / 255.0f);
+__device__ __forceinline__ float detail_tap(const MarchUniforms& u, float dx, float dy, float dz) {
+  if constexpr (ST == PSC_STORAGE_F16) {
+    if constexpr (FILT == PSC_FILTER_TEXTURE) {
+      return tex3D<float>(u.tex_detail, dx * u.inv_detail_scale, dy * u.inv_detail_scale,
+                          dz * u.inv_detail_scale) * (1.0f / 2040.0f);
+    } else {
+      const float k = u.detail_texel_scale;
+      return detail_quad_tap(u.detail_quad, fmaf(dx, k, -0.5f), fmaf(dy, k, -0.5f), fmaf(dz, k, -0.5f));
     }
-    return r;
   } else {
-    const float k = u.detail_texel_scale;
-    return trilinear_texel<ST, 32>(u.noise_detail, fmaf(dx, k, -0.5f), fmaf(dy, k, -0.5f),
-                                   fmaf(dz, k, -0.5f), u.noise_scale);
+    float4 d;
+    if constexpr (FILT == PSC_FILTER_TEXTURE) {
+      d = tex3D<float4>(u.tex_detail, dx * u.inv_detail_scale, dy * u.inv_detail_scale,
+                        dz * u.inv_detail_scale);
+    } else {
+      const float k = u.detail_texel_scale;
+      d = trilinear_texel<ST, 32>(u.noise_detail, fmaf(dx, k, -0.5f), fmaf(dy, k, -0.5f),
+                                  fmaf(dz, k, -0.5f), u.noise_scale);
+    }
+    return fmaf(d.z, 0.125f, fmaf(d.y, 0.25f, d.x * 0.625f));
   }
 }
 
@@ -149,15 +232,39 @@ __device__ __forceinline__ float ndf_fast(float h, uint32_t t, float anvil_bias)
 }
 
 // Base-shape part shared by the primary and light densities
-// (cloud_march.wgsl:463-494).  `h` in [0,1], `eff` >= 0.01 already checked.
-template <int ST, int FILT, bool LIGHT>
-__device__ __forceinline__ float base_shape(const MarchUniforms& u, const LayerConst& L, float ax,
-                                            float ay, float az, float h, float eff, uint32_t type) {
-  const float4 b = base_tap<ST, FILT, LIGHT>(u, ax, ay, az);
-  const float lf = clamp01(fmaf(b.w, 0.125f, fmaf(b.z, 0.25f, b.y * 0.625f)) + L.lf_bias);
-  const float base_cloud = __fdividef(b.x + (1.0f - lf), fmaxf(2.0f - lf, 1e-5f));
-  const float cloud = base_cloud * ndf_fast(h, type, L.anvil_bias);
-  return __fdividef(cloud - (1.0f - eff), fmaxf(eff, 1e-5f)) * eff;
+// (cloud_march.wgsl:463-494) from a base tap `b` = (R, low-frequency fbm)
+// and the profile value `nd` = ndf(h, type).  The coverage remap
+// remap(cloud, 1 - eff, 1, 0, 1) * eff equals cloud - (1 - eff) wherever the
+// density is not gated off (eff >= 0.01), and 2 - lf >= 1, so neither
+// needs its guard.
+__device__ __forceinline__ float shape_from(float2 b, float lf_bias, float nd, float one_minus_eff) {
+  const float lf = clamp01(b.y + lf_bias);
+  const float base_cloud = __fdividef(b.x + (1.0f - lf), 2.0f - lf);
+  return fmaf(base_cloud, nd, -one_minus_eff);
+}
+
+// ndf_fast for types 0..6 as two reciprocal smoothsteps with per-type
+// constants: ssr(0, inv_a, h) * g, g = ssr(e1, inv_w1, h) or 1 - that.
+// Chosen once per dense sample, so the light taps carry no switch.
+struct NdfCoef {
+  float inv_a, e1, inv_w1;
+  bool flip;
+};
+__device__ __forceinline__ NdfCoef ndf_coef(uint32_t t) {
+  switch (t) {
+    case 0: return {1.0f / 0.07f, 1.0f, 1.0f / -0.8f, false};
+    case 1: return {1.0f / 0.10f, 0.6f, 1.0f / 0.4f, true};
+    case 2: return {1.0f / 0.15f, 1.0f, 1.0f / -0.6f, false};
+    case 3: return {1.0f / 0.20f, 1.0f, 1.0f / -0.7f, false};
+    case 4: return {1.0f / 0.30f, 0.7f, 1.0f / 0.3f, true};
+    case 5: return {1.0f / 0.40f, 0.6f, 1.0f / 0.4f, true};
+    case 6: return {1.0f / 0.50f, 0.8f, 1.0f / 0.2f, true};
+    default: return {0.0f, 0.0f, 0.0f, false};  // unknown types: ndf = 0
+  }
+}
+__device__ __forceinline__ float ndf_eval(const NdfCoef& k, float h) {
+  const float g = ssr(k.e1, k.inv_w1, h);
+  return ssr(0.0f, k.inv_a, h) * (k.flip ? 1.0f - g : g);
 }
 
 template <int ST, int FILT>
@@ -169,7 +276,9 @@ __device__ __forceinline__ float density_light(const MarchUniforms& u, const Lay
   const float sk = h * L.skew_thickness;
   const float ax = fmaf(-L.skew_x, sk, qx - L.wind_off_x);
   const float az = fmaf(-L.skew_z, sk, qz - L.wind_off_z);
-  return clamp01(base_shape<ST, FILT, true>(u, L, ax, qy, az, h, eff, type)) * L.density_scale;
+  const float2 b = base_tap<ST, FILT, true>(u, ax, qy, az);
+  return clamp01(shape_from(b, L.lf_bias, ndf_fast(h, type, L.anvil_bias), 1.0f - eff)) *
+         L.density_scale;
 }
 
 __device__ __forceinline__ float alt_from(const MarchUniforms& u, float qx, float qy, float qz,
@@ -212,6 +321,97 @@ __device__ __noinline__ float light_cone(const MarchUniforms& u, const LayerCons
   return od;
 }
 
+// Light march through the texture unit.  Per dense sample the tap geometry
+// is reduced to constants: the distance from the planet centre along the
+// sun ray is r(t)^2 = A + t (B + t) with A = r0^2, B = 2 r0 cos(up, sun),
+// so alt(t) = h0 + t (B + t) / (r0 + r(t)) (the stable form alt_from
+// uses), and the texture coordinates of a tap are affine in t and h.  Taps
+// run in batches of 4, then 2, then 1 (no padded slots): every position and
+// fetch of a batch first, then the densities and the optical-depth sum in
+// tap order, plain or compensated as in the one-tap-at-a-time loop.  A tap
+// outside the layer's height range is fetched but adds zero, as
+// density_light returns for it.
+struct LightRay {
+  float A, B, r0, h0;  // geometry above
+  float ih, hb;        // h = alt * ih - hb
+  float px, py, pz;    // texture coordinates of the sample, wind removed
+  float sx, sy, sz;    // sun direction in texture units per metre
+  float kx, kz;        // skew shift in texture units per unit of h
+  float step, one_minus_eff;
+};
+
+// ndf of a non-Cumulonimbus type from its coefficients, and of Cumulonimbus.
+struct NdfGeneral {
+  NdfCoef k;
+  __device__ __forceinline__ float operator()(float h) const { return ndf_eval(k, h); }
+};
+struct NdfCb {
+  float anvil_bias;
+  __device__ __forceinline__ float operator()(float h) const { return ndf_fast(h, 7u, anvil_bias); }
+};
+
+// Base-noise tap of the light march at normalised texture coordinates.
+template <int ST>
+__device__ __forceinline__ float2 light_tex_tap(const MarchUniforms& u, float x, float y, float z) {
+  if constexpr (ST == PSC_STORAGE_F16) {
+    const float2 r = tex3D<float2>(u.tex_base, x, y, z);
+    return make_float2(r.x * (1.0f / 255.0f), r.y * (1.0f / 2040.0f));
+  } else {
+    const float4 b = tex3D<float4>(u.tex_base, x, y, z);
+    return make_float2(b.x, fmaf(b.w, 0.125f, fmaf(b.z, 0.25f, b.y * 0.625f)));
+  }
+}
+
+template <int ST, class Prof, uint32_t NB>
+__device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerConst& L,
+                                           const LightRay& lr, const Prof& prof, uint32_t i0,
+                                           float& od, float& comp) {
+  float2 bt[NB];
+  float hh[NB];
+#pragma unroll
+  for (uint32_t j = 0; j < NB; ++j) {
+    const float t = ((float)(i0 + j) + 0.5f) * lr.step;
+    const float bt_t = lr.B + t;
+    const float r = sqrtf(fmaf(t, bt_t, lr.A));
+    const float alt = lr.h0 + __fdividef(t * bt_t, lr.r0 + r);
+    const float h = fmaf(alt, lr.ih, -lr.hb);
+    hh[j] = h;
+    bt[j] = light_tex_tap<ST>(u, fmaf(-lr.kx, h, fmaf(lr.sx, t, lr.px)), fmaf(lr.sy, t, lr.py),
+                              fmaf(-lr.kz, h, fmaf(lr.sz, t, lr.pz)));
+  }
+#pragma unroll
+  for (uint32_t j = 0; j < NB; ++j) {
+    const float h = hh[j];
+    const float d = (h >= 0.0f && h <= 1.0f)
+                        ? clamp01(shape_from(bt[j], L.lf_bias, prof(h), lr.one_minus_eff)) * L.density_scale
+                        : 0.0f;
+    const float term = d * lr.step;
+    if (u.kahan) {
+      const float y = term - comp;
+      const float tt = od + y;
+      comp = (tt - od) - y;
+      od = tt;
+    } else {
+      od += term;
+    }
+  }
+}
+
+template <int ST, class Prof>
+__device__ __forceinline__ float light_march_tex(const MarchUniforms& u, const LayerConst& L,
+                                                 const LightRay& lr, const Prof& prof) {
+  const uint32_t n = u.light_steps;
+  float od = 0.0f, comp = 0.0f;
+  uint32_t i = 0;
+  for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, 4>(u, L, lr, prof, i, od, comp);
+  if (i + 2u <= n) {
+    light_taps<ST, Prof, 2>(u, L, lr, prof, i, od, comp);
+    i += 2u;
+  }
+  if (i < n) light_taps<ST, Prof, 1>(u, L, lr, prof, i, od, comp);
+  return od;
+}
+
 // Optical depth toward the sun (cloud_march.wgsl:543-578).
 template <int ST, int FILT>
 __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerConst& L, float px,
@@ -222,6 +422,28 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
   const float dist = fmaxf((L.top_m - alt) * u.inv_cos_sun, 1.0f);
   if (u.cone) return light_cone<ST, FILT>(u, L, px, py, pz, alt, eff, type, r0, cv, dist);
   const float step = __fdividef(dist, (float)u.light_steps);
+  if constexpr (FILT != PSC_FILTER_EXACT) {
+    const float k = u.inv_base_scale;
+    LightRay lr;
+    lr.A = r0 * r0;
+    lr.B = 2.0f * r0 * cv;
+    lr.r0 = r0;
+    lr.h0 = alt;
+    lr.ih = L.inv_thickness;
+    lr.hb = L.base_m * L.inv_thickness;
+    lr.px = (px - L.wind_off_x) * k;
+    lr.py = py * k;
+    lr.pz = (pz - L.wind_off_z) * k;
+    lr.sx = u.sun[0] * k;
+    lr.sy = u.sun[1] * k;
+    lr.sz = u.sun[2] * k;
+    lr.kx = L.skew_x * L.skew_thickness * k;
+    lr.kz = L.skew_z * L.skew_thickness * k;
+    lr.step = step;
+    lr.one_minus_eff = 1.0f - eff;
+    if (type == 7u) return light_march_tex<ST>(u, L, lr, NdfCb{L.anvil_bias});
+    return light_march_tex<ST>(u, L, lr, NdfGeneral{ndf_coef(type)});
+  }
   float od = 0.0f, comp = 0.0f;
   for (uint32_t i = 0; i < u.light_steps; ++i) {
     const float t = ((float)i + 0.5f) * step;
@@ -258,7 +480,7 @@ __device__ __forceinline__ float3 sun_trans_fast(const MarchUniforms& u, float a
   const float d_min = top - r, d_max = rho + u.big_h;
   const float xm = clamp01(__fdividef(d - d_min, fmaxf(d_max - d_min, 1.0f)));
   const float xr = __fdividef(rho, fmaxf(u.big_h, 1.0f));
-  const float4 t = lut2d(u.lut_trans, 256, 64, xm, xr);
+  const float4 t = u.tex_trans ? tex2D<float4>(u.tex_trans, xm, xr) : lut2d(u.lut_trans, 256, 64, xm, xr);
   return make_float3(t.x, t.y, t.z);
 }
 
@@ -279,7 +501,7 @@ __device__ __forceinline__ float3 sky_fast(const MarchUniforms& u, float alt, fl
   }
   float du = (fast_atan2(ux, uz) - u.sun_az) * (1.0f / (2.0f * kPi));
   du = du - floorf(du);
-  const float4 s = lut2d(u.lut_sky, 192, 108, du, vv);
+  const float4 s = u.tex_sky ? tex2D<float4>(u.tex_sky, du, vv) : lut2d(u.lut_sky, 192, 108, du, vv);
   return make_float3(s.x * u.sun_illum[0], s.y * u.sun_illum[1], s.z * u.sun_illum[2]);
 }
 
@@ -386,21 +608,23 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
       const float h = (alt - L.base_m) * L.inv_thickness;
       if (h >= 0.0f && h <= 1.0f) {
         const float wsx = px3 - L.wind_off_x, wsz = pz3 - L.wind_off_z;
+        const float sk = h * L.skew_thickness;
+        const float ax = fmaf(-L.skew_x, sk, wsx);
+        const float az = fmaf(-L.skew_z, sk, wsz);
+        // weather, type and base fetches do not depend on each other
         const float wr = weather_fast(u, fmaf(wsx, u.inv_weather_scale, 0.5f),
                                       fmaf(wsz, u.inv_weather_scale, 0.5f));
+        const uint32_t type = effective_type(u, wsx, wsz, L.cloud_type);
+        const float2 bt = base_tap<ST, FILT, false>(u, ax, py3, az);
         const float eff = clamp01(wr * L.coverage);
-        if (eff >= 0.01f) {
-          const uint32_t type = effective_type(u, wsx, wsz, L.cloud_type);
-          const float sk = h * L.skew_thickness;
-          const float ax = fmaf(-L.skew_x, sk, wsx);
-          const float az = fmaf(-L.skew_z, sk, wsz);
-          float cloud = base_shape<ST, FILT, false>(u, L, ax, py3, az, h, eff, type);
+        float cloud = shape_from(bt, L.lf_bias, ndf_fast(h, type, L.anvil_bias), 1.0f - eff);
+        if (eff >= 0.01f) {  // coverage gate (cloud_march.wgsl:450-451)
           if (cloud > 0.0f) {  // curl-perturbed detail erosion (:502-527)
-            const float2 c2 = curl_sample(u.curl, ax * u.inv_detail_scale, az * u.inv_detail_scale);
+            const float2 c2 = curl_quad_tap(u.curl_quad, fmaf(ax, u.curl_texel_scale, -0.5f),
+                                            fmaf(az, u.curl_texel_scale, -0.5f));
             const float ddx = fmaf(fmaf(c2.x, 2.0f, -1.0f), u.curl_offset_scale, ax);
             const float ddz = fmaf(fmaf(c2.y, 2.0f, -1.0f), u.curl_offset_scale, az);
-            const float4 det = detail_tap<ST, FILT>(u, ddx, py3, ddz);
-            const float hf = fmaf(det.z, 0.125f, fmaf(det.y, 0.25f, det.x * 0.625f));
+            const float hf = detail_tap<ST, FILT>(u, ddx, py3, ddz);
             const float dmod = mixf(hf, 1.0f - hf, clamp01(h * 10.0f));
             const float lo = dmod * L.layer_detail;
             cloud = __fdividef(cloud - lo, fmaxf(1.0f - lo, 1e-5f));

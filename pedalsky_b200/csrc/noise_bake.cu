@@ -225,7 +225,82 @@ __global__ void k_convert(const uint32_t* __restrict__ src, void* __restrict__ d
   }
 }
 
+// Channel-folded FP16 forms of the noise volumes, read by the FAST schedule.
+// The march uses the base volume only through R and the low-frequency fbm
+// 0.625 G + 0.25 B + 0.125 A, and the detail volume only through
+// 0.625 R + 0.25 G + 0.125 B (cloud_march.wgsl:463-470, 512-515).  Filtering
+// is linear, so filtering the folded channel equals folding the filtered
+// channels.  On bytes the folds are integers: base (R, 5G + 2B + A) and
+// detail 5R + 2G + B, at most 2040, which FP16 holds exactly; the kernels
+// rescale by 1/255 and 1/2040 after filtering.
+//   fold: one texel per entry (source of the texture arrays);
+//   quad: the 2x2 footprint (x, x+1) x (y, y+1) of slab z, repeat-wrapped,
+//         per entry, so an exact trilinear tap is one load per slab.
+__device__ __forceinline__ uint32_t fold_base_texel(uint32_t w) {
+  const uint32_t r = w & 0xffu, g = (w >> 8) & 0xffu, b = (w >> 16) & 0xffu, a = w >> 24;
+  const __half2 h = __floats2half2_rn((float)r, (float)(5u * g + 2u * b + a));
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ uint32_t fold_detail_texel(uint32_t w) {
+  const uint32_t r = w & 0xffu, g = (w >> 8) & 0xffu, b = (w >> 16) & 0xffu;
+  return __half_as_ushort(__float2half_rn((float)(5u * r + 2u * g + b)));
+}
+
+template <uint32_t N>
+__global__ void k_fold_base(const uint32_t* __restrict__ src, uint32_t* __restrict__ fold,
+                            uint4* __restrict__ quad) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * N * N) return;
+  const uint32_t x = i % N, y = (i / N) % N, z = i / (N * N);
+  const uint32_t x1 = (x + 1u) & (N - 1u), y1 = (y + 1u) & (N - 1u);
+  const uint32_t row0 = (z * N + y) * N, row1 = (z * N + y1) * N;
+  fold[i] = fold_base_texel(src[i]);
+  quad[i] = make_uint4(fold_base_texel(src[row0 + x]), fold_base_texel(src[row0 + x1]),
+                       fold_base_texel(src[row1 + x]), fold_base_texel(src[row1 + x1]));
+}
+
+template <uint32_t N>
+__global__ void k_fold_detail(const uint32_t* __restrict__ src, uint16_t* __restrict__ fold,
+                              uint2* __restrict__ quad) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * N * N) return;
+  const uint32_t x = i % N, y = (i / N) % N, z = i / (N * N);
+  const uint32_t x1 = (x + 1u) & (N - 1u), y1 = (y + 1u) & (N - 1u);
+  const uint32_t row0 = (z * N + y) * N, row1 = (z * N + y1) * N;
+  fold[i] = (uint16_t)fold_detail_texel(src[i]);
+  quad[i] = make_uint2(fold_detail_texel(src[row0 + x]) | (fold_detail_texel(src[row0 + x1]) << 16),
+                       fold_detail_texel(src[row1 + x]) | (fold_detail_texel(src[row1 + x1]) << 16));
+}
+
+// Curl tile (128^2 RG8) as 2x2 quads of (R, G) half pairs, repeat-wrapped:
+// a bilinear curl tap is one 16-byte load.  Bytes are exact in FP16.
+__global__ void k_curl_quads(const uint16_t* __restrict__ src, uint4* __restrict__ quad) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 128u * 128u) return;
+  const uint32_t x = i & 127u, y = i >> 7, x1 = (x + 1u) & 127u, y1 = (y + 1u) & 127u;
+  auto pair = [&](uint32_t xx, uint32_t yy) {
+    const uint32_t t = src[yy * 128u + xx];
+    const __half2 h = __floats2half2_rn((float)(t & 0xffu), (float)(t >> 8));
+    return *reinterpret_cast<const uint32_t*>(&h);
+  };
+  quad[i] = make_uint4(pair(x, y), pair(x1, y), pair(x, y1), pair(x1, y1));
+}
+
 }  // namespace
+
+int launch_curl_quads(const uint8_t* curl, uint4* quad, cudaStream_t s) {
+  k_curl_quads<<<128u * 128u / 256u, 256, 0, s>>>(reinterpret_cast<const uint16_t*>(curl), quad);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
+
+int launch_fold_storage(const uint8_t* base_u8, const uint8_t* detail_u8, uint32_t* base_fold,
+                        uint4* base_quad, uint16_t* detail_fold, uint2* detail_quad, cudaStream_t s) {
+  k_fold_base<128><<<128u * 128u * 128u / 256u, 256, 0, s>>>(
+      reinterpret_cast<const uint32_t*>(base_u8), base_fold, base_quad);
+  k_fold_detail<32><<<32u * 32u * 32u / 256u, 256, 0, s>>>(
+      reinterpret_cast<const uint32_t*>(detail_u8), detail_fold, detail_quad);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
 
 int launch_noise_bakes(uint8_t* base, uint8_t* detail, uint8_t* curl, cudaStream_t s) {
   k_bake_base<<<dim3(32, 32, 32), dim3(4, 4, 4), 0, s>>>(base);

@@ -43,10 +43,24 @@ struct psc_ctx {
   uint16_t* d_lut_h[4] = {nullptr, nullptr, nullptr, nullptr};  // RGBA16F bake outputs
   bool have_lut[4] = {false, false, false, false};
 
-  // texture-unit path
+  // F16 storage, FAST schedule: channel-folded volumes (k_fold_* in
+  // noise_bake.cu), one texel per entry and 2x2 quads per entry
+  uint32_t* d_base_fold = nullptr;   // 128^3 half2 (R, 5G+2B+A)
+  uint4* d_base_quad = nullptr;      // 128^3 x 4 half2
+  uint16_t* d_detail_fold = nullptr; // 32^3 half (5R+2G+B)
+  uint2* d_detail_quad = nullptr;    // 32^3 x 4 half
+  uint4* d_curl_quad = nullptr;      // 128^2 x 4 half2 (R, G), FAST schedule
+
+  // texture-unit path: RGBA8 volumes for U8 storage, the folded volumes for
+  // F16 storage
   cudaArray_t arr_base = nullptr, arr_detail = nullptr;
   cudaTextureObject_t tex_base = 0, tex_detail = 0;
   bool tex_dirty = true;
+  // transmittance and sky-view LUTs read through the texture unit (bilinear,
+  // clamp): transmittance bound to its float4 copy in d_lut, sky-view to the
+  // array arr_sky (copied from d_lut on upload); 0 until created
+  cudaTextureObject_t tex_lut[4] = {0, 0, 0, 0};
+  cudaArray_t arr_sky = nullptr;
 
   uint64_t launches = 0;
 

@@ -24,6 +24,9 @@
 namespace psc {
 int launch_convert_storage(const uint8_t* src, void* dst, uint32_t n_texels, int storage,
                            float fp8_scale, cudaStream_t s);
+int launch_curl_quads(const uint8_t* curl, uint4* quad, cudaStream_t s);
+int launch_fold_storage(const uint8_t* base_u8, const uint8_t* detail_u8, uint32_t* base_fold,
+                        uint4* base_quad, uint16_t* detail_fold, uint2* detail_quad, cudaStream_t s);
 }
 
 namespace {
@@ -328,6 +331,13 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
   u.lut_ap = c->d_lut[PSC_LUT_AERIAL];
   u.tex_base = c->tex_base;
   u.tex_detail = c->tex_detail;
+  u.curl_quad = c->d_curl_quad;
+  u.base_quad = c->d_base_quad;
+  u.detail_quad = c->d_detail_quad;
+  // texture-unit sampling of the transmittance LUT belongs to the filtered
+  // forms; EXACT keeps FP32 weights everywhere
+  u.tex_trans = c->opts.filter != PSC_FILTER_EXACT ? c->tex_lut[PSC_LUT_TRANSMITTANCE] : 0;
+  u.tex_sky = c->opts.filter != PSC_FILTER_EXACT ? c->tex_lut[PSC_LUT_SKYVIEW] : 0;
 }
 
 void build_uniforms(const psc_ctx* c, uint32_t width, uint32_t height, psc::MarchUniforms& u) {
@@ -346,6 +356,19 @@ int build_storage(psc_ctx* c) {
   if (psc::launch_convert_storage(c->d_base_u8, c->d_base_store, 128u * 128u * 128u, st, c->fp8_scale, 0) ||
       psc::launch_convert_storage(c->d_detail_u8, c->d_detail_store, 32u * 32u * 32u, st, c->fp8_scale, 0))
     return fail(PSC_ERR_CUDA, "storage conversion launch failed");
+  if (c->have_curl) {  // the FAST schedule reads the curl tile as quads
+    if (!c->d_curl_quad) PSC_CUDA(cudaMalloc(&c->d_curl_quad, 128u * 128u * 16u), "cudaMalloc curl quads");
+    if (psc::launch_curl_quads(c->d_curl, c->d_curl_quad, 0)) return fail(PSC_ERR_CUDA, "curl quad launch failed");
+  }
+  if (st == PSC_STORAGE_F16) {  // the FAST schedule reads the channel-folded forms
+    if (!c->d_base_fold) PSC_CUDA(cudaMalloc(&c->d_base_fold, 128u * 128u * 128u * 4u), "cudaMalloc base fold");
+    if (!c->d_base_quad) PSC_CUDA(cudaMalloc(&c->d_base_quad, 128u * 128u * 128u * 16u), "cudaMalloc base quads");
+    if (!c->d_detail_fold) PSC_CUDA(cudaMalloc(&c->d_detail_fold, 32u * 32u * 32u * 2u), "cudaMalloc detail fold");
+    if (!c->d_detail_quad) PSC_CUDA(cudaMalloc(&c->d_detail_quad, 32u * 32u * 32u * 8u), "cudaMalloc detail quads");
+    if (psc::launch_fold_storage(c->d_base_u8, c->d_detail_u8, c->d_base_fold, c->d_base_quad, c->d_detail_fold,
+                                 c->d_detail_quad, 0))
+      return fail(PSC_ERR_CUDA, "channel fold launch failed");
+  }
   PSC_CUDA(cudaDeviceSynchronize(), "storage conversion");
   c->store_form = st;
   return PSC_OK;
@@ -361,15 +384,16 @@ void destroy_textures(psc_ctx* c) {
   c->tex_dirty = true;
 }
 
-// 3D texture over an RGBA8 (read as normalised float) or RGBA16F volume
-// (read as stored; the F16 volume holds the byte values 0..255), linear
-// filtering, repeat addressing, normalised coordinates: the noise sampler of
-// crates/ps-clouds/src/noise.rs:178-187.
-int make_volume_texture(const void* d_src, uint32_t n, bool half4, cudaArray_t* arr,
+// 3D texture over an RGBA8 volume (read as normalised float) or a
+// channel-folded FP16 volume (half2 base / half detail, read as stored),
+// linear filtering, repeat addressing, normalised coordinates: the noise
+// sampler of crates/ps-clouds/src/noise.rs:178-187.
+int make_volume_texture(const void* d_src, uint32_t n, int half_channels, cudaArray_t* arr,
                         cudaTextureObject_t* tex) {
-  const cudaChannelFormatDesc fmt =
-      half4 ? cudaCreateChannelDescHalf4() : cudaCreateChannelDesc<uchar4>();
-  const size_t texel = half4 ? 8 : 4;
+  const cudaChannelFormatDesc fmt = half_channels == 2   ? cudaCreateChannelDescHalf2()
+                                    : half_channels == 1 ? cudaCreateChannelDescHalf1()
+                                                         : cudaCreateChannelDesc<uchar4>();
+  const size_t texel = half_channels ? 2u * half_channels : 4u;
   const cudaExtent ext = make_cudaExtent(n, n, n);
   PSC_CUDA(cudaMalloc3DArray(arr, &fmt, ext), "cudaMalloc3DArray");
   cudaMemcpy3DParms cp{};
@@ -384,7 +408,7 @@ int make_volume_texture(const void* d_src, uint32_t n, bool half4, cudaArray_t* 
   cudaTextureDesc td{};
   td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeWrap;
   td.filterMode = cudaFilterModeLinear;
-  td.readMode = half4 ? cudaReadModeElementType : cudaReadModeNormalizedFloat;
+  td.readMode = half_channels ? cudaReadModeElementType : cudaReadModeNormalizedFloat;
   td.normalizedCoords = 1;
   PSC_CUDA(cudaCreateTextureObject(tex, &rd, &td, nullptr), "cudaCreateTextureObject");
   return PSC_OK;
@@ -393,12 +417,14 @@ int make_volume_texture(const void* d_src, uint32_t n, bool half4, cudaArray_t* 
 int build_textures(psc_ctx* c) {
   if (c->opts.filter == PSC_FILTER_EXACT || !c->tex_dirty) return PSC_OK;
   destroy_textures(c);
-  const bool h4 = c->opts.storage == PSC_STORAGE_F16;
-  int rc = make_volume_texture(h4 ? c->d_base_store : c->d_base_u8, 128, h4, &c->arr_base,
-                               &c->tex_base);
+  const bool f16 = c->opts.storage == PSC_STORAGE_F16;
+  if (f16 && (!c->d_base_fold || !c->d_detail_fold))
+    return fail(PSC_ERR_MISSING_INPUT, "folded F16 volumes were not built");
+  int rc = make_volume_texture(f16 ? (const void*)c->d_base_fold : c->d_base_u8, 128, f16 ? 2 : 0,
+                               &c->arr_base, &c->tex_base);
   if (rc) return rc;
-  rc = make_volume_texture(h4 ? c->d_detail_store : c->d_detail_u8, 32, h4, &c->arr_detail,
-                           &c->tex_detail);
+  rc = make_volume_texture(f16 ? (const void*)c->d_detail_fold : c->d_detail_u8, 32, f16 ? 1 : 0,
+                           &c->arr_detail, &c->tex_detail);
   if (rc) return rc;
   c->tex_dirty = false;
   return PSC_OK;
@@ -488,6 +514,22 @@ int validate_tuning(const PscBatchTuning& t) {
 
 // Host staging of one batch: per-view uniform blocks, view records, frame
 // records for the LUT bakes and the cost-sorted tile list.
+// Uniform block of one batch view: its own scene, and its own sky-view and
+// aerial-perspective LUTs (baked per view into `sky` / `ap`, read with plain
+// loads; the context's sky-view texture belongs to its own frame).
+void build_batch_view_uniforms(const psc_ctx* c, const PscBatchView& bv, float4* sky, float4* ap,
+                               psc::MarchUniforms& u) {
+  PscCloudParamsGpu p = bv.params;
+  p.cloud_layer_count = bv.n_layers;
+  PscCloudLayerGpu layers[8];
+  std::memset(layers, 0, sizeof(layers));
+  for (uint32_t l = 0; l < bv.n_layers; ++l) layers[l] = bv.layers[l];
+  build_uniforms_for(c, p, layers, bv.frame, bv.width, bv.height, u);
+  u.lut_sky = sky;
+  u.tex_sky = 0;
+  u.lut_ap = ap;
+}
+
 int stage_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32_t* n_tiles_out) {
   const PscBatchTuning& tu = c->batch_tuning;
   const uint32_t tile_w = tu.tile_w, tile_h = (tu.threads / 32 / (tu.tile_w / 8)) * 4;
@@ -505,15 +547,8 @@ int stage_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32_t* n_t
   const size_t fl = psc::frame_lite_size();
   for (uint32_t i = 0; i < n; ++i) {
     const PscBatchView& bv = views[i];
-    PscCloudParamsGpu p = bv.params;
-    p.cloud_layer_count = bv.n_layers;
-    PscCloudLayerGpu layers[8];
-    std::memset(layers, 0, sizeof(layers));
-    for (uint32_t l = 0; l < bv.n_layers; ++l) layers[l] = bv.layers[l];
-    psc::MarchUniforms& u = c->h_bu[i];
-    build_uniforms_for(c, p, layers, bv.frame, bv.width, bv.height, u);
-    u.lut_sky = c->d_bsky + (size_t)i * 192 * 108;
-    u.lut_ap = c->d_bap + (size_t)i * 32 * 32 * 64;
+    build_batch_view_uniforms(c, bv, c->d_bsky + (size_t)i * PSC_SKYVIEW_W * PSC_SKYVIEW_H,
+                              c->d_bap + (size_t)i * PSC_AP_W * PSC_AP_H * PSC_AP_D, c->h_bu[i]);
     c->h_bv[i] = psc::ViewDev{bv.width, bv.height, 0, 0, bv.depth, reinterpret_cast<float4*>(bv.out_luminance),
                               reinterpret_cast<float4*>(bv.out_transmittance), reinterpret_cast<float4*>(bv.hdr)};
     psc::frame_lite_from(bv.frame, static_cast<char*>(c->h_bframes) + i * fl);
@@ -566,8 +601,49 @@ int upload_lut_float4(psc_ctx* c, int kind, const uint16_t* h16) {
   const size_t n = lut_texels(kind);
   std::vector<float> f(n * 4);
   for (size_t i = 0; i < n * 4; ++i) f[i] = half_bits_to_float(h16[i]);
-  if (!c->d_lut[kind]) PSC_CUDA(cudaMalloc(&c->d_lut[kind], n * sizeof(float4)), "cudaMalloc LUT");
+  if (!c->d_lut[kind]) {
+    PSC_CUDA(cudaMalloc(&c->d_lut[kind], n * sizeof(float4)), "cudaMalloc LUT");
+    if (kind == PSC_LUT_TRANSMITTANCE) {
+      // bilinear, clamp-to-edge, normalised coordinates: the LUT sampler of
+      // the reference (crates/ps-clouds/src/lib.rs:256-265), bound to the
+      // float4 copy so later uploads and bakes need no new object
+      const uint32_t w = PSC_TRANSMITTANCE_W, h = PSC_TRANSMITTANCE_H;
+      cudaResourceDesc rd{};
+      rd.resType = cudaResourceTypePitch2D;
+      rd.res.pitch2D.devPtr = c->d_lut[kind];
+      rd.res.pitch2D.desc = cudaCreateChannelDesc<float4>();
+      rd.res.pitch2D.width = w;
+      rd.res.pitch2D.height = h;
+      rd.res.pitch2D.pitchInBytes = (size_t)w * sizeof(float4);
+      cudaTextureDesc td{};
+      td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+      td.filterMode = cudaFilterModeLinear;
+      td.readMode = cudaReadModeElementType;
+      td.normalizedCoords = 1;
+      PSC_CUDA(cudaCreateTextureObject(&c->tex_lut[kind], &rd, &td, nullptr), "LUT texture object");
+    }
+  }
   PSC_CUDA(cudaMemcpy(c->d_lut[kind], f.data(), n * sizeof(float4), cudaMemcpyHostToDevice), "LUT upload");
+  if (kind == PSC_LUT_SKYVIEW) {
+    // the sky-view LUT also lives in a float4 array behind a texture object
+    // (bilinear, clamp, normalised coordinates), refreshed on every upload
+    const size_t row = PSC_SKYVIEW_W * sizeof(float4);
+    if (!c->arr_sky) {
+      const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float4>();
+      PSC_CUDA(cudaMallocArray(&c->arr_sky, &fmt, PSC_SKYVIEW_W, PSC_SKYVIEW_H), "cudaMallocArray sky-view");
+      cudaResourceDesc rd{};
+      rd.resType = cudaResourceTypeArray;
+      rd.res.array.array = c->arr_sky;
+      cudaTextureDesc td{};
+      td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+      td.filterMode = cudaFilterModeLinear;
+      td.readMode = cudaReadModeElementType;
+      td.normalizedCoords = 1;
+      PSC_CUDA(cudaCreateTextureObject(&c->tex_lut[kind], &rd, &td, nullptr), "sky-view texture object");
+    }
+    PSC_CUDA(cudaMemcpy2DToArray(c->arr_sky, 0, 0, c->d_lut[kind], row, row, PSC_SKYVIEW_H,
+                                 cudaMemcpyDeviceToDevice), "sky-view array copy");
+  }
   c->have_lut[kind] = true;
   return PSC_OK;
 }
@@ -628,14 +704,8 @@ int fill_batch(const psc_ctx* c, const PscBatchView* views, uint32_t n, const Ps
   const size_t fl = psc::frame_lite_size();
   for (uint32_t i = 0; i < n; ++i) {
     const PscBatchView& bv = views[i];
-    PscCloudParamsGpu p = bv.params;
-    p.cloud_layer_count = bv.n_layers;
-    PscCloudLayerGpu layers[8];
-    std::memset(layers, 0, sizeof(layers));
-    for (uint32_t l = 0; l < bv.n_layers; ++l) layers[l] = bv.layers[l];
-    build_uniforms_for(c, p, layers, bv.frame, bv.width, bv.height, hu[i]);
-    hu[i].lut_sky = sky + (size_t)i * PSC_SKYVIEW_W * PSC_SKYVIEW_H;
-    hu[i].lut_ap = ap + (size_t)i * PSC_AP_W * PSC_AP_H * PSC_AP_D;
+    build_batch_view_uniforms(c, bv, sky + (size_t)i * PSC_SKYVIEW_W * PSC_SKYVIEW_H,
+                              ap + (size_t)i * PSC_AP_W * PSC_AP_H * PSC_AP_D, hu[i]);
     hv[i] = psc::ViewDev{bv.width, bv.height, 0, 0, bv.depth, reinterpret_cast<float4*>(bv.out_luminance),
                          reinterpret_cast<float4*>(bv.out_transmittance), reinterpret_cast<float4*>(bv.hdr)};
     psc::frame_lite_from(bv.frame, static_cast<char*>(hframes) + i * fl);
@@ -1042,11 +1112,18 @@ int psc_destroy(psc_ctx* c) {
   dfree(c->d_detail_u8);
   dfree(c->d_base_store);
   dfree(c->d_detail_store);
+  dfree(c->d_base_fold);
+  dfree(c->d_base_quad);
+  dfree(c->d_detail_fold);
+  dfree(c->d_detail_quad);
+  dfree(c->d_curl_quad);
   dfree(c->d_curl);
   dfree(c->d_blue);
   dfree(c->d_weather);
   dfree(c->d_type);
   for (int k = 0; k < 4; ++k) {
+    if (c->tex_lut[k]) cudaDestroyTextureObject(c->tex_lut[k]);
+    if (k == PSC_LUT_SKYVIEW && c->arr_sky) cudaFreeArray(c->arr_sky);
     dfree(c->d_lut[k]);
     dfree(c->d_lut_h[k]);
   }

@@ -105,6 +105,13 @@ struct alignas(16) MarchUniforms {
   const float4* lut_sky;       // 192x108
   const float4* lut_ap;        // 32x32x64
   cudaTextureObject_t tex_base, tex_detail;  // PSC_FILTER_TEXTURE only
+  // F16 storage in the FAST schedule: channel-folded volumes (R, fbm) and
+  // (detail fbm) as 2x2 quads per entry (noise_bake.cu:k_fold_*)
+  const uint4* base_quad;
+  const uint2* detail_quad;
+  const uint4* curl_quad;      // FAST schedule: curl tile as 2x2 (R, G) half quads
+  // transmittance / sky-view LUTs through the texture unit; 0 = plain loads
+  cudaTextureObject_t tex_trans, tex_sky;
   int* error_word;             // device, debug checks
 };
 

@@ -51,12 +51,17 @@ def _run_batch(views, noise, tuning=(128, 16, 0), reps=1):
     return out
 
 
-def _compare(views, got, noise, rtol=2e-6):
+def _compare(views, got, noise, rtol=5e-5):
+    """Transmittance must be bit-identical (same density path); luminance
+    may differ by rounding only: the two kernels are separate translation
+    units, and the assembler is free to fuse a multiply and an add into one
+    FMA in one of them and not the other (observed: <= 1.3e-5 relative)."""
     worst = 0.0
     for s, (L, T) in zip(views, got):
         L1, T1 = _single(s, noise)
+        assert np.array_equal(T, T1)
         d = np.abs(L - L1)[..., :3] / np.maximum(np.abs(L1[..., :3]), 1.0)
-        worst = max(worst, float(d.max()), float(np.abs(T - T1).max()))
+        worst = max(worst, float(d.max()))
     assert worst <= rtol, worst
     return worst
 
