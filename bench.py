@@ -35,6 +35,23 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Mrays/s at 1080p, FP16-stored vs FP32 march at <=1e-3 rel err; % L2/tex roofline"
 UNIT = "Mrays/s"
 WORKLOAD = "precision_1080p"
+# Frame workloads: name -> (default size, frames per step, description).
+FRAME_WORKLOADS = {
+    "precision_1080p": ((1920, 1080), 1, {"layers": "Cu 1500-2300 cov 0.5; As 4000-5000 cov 0.7; "
+                                                    "Ci 8000-9000 cov 0.3", "primary_steps": 128,
+                                          "light_steps": 6}),
+    "stress_2160p": ((3840, 2160), 8, {"layers": "Cb 600-12000 cov 0.8 x 2048^2 f32 coverage grid",
+                                       "primary_steps": 256, "light_steps": 8,
+                                       "frames": "8, simulated_seconds 0..7, 15 m/s wind"}),
+}
+
+
+def frame_scenes(workload, W, H, **kw):
+    """The scenes of one step of a frame workload."""
+    from pedalsky_b200 import scenes
+    if workload == "stress_2160p":
+        return [scenes.stress_2160p(W, H, frame_index=k, **kw) for k in range(8)]
+    return [scenes.precision_1080p(W, H, **kw)]
 
 
 def parse():
@@ -48,12 +65,13 @@ def parse():
     ap.add_argument("--filter", default="hybrid", choices=["exact", "texture", "hybrid"])
     ap.add_argument("--no-plain-reference", action="store_true",
                     help="skip timing the plain FP32-storage drop-in kernel for the speed-up ratio")
-    ap.add_argument("--width", type=int, default=1920)
-    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--width", type=int, default=None, help="default: the workload's size")
+    ap.add_argument("--height", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="precision_1080p",
-                    choices=["precision_1080p", "batch_64", "grid_512"],
-                    help="batch_64: the 64-view uneven batch in one persistent kernel")
+                    choices=["precision_1080p", "stress_2160p", "batch_64", "grid_512"],
+                    help="stress_2160p: eight 4K frames of a Cumulonimbus over a 2048^2 coverage "
+                         "grid; batch_64: the 64-view uneven batch in one persistent kernel")
     ap.add_argument("--batch-views", type=int, default=64)
     return ap.parse_args()
 
@@ -118,25 +136,51 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def bytes_per_ray(storage: str) -> dict:
-    """Algorithmic texel bytes per primary ray of this workload (executed
-    fetches counted by the instrumented CPU restatement on the same scene,
-    committed in tests/golden/fetch_counts.json) in this kernel's formats."""
+def bytes_per_ray(storage: str, schedule: str = "fast", workload: str = WORKLOAD) -> dict:
+    """Algorithmic texel bytes per primary ray of this workload: executed
+    fetches counted by the instrumented CPU restatement on the same scene
+    (tests/golden/fetch_counts.json) times texels per fetch (bilinear 4,
+    trilinear 8, load 1) times the bytes per texel of the form the kernel
+    reads.  The FAST schedule with FP16 storage reads channel-folded volumes:
+    base (R, fbm) 4 B and detail (fbm) 2 B per texel, the curl tile as (R, G)
+    half pairs 4 B per texel; other forms read RGBA texels (4 B for RGBA8
+    and FP8, 8 B for FP16/BF16, 16 B for FP32).  LUT texels are RGBA32F.
+    Outputs: L and T written, the HDR target read and written (64 B)."""
     p = ROOT / "tests" / "golden" / "fetch_counts.json"
     if not p.exists():
         return {}
-    d = json.loads(p.read_text()).get(WORKLOAD)
+    d = json.loads(p.read_text()).get(workload)
     if not d:
         return {}
-    tex = {"u8": 4, "fp8": 4, "f16": 8, "bf16": 8, "f32": 16}[storage]
     c = d["counts"]
+    if schedule == "fast" and storage == "f16":
+        base_b, detail_b, curl_b = 4, 2, 4
+    else:
+        base_b = detail_b = {"u8": 4, "fp8": 4, "f16": 8, "bf16": 8, "f32": 16}[storage]
+        curl_b = 2
     per_kind = {
-        "weather": 4 * 4, "type": 1, "base": 8 * tex, "curl": 4 * 2, "detail": 8 * tex,
-        "light": 8 * tex, "trans": 4 * 16, "sky": 4 * 16, "ap": 8 * 16, "blue": 4, "depth": 4,
+        "weather": 4 * 4, "base": 8 * base_b, "curl": 4 * curl_b, "detail": 8 * detail_b,
+        "light": 8 * base_b, "trans": 4 * 16, "sky": 4 * 16, "ap": 8 * 16, "blue": 4, "depth": 4,
     }
-    total = sum(c[k] * v for k, v in per_kind.items()) + c["pixels"] * (32 + 32)
+    total = sum(c[k] * v for k, v in per_kind.items()) + c["pixels"] * 64
     return {"bytes_per_ray": total / c["pixels"], "pixels": c["pixels"],
-            "dense_per_ray": c["dense"] / c["pixels"], "steps_per_ray": c["steps"] / c["pixels"]}
+            "dense_per_ray": c["dense"] / c["pixels"], "steps_per_ray": c["steps"] / c["pixels"],
+            "light_fetches_per_ray": c["light"] / c["pixels"]}
+
+
+# DRAM bytes (read + write) per launch of the timed kernel, from one ncu
+# capture of the benchmark command (profiles/k_march_fast_f16_hybrid_1080p.md).
+DRAM_TRAFFIC_PER_LAUNCH = {("precision_1080p", "fast", "f16", "hybrid", 1920, 1080): 112875520}
+
+
+def fetch_peaks(device: int) -> dict:
+    """L2 / L1 read bandwidth and trilinear texture fetch rate of this GPU,
+    measured by the library's calibration kernels (psc_measure_fetch_peaks)."""
+    from pedalsky_b200 import capi
+    fp = capi.FetchPeaks()
+    capi.call("psc_measure_fetch_peaks", device, C.byref(fp), None)
+    return {"l2_read_gbs": fp.l2_read_gbs, "l1_read_gbs": fp.l1_read_gbs,
+            "tex_trilinear_gfetch_s": fp.tex_trilinear_gfetch_s}
 
 
 def cpu_baseline(scene, sample_rows: int, reps: int = 1):
@@ -204,9 +248,11 @@ def run_reference(args):
         return 0
     if args.workload == "grid_512":
         return run_reference_grid(args)
-    from pedalsky_b200 import scenes
-    s = scenes.precision_1080p(args.width, args.height)
-    sample = 64  # rows per step
+    wl = args.workload if args.workload in FRAME_WORKLOADS else WORKLOAD
+    (dw, dh), n_frames, desc = FRAME_WORKLOADS[wl]
+    W, H = args.width or dw, args.height or dh
+    s = frame_scenes(wl, W, H)[0]
+    sample = 64 if wl == WORKLOAD else 32  # rows per step
     for _ in range(args.warmup):
         cpu_baseline(s, sample)
     vals = []
@@ -216,16 +262,15 @@ def run_reference(args):
     value = float(np.median(vals)) / 1e6
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * args.width * args.height / (value * 1e6),
+        "warmup": args.warmup, "ms_per_step": 1e3 * n_frames * W * H / (value * 1e6),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded reference noise hash, reference synthesis)",
         "impl": "reference",
-        "config": {"workload": f"{WORKLOAD} {args.width}x{args.height}", "layers": 3,
-                   "primary_steps": 128, "light_steps": 6,
+        "config": {"workload": f"{wl} {W}x{H}", **desc,
                    "note": "CPU restatement of the reference FP32 march (the reference's WGSL "
                            "cannot run here: no graphics stack)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{rays} rays per step (8 row bands of the 1080p frame)"},
+                         "sample": f"{rays} rays per step (8 row bands of the first frame)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -249,10 +294,14 @@ def run_ours(args):
     storage = capi.STORAGE_NAMES[args.storage]
     schedule = capi.SCHED_FAST if args.schedule == "fast" else capi.SCHED_PLAIN
     filt = capi.FILTER_NAMES[args.filter]
-    W, H = args.width, args.height
-    # each rank renders frame `rank` of the sequence (weak scaling)
-    s = scenes.precision_1080p(W, H, storage=storage, schedule=schedule, filt=filt)
-    s.frame.frame_index = rank
+    wl = args.workload
+    (dw, dh), n_frames, desc = FRAME_WORKLOADS[wl]
+    W, H = args.width or dw, args.height or dh
+    # each rank renders its own frame(s) of the sequence (weak scaling)
+    frames = frame_scenes(wl, W, H, storage=storage, schedule=schedule, filt=filt)
+    for f in frames:
+        f.frame.frame_index += rank * n_frames
+    s = frames[0]
     sub = subsystem_for_scene(s, device=local, luts=None)  # noise + LUTs baked on the device
     stream = torch.cuda.Stream(device=dev)
     sh = C.c_void_p(stream.cuda_stream)
@@ -268,12 +317,20 @@ def run_ours(args):
     sub.set_options(o)
     view = capi.View(W, H, depth.data_ptr(), L.data_ptr(), T.data_ptr(), hdr.data_ptr())
 
+    def render_step():
+        """One step: every frame of the workload (the frames differ only in
+        simulated time, so the sky-view and AP LUTs stay valid)."""
+        for f in frames:
+            if n_frames > 1:
+                call("psc_set_frame", sub.handle, C.byref(f.frame), C.byref(f.world))
+            hdr.copy_(bg, non_blocking=True)
+            call("psc_render", sub.handle, C.byref(view), 1, sh)
+
     def timed_steps(clk=None):
         """W untimed steps, then K device-timed steps (L2 flushed before each)."""
         with torch.cuda.stream(stream):
             for _ in range(args.warmup):
-                hdr.copy_(bg, non_blocking=True)
-                call("psc_render", sub.handle, C.byref(view), 1, sh)
+                render_step()
         torch.cuda.synchronize()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(args.steps)]
@@ -284,9 +341,8 @@ def run_ours(args):
             with torch.cuda.stream(stream):
                 for i in range(args.steps):
                     flush.zero_()                      # evict L2 between timed steps
-                    hdr.copy_(bg, non_blocking=True)
                     evs[i][0].record(stream)
-                    call("psc_render", sub.handle, C.byref(view), 1, sh)
+                    render_step()
                     evs[i][1].record(stream)
             torch.cuda.synchronize()
         ms_list = [a.elapsed_time(b) for a, b in evs]
@@ -295,11 +351,17 @@ def run_ours(args):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return ms_list, float(t.item())
 
+    peaks_fetch = None
+    try:
+        peaks_fetch = fetch_peaks(local)
+    except Exception as e:  # the calibration is reported, never required
+        print(f"fetch-peak calibration failed: {e}", file=sys.stderr)
     launches0 = sub.launch_count()
     clk = ClockSampler(local)
     step_ms, ms_max = timed_steps(clk)
     kernel_launches = sub.launch_count() - launches0
-    value = world * W * H / (ms_max * 1e-3) / 1e6
+    rays_step = n_frames * W * H
+    value = world * rays_step / (ms_max * 1e-3) / 1e6
 
     # the plain FP32-storage drop-in kernel on the same frame, for the ratio
     plain = None
@@ -310,7 +372,7 @@ def run_ours(args):
         sub.set_options(o_plain)
         _, ms_plain = timed_steps()
         sub.set_options(o)
-        plain = {"value": world * W * H / (ms_plain * 1e-3) / 1e6, "ms_per_step": ms_plain,
+        plain = {"value": world * rays_step / (ms_plain * 1e-3) / 1e6, "ms_per_step": ms_plain,
                  "config": "plain schedule, f32 storage, exact filtering"}
 
     # end to end through the C ABI with host buffers: pinned H2D of the
@@ -324,10 +386,13 @@ def run_ours(args):
             flush.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            hdr.copy_(h_bg, non_blocking=True)
-            depth.copy_(h_depth, non_blocking=True)
-            call("psc_render", sub.handle, C.byref(view), 1, sh)
-            h_out.copy_(hdr, non_blocking=True)
+            for f in frames:
+                if n_frames > 1:
+                    call("psc_set_frame", sub.handle, C.byref(f.frame), C.byref(f.world))
+                hdr.copy_(h_bg, non_blocking=True)
+                depth.copy_(h_depth, non_blocking=True)
+                call("psc_render", sub.handle, C.byref(view), 1, sh)
+                h_out.copy_(hdr, non_blocking=True)
             b.record(stream)
             b.synchronize()
             if i >= args.warmup:
@@ -335,9 +400,9 @@ def run_ours(args):
     te = torch.tensor([float(np.mean(e2e_ms))], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * W * H / (float(te.item()) * 1e-3) / 1e6
-    h2d = h_bg.numel() * 4 + h_depth.numel() * 4
-    d2h = h_out.numel() * 4
+    e2e_value = world * rays_step / (float(te.item()) * 1e-3) / 1e6
+    h2d = n_frames * (h_bg.numel() * 4 + h_depth.numel() * 4)
+    d2h = n_frames * h_out.numel() * 4
 
     if rank == 0:
         peaks = {}
@@ -345,23 +410,38 @@ def run_ours(args):
         if pk.exists():
             peaks = json.loads(pk.read_text())
         hbm = peaks.get("hbm_gbs")
-        bpr = bytes_per_ray(args.storage)
+        bpr = bytes_per_ray(args.storage, args.schedule, wl)
         roof = None
         if bpr:
-            achieved = bpr["bytes_per_ray"] * W * H / (ms_max * 1e-3) / 1e9
+            achieved = bpr["bytes_per_ray"] * rays_step / (ms_max * 1e-3) / 1e9
             peak = hbm if hbm else 6650.0
+            traffic = DRAM_TRAFFIC_PER_LAUNCH.get((wl, args.schedule, args.storage, args.filter, W, H))
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "traffic": None,
+                    "frac": achieved / peak, "traffic": traffic,
                     "peak_source": "measured" if hbm else "fallback",
-                    "bytes_per_ray": bpr["bytes_per_ray"],
-                    "note": "algorithmic texel bytes of executed fetches; the noise/LUT working "
-                            "set is L2-resident, so these are served from L1/L2, not HBM"}
+                    "bytes_per_ray": bpr["bytes_per_ray"], "kernel": "k_march_fast",
+                    "note": "achieved = algorithmic texel bytes of the executed fetches per launch / "
+                            "kernel time.  The noise/LUT working set is L2-resident, so these bytes "
+                            "are served by L1/TEX and L2, not HBM (DRAM traffic per launch is "
+                            "`traffic`); `fetch` relates them to the on-chip ceilings measured on "
+                            "this GPU"}
+            if peaks_fetch:
+                light_rate = bpr["light_fetches_per_ray"] * rays_step / (ms_max * 1e-3) / 1e9
+                roof["fetch"] = {
+                    "l2_read_peak_gbs": peaks_fetch["l2_read_gbs"],
+                    "frac_of_l2_read": achieved / peaks_fetch["l2_read_gbs"],
+                    "l1_read_peak_gbs": peaks_fetch["l1_read_gbs"],
+                    "frac_of_l1_read": achieved / peaks_fetch["l1_read_gbs"],
+                    "tex_trilinear_peak_gfetch_s": peaks_fetch["tex_trilinear_gfetch_s"],
+                    "light_march_gfetch_s": light_rate,
+                    "frac_of_tex_trilinear": light_rate / peaks_fetch["tex_trilinear_gfetch_s"],
+                    "source": "psc_measure_fetch_peaks, this run"}
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             try:
-                v, rays, threads, secs = cpu_baseline(s, 64)
+                v, rays, threads, secs = cpu_baseline(s, 64 if wl == WORKLOAD else 32)
                 cpu = {"value": v / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-                       "sample": f"{rays} rays (8 row bands of the 1080p frame), {secs:.1f} s"}
+                       "sample": f"{rays} rays (8 row bands of the first {W}x{H} frame), {secs:.1f} s"}
             except Exception as e:  # the baseline is reported, never the product
                 cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                        "sample": f"failed: {e}"}
@@ -370,8 +450,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded reference noise hash, reference synthesis)",
-            "config": {"workload": f"{WORKLOAD} {W}x{H}", "layers": 3, "primary_steps": 128,
-                       "light_steps": 6, "storage": args.storage, "schedule": args.schedule,
+            "config": {"workload": f"{wl} {W}x{H}", **desc, "storage": args.storage,
+                       "schedule": args.schedule,
                        "filter": args.filter, "composite": "fused",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"views{world}"},

@@ -497,6 +497,21 @@ int psc_adjoint(psc_ctx* ctx, const PscDensityGrid* grid, const PscView* view,
 #define PSC_NOALLOC_MAX_VIEWS 64u
 #define PSC_NOALLOC_MAX_TILES (1u << 20)
 
+/* No counterpart in the reference.  Calibration of the fetch roofline the
+ * march is measured against (its working set is L2-resident, so its ceilings
+ * are on-chip): L2 read bandwidth (16-byte L2-only loads streaming a 64 MiB
+ * resident buffer), L1 read bandwidth (16-byte loads that hit in L1) and the
+ * trilinear fetch rate of a two-channel FP16 3D texture (the light march's
+ * fetch), each saturated from every SM.  Allocates and frees its own
+ * buffers; takes about 0.1 s. */
+typedef struct PscFetchPeaks {
+  float l2_read_gbs;
+  float l1_read_gbs;
+  float tex_trilinear_gfetch_s;  /* 10^9 trilinear fetches per second */
+  float _reserved;
+} PscFetchPeaks;
+int psc_measure_fetch_peaks(int cuda_device, PscFetchPeaks* out, void* stream);
+
 /* No counterpart in the reference (which allocates its GPU resources through
  * wgpu at set-up).  psc_render_batch with no allocation at call time, for
  * callers that cannot call cudaMalloc while rendering: a real-time frame loop

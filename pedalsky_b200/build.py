@@ -31,6 +31,7 @@ CUDA_UNITS = {
     "grid_march.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
+    "fetch_peak.cu": [],
 }
 CXX_UNITS = ["psc_host.cpp"]
 

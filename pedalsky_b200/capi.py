@@ -149,6 +149,11 @@ class DensityGrid(C.Structure):
 assert C.sizeof(DensityGrid) == 48
 
 
+class FetchPeaks(C.Structure):
+    _fields_ = [("l2_read_gbs", f32), ("l1_read_gbs", f32), ("tex_trilinear_gfetch_s", f32),
+                ("_reserved", f32)]
+
+
 class PscError(RuntimeError):
     def __init__(self, code: int, func: str, msg: str):
         super().__init__(f"{func}: {PSC_ERR.get(code, code)} ({code}): {msg}")
@@ -197,6 +202,7 @@ _PROTOS = {
     "psc_autotune_batch": [_vp, P(BatchView), u32, u32, P(BatchTuning), P(C.c_float), _vp],
     "psc_render_grid": [_vp, P(DensityGrid), P(View), _vp],
     "psc_adjoint": [_vp, P(DensityGrid), P(View), _vp, _vp, _vp, _vp, _vp, _vp],
+    "psc_measure_fetch_peaks": [i32, P(FetchPeaks), _vp],
 }
 _RESTYPES = {
     "psc_last_error": C.c_char_p, "psc_abi_version": u32, "psc_sizeof_params": C.c_size_t,

@@ -4,7 +4,8 @@
 
 fetch_counts.json  executed-fetch counts per kind (instrumented FP64 CPU
                    restatement) for each benchmark workload, the voxel-grid
-                   one included; bench.py turns them into algorithmic bytes
+                   one included (the stress workload's first frame stands for
+                   its eight); bench.py turns them into algorithmic bytes
                    per ray.
 plain_96x54.npz    FP64-oracle L/T of the plain workload at 96x54 (float32),
 precision_96x54.npz  and of the three-layer workload; the GPU parity tests
@@ -31,7 +32,8 @@ def main():
     noise = pyoracle.bake_noise()
     counts = {}
     for name, make in (("precision_1080p", lambda: scenes.precision_1080p()),
-                       ("plain_320x180", lambda: scenes.plain_320x180())):
+                       ("plain_320x180", lambda: scenes.plain_320x180()),
+                       ("stress_2160p", lambda: scenes.stress_2160p(frame_index=0))):
         s = make()
         luts = pyoracle.bake_luts(s.frame, s.world)
         _, _, c = pyoracle.render(s, noise, luts, precision=pyoracle.FP64, counters=True)

@@ -330,3 +330,35 @@ def test_row_bands_reassemble_the_full_frame(oracle_noise, sched):
         call("psc_render", sub.handle, C.byref(bad), 1, None)
     sub.close()
     assert np.array_equal(out_L, whole_L) and np.array_equal(out_T, whole_T)
+
+
+@pytest.fixture(scope="module")
+def stress_refs(oracle, oracle_noise):
+    """FP64 references of the stress workload (Cumulonimbus 600-12000 m over
+    the 2048^2 FP32 coverage grid, 256 + 8 steps) at 384x216, for the first
+    and last of its eight frames (wind drift after 0 s and 7 s at 15 m/s)."""
+    out = {}
+    for fi in (0, 7):
+        s = scenes.stress_2160p(384, 216, frame_index=fi)
+        luts = oracle.bake_luts(s.frame, s.world)
+        L, T = oracle.render(s, oracle_noise, luts)
+        out[fi] = (luts, composite(L, T, s.background))
+    return out
+
+
+@pytest.mark.parametrize("fi", [0, 7])
+@pytest.mark.parametrize("sched,storage,filt", [
+    ("plain", "f32", "exact"), ("fast", "f16", "exact"), ("fast", "f16", "hybrid")])
+def test_stress_cumulonimbus_coverage_grid(stress_refs, oracle_noise, fi, sched, storage, filt):
+    luts, ref = stress_refs[fi]
+    s = scenes.stress_2160p(384, 216, frame_index=fi, schedule=SCHEDULES[sched],
+                            storage=capi.STORAGE_NAMES[storage], filt=capi.FILTER_NAMES[filt])
+    _, _, hdr = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
+    _check(f"stress_384x216/frame{fi}/{sched}/{storage}/{filt}", hdr, ref)
+
+
+def test_stress_frames_differ_by_wind_drift(stress_refs):
+    """The eight frames are not one image: 7 s of 15 m/s drift moves the
+    clouds (guards against the simulated time being ignored)."""
+    a, b = stress_refs[0][1], stress_refs[7][1]
+    assert rel_stats(a, b)["p99"] > 1e-3
