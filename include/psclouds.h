@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PSC_ABI_VERSION 1u
+#define PSC_ABI_VERSION 2u
 
 /* ---------------------------------------------------------------- status */
 enum {
@@ -68,6 +68,7 @@ enum {
 #define PSC_WIND_Y 16u
 #define PSC_WIND_Z 32u
 #define PSC_TYPE_SENTINEL 255u           /* cloud_type_grid.rs SENTINEL     */
+#define PSC_MAX_CLOUD_VIEWS 2u           /* lib.rs:69, TAA history slots    */
 
 /* ------------------------------------------------- byte-exact uniforms */
 
@@ -208,7 +209,11 @@ typedef struct PscMarchOptions {
   uint32_t debug_checks;    /* 1: bounds-check every texel index          */
   uint32_t tile_w;          /* CTA tile width in pixels (0 = default)     */
   uint32_t tile_h;          /* CTA tile height in pixels (0 = default)    */
-  uint32_t _reserved[4];
+  uint32_t half_res;        /* 1: half-res march + Catmull-Rom composite
+                               (CloudsTuning::half_res_render)            */
+  uint32_t taa;             /* 1: TAA resolve of the cloud RT
+                               (temporal_taa && !freeze_time)             */
+  uint32_t _reserved[2];
 } PscMarchOptions;
 
 /* One view to render: a width x height rectangle of pixels.  By default
@@ -383,8 +388,52 @@ int psc_download_lut(psc_ctx* ctx, int kind, uint16_t* rgba16f, size_t count);
 /* March `n` views (each with the context's frame uniforms rescaled to the
  * view size) and write L/T per pixel — the `clouds::march` pass
  * (crates/ps-clouds/src/lib.rs:736-994).  With options.composite = 1 the
- * `clouds::composite` blend is fused into the same kernel. */
+ * `clouds::composite` blend is fused into the same kernel.
+ *
+ * With options.half_res or options.taa the call runs the reference's three
+ * passes for ONE view (n = 1) covering its whole viewport: the march into
+ * the context's cloud RT (psc_cloud_rt_size: floor(w/2) x floor(h/2) at
+ * half res, the depth read at the scaled position as the patched march
+ * does, crates/ps-clouds/src/pipeline.rs:277-319), the TAA resolve of the
+ * active view (psc_taa_resolve) when options.taa, and, with
+ * options.composite = 1, the composite into hdr (width x height): the
+ * 9-tap Catmull-Rom reconstruction at half res
+ * (cloud_composite_halfres.wgsl:60-126), the plain blend otherwise.
+ * out_luminance / out_transmittance, when not null, receive the resolved
+ * cloud RT (cloud-RT size, RGBA32F). */
 int psc_render(psc_ctx* ctx, const PscView* views, uint32_t n, void* stream);
+
+/* Cloud-RT size for a width x height target: ((w as f32 * 0.5) as u32).max(1)
+ * per axis with half_res (crates/ps-clouds/src/lib.rs:751-758), else w x h. */
+int psc_cloud_rt_size(uint32_t width, uint32_t height, uint32_t half_res, uint32_t* rt_width,
+                      uint32_t* rt_height);
+
+/* `clouds::taa` (shaders/clouds/cloud_taa.wgsl:81-197) of the active view:
+ * reprojects each pixel at infinite depth through the frame's
+ * prev_view_proj, samples the view's history bilinearly, clamps it into the
+ * 3x3 neighbourhood AABB of the current RT and blends 1/8 current (the
+ * first frame after enabling, a resize or psc_invalidate_taa_history
+ * outputs the current sample).  Ping-pong history lives in the context
+ * (per view, lib.rs:776-825); the resolve is also copied to out_l / out_t
+ * when not null.  Buffers are w x h RGBA32F on the device. */
+int psc_taa_resolve(psc_ctx* ctx, const float* cur_luminance, const float* cur_transmittance,
+                    uint32_t width, uint32_t height, float* out_luminance,
+                    float* out_transmittance, void* stream);
+
+/* Select the view whose TAA history later calls use, clamped to
+ * PSC_MAX_CLOUD_VIEWS - 1 (set_active_view, lib.rs:722). */
+int psc_set_active_view(psc_ctx* ctx, uint32_t view);
+
+/* Discard every view's TAA history (invalidate_taa_history, lib.rs:729). */
+int psc_invalidate_taa_history(psc_ctx* ctx);
+
+/* Half-res `clouds::composite` (cloud_composite_halfres.wgsl:110-126):
+ * Catmull-Rom reconstruction of an rt_width x rt_height cloud RT at every
+ * pixel of the width x height hdr target, L >= 0, T in [0, 1], then
+ * hdr.rgba = L.rgba + hdr.rgba * T.rgba. */
+int psc_composite_halfres(const float* luminance, const float* transmittance, uint32_t rt_width,
+                          uint32_t rt_height, float* hdr, uint32_t width, uint32_t height,
+                          void* stream);
 
 /* `clouds::composite` (cloud_composite.wgsl:48-57, blend One/Src1,
  * pipeline.rs:469-484): hdr.rgba = L.rgba + hdr.rgba * T.rgba. */

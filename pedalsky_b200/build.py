@@ -32,6 +32,7 @@ CUDA_UNITS = {
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
     "fetch_peak.cu": [],
+    "post.cu": [],
 }
 CXX_UNITS = ["psc_host.cpp"]
 

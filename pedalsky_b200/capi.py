@@ -96,7 +96,8 @@ class MarchOptions(C.Structure):
     _fields_ = [
         ("phase_mode", u32), ("hg_g_forward", f32), ("hg_g_backward", f32), ("hg_blend", f32),
         ("storage", u32), ("filter", u32), ("schedule", u32), ("kahan", u32), ("composite", u32),
-        ("debug_checks", u32), ("tile_w", u32), ("tile_h", u32), ("_reserved", u32 * 4),
+        ("debug_checks", u32), ("tile_w", u32), ("tile_h", u32), ("half_res", u32), ("taa", u32),
+        ("_reserved", u32 * 2),
     ]
 
 
@@ -203,6 +204,11 @@ _PROTOS = {
     "psc_render_grid": [_vp, P(DensityGrid), P(View), _vp],
     "psc_adjoint": [_vp, P(DensityGrid), P(View), _vp, _vp, _vp, _vp, _vp, _vp],
     "psc_measure_fetch_peaks": [i32, P(FetchPeaks), _vp],
+    "psc_cloud_rt_size": [u32, u32, u32, P(u32), P(u32)],
+    "psc_taa_resolve": [_vp, _vp, _vp, u32, u32, _vp, _vp, _vp],
+    "psc_set_active_view": [_vp, u32],
+    "psc_invalidate_taa_history": [_vp],
+    "psc_composite_halfres": [_vp, _vp, u32, u32, _vp, u32, u32, _vp],
 }
 _RESTYPES = {
     "psc_last_error": C.c_char_p, "psc_abi_version": u32, "psc_sizeof_params": C.c_size_t,

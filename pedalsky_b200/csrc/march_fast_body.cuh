@@ -442,7 +442,10 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
     lr.step = step;
     lr.one_minus_eff = 1.0f - eff;
     if (type == 7u) return light_march_tex<ST>(u, L, lr, NdfCb{L.anvil_bias});
-    return light_march_tex<ST>(u, L, lr, NdfGeneral{ndf_coef(type)});
+    return light_march_tex<ST>(
+        u, L, lr,
+        NdfGeneral{u.type_grid ? ndf_coef(type)
+                               : NdfCoef{L.ndf_inv_a, L.ndf_e1, L.ndf_inv_w1, L.ndf_mode == 2u}});
   }
   float od = 0.0f, comp = 0.0f;
   for (uint32_t i = 0; i < u.light_steps; ++i) {
@@ -492,7 +495,8 @@ __device__ __forceinline__ float3 sky_fast(const MarchUniforms& u, float alt, fl
   const float a = fmaxf(alt, 0.0f);
   const float rho = sqrtf(a * (2.0f * R + a));
   const float vza = fast_atan2(sqrtf(fmaf(ux, ux, uz * uz)), uy);
-  const float zha = 1.57079632679f + fast_atan2(rho, R);
+  // pi/2 + atan2(rho, R) with rho < R (altitudes below 2600 km)
+  const float zha = 1.57079632679f + atan01(fminf(__fdividef(rho, R), 1.0f));
   float vv;
   if (vza < zha) {
     vv = sqrtf(clamp01(__fdividef(vza, fmaxf(zha, 1e-6f)))) * 0.5f;
@@ -505,9 +509,17 @@ __device__ __forceinline__ float3 sky_fast(const MarchUniforms& u, float alt, fl
   return make_float3(s.x * u.sun_illum[0], s.y * u.sun_illum[1], s.z * u.sun_illum[2]);
 }
 
-// Weather R channel, repeat + bilinear; power-of-two sizes wrap with a mask.
+// Weather R channel, repeat + bilinear; power-of-two sizes wrap with a mask,
+// and up to 1024^2 read one 16-byte 2x2 footprint per tap.
 __device__ __forceinline__ float weather_fast(const MarchUniforms& u, float uu, float vv) {
   const uint32_t W = u.weather_w, H = u.weather_h;
+  if (u.weather_quad) {
+    const float x = fmaf(uu, (float)W, -0.5f), y = fmaf(vv, (float)H, -0.5f);
+    const float fx = floorf(x), fy = floorf(y);
+    const float wx = x - fx, wy = y - fy;
+    const float4 q = __ldg(u.weather_quad + ((uint32_t)(int)fy & (H - 1)) * W + ((uint32_t)(int)fx & (W - 1)));
+    return lerpf(lerpf(q.x, q.y, wx), lerpf(q.z, q.w, wx), wy);
+  }
   if (((W & (W - 1)) | (H & (H - 1))) != 0) return weather_sample(u.weather, W, H, uu, vv);
   const float x = fmaf(uu, (float)W, -0.5f), y = fmaf(vv, (float)H, -0.5f);
   const float fx = floorf(x), fy = floorf(y);
@@ -544,7 +556,9 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
     s_t1[j * stride + slot] = rs.t1[j];
   }
   const uint32_t order = rs.order, hit_mask = rs.hit_mask;
-  const float ray_r0 = rs.r0, ray_cv = rs.cos_view, ray_h0 = rs.h0;
+  const float ray_r0 = rs.r0, ray_h0 = rs.h0;
+  // distance from the planet centre along the ray: r(t)^2 = A + t (B + t)
+  const float ray_A = ray_r0 * ray_r0, ray_B = 2.0f * ray_r0 * rs.cos_view;
   const float dx = rs.dir[0], dy = rs.dir[1], dz = rs.dir[2];
   const float cx = u.cam[0], cy = u.cam[1], cz = u.cam[2];
   const float cos_theta = fmaf(dx, u.sun[0], fmaf(dy, u.sun[1], dz * u.sun[2]));
@@ -604,7 +618,8 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
     for (uint32_t s = 0; s < u.cloud_steps; ++s) {
       const float t = fmaf((float)s + jitter, step, t0);
       const float px3 = fmaf(dx, t, cx), py3 = fmaf(dy, t, cy), pz3 = fmaf(dz, t, cz);
-      const float alt = alt_from(u, px3, py3, pz3, ray_r0, ray_cv, ray_h0, t);
+      const float bt = ray_B + t;
+      const float alt = ray_h0 + __fdividef(t * bt, ray_r0 + sqrtf(fmaf(t, bt, ray_A)));
       const float h = (alt - L.base_m) * L.inv_thickness;
       if (h >= 0.0f && h <= 1.0f) {
         const float wsx = px3 - L.wind_off_x, wsz = pz3 - L.wind_off_z;
@@ -615,9 +630,12 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
         const float wr = weather_fast(u, fmaf(wsx, u.inv_weather_scale, 0.5f),
                                       fmaf(wsz, u.inv_weather_scale, 0.5f));
         const uint32_t type = effective_type(u, wsx, wsz, L.cloud_type);
-        const float2 bt = base_tap<ST, FILT, false>(u, ax, py3, az);
+        const float2 bs = base_tap<ST, FILT, false>(u, ax, py3, az);
         const float eff = clamp01(wr * L.coverage);
-        float cloud = shape_from(bt, L.lf_bias, ndf_fast(h, type, L.anvil_bias), 1.0f - eff);
+        const float nd = (!u.type_grid && L.ndf_mode)
+                             ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_e1, L.ndf_inv_w1, L.ndf_mode == 2u}, h)
+                             : ndf_fast(h, type, L.anvil_bias);
+        float cloud = shape_from(bs, L.lf_bias, nd, 1.0f - eff);
         if (eff >= 0.01f) {  // coverage gate (cloud_march.wgsl:450-451)
           if (cloud > 0.0f) {  // curl-perturbed detail erosion (:502-527)
             const float2 c2 = curl_quad_tap(u.curl_quad, fmaf(ax, u.curl_texel_scale, -0.5f),

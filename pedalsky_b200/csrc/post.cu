@@ -1,0 +1,199 @@
+// Passes between the cloud march and the HDR target (the reference's
+// clouds::taa and clouds::composite passes, crates/ps-clouds/src/lib.rs:
+// 1000-1097):
+//   * k_depth_halfres: the depth a half-res cloud-RT pixel (x, y) sees, the
+//     full-res texel at ivec2(vec2(x, y) * viewport / rt) (the half-res march
+//     patch, crates/ps-clouds/src/pipeline.rs:296-305);
+//   * k_taa_resolve: shaders/clouds/cloud_taa.wgsl:81-197 — reprojection at
+//     infinite depth through prev_view_proj (FP64), bilinear history, 3x3
+//     neighbourhood AABB clamp, blend, L >= 0 and T in [0, 1];
+//   * k_composite_halfres: shaders/clouds/cloud_composite_halfres.wgsl:60-126
+//     — Catmull-Rom (B = 0, C = 0.5) reconstruction of the half-res RT at each
+//     full-res pixel, evaluated as the 4x4 kernel on clamped texel indices
+//     (the reference's 9 offset-bilinear taps are an exact rewriting of it),
+//     then L >= 0, T in [0, 1] and dst = L + dst * T on all four channels.
+// All three are one thread per output pixel, 16x16 CTAs; every index is
+// clamped into its image.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "psc_internal.h"
+
+namespace psc {
+namespace {
+
+__device__ __forceinline__ int clampi(int i, int n) { return min(max(i, 0), n - 1); }
+__device__ __forceinline__ float4 f4(float a) { return make_float4(a, a, a, a); }
+__device__ __forceinline__ float4 add4(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 mul4(float4 a, float s) {
+  return make_float4(a.x * s, a.y * s, a.z * s, a.w * s);
+}
+__device__ __forceinline__ float4 fma4(float4 a, float s, float4 c) {
+  return make_float4(fmaf(a.x, s, c.x), fmaf(a.y, s, c.y), fmaf(a.z, s, c.z), fmaf(a.w, s, c.w));
+}
+__device__ __forceinline__ float4 min4(float4 a, float4 b) {
+  return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w));
+}
+__device__ __forceinline__ float4 max4(float4 a, float4 b) {
+  return make_float4(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
+}
+__device__ __forceinline__ float4 clamp4(float4 v, float4 lo, float4 hi) { return min4(max4(v, lo), hi); }
+
+__global__ void k_depth_halfres(const float* __restrict__ depth, uint32_t W, uint32_t H,
+                                float* __restrict__ out, uint32_t rw, uint32_t rh) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= rw || y >= rh) return;
+  const float sx = (float)W / (float)rw, sy = (float)H / (float)rh;
+  const uint32_t dx = min((uint32_t)((float)x * sx), W - 1u);
+  const uint32_t dy = min((uint32_t)((float)y * sy), H - 1u);
+  out[(size_t)y * rw + x] = __ldg(depth + (size_t)dy * W + dx);
+}
+
+// Bilinear, clamp-to-edge, FP32 weights, at normalised (u, v).
+__device__ __forceinline__ float4 bilinear_clamp(const float4* __restrict__ t, int w, int h, float u,
+                                                 float v) {
+  const float x = u * (float)w - 0.5f, y = v * (float)h - 0.5f;
+  const float fx = floorf(x), fy = floorf(y);
+  const float ax = x - fx, ay = y - fy;
+  const int x0 = clampi((int)fx, w), x1 = clampi((int)fx + 1, w);
+  const int y0 = clampi((int)fy, h), y1 = clampi((int)fy + 1, h);
+  const float4 a00 = __ldg(t + y0 * w + x0), a10 = __ldg(t + y0 * w + x1);
+  const float4 a01 = __ldg(t + y1 * w + x0), a11 = __ldg(t + y1 * w + x1);
+  const float4 a = add4(mul4(a00, 1.0f - ax), mul4(a10, ax));
+  const float4 b = add4(mul4(a01, 1.0f - ax), mul4(a11, ax));
+  return add4(mul4(a, 1.0f - ay), mul4(b, ay));
+}
+
+__global__ void k_taa_resolve(const TaaParams p) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= p.w || y >= p.h) return;
+  const int w = (int)p.w, h = (int)p.h;
+  const size_t i = (size_t)y * p.w + x;
+  const float4 cl = __ldg(p.cur_l + i), ct = __ldg(p.cur_t + i);
+  const float bw = fminf(fmaxf(p.blend_weight, 0.0f), 1.0f);
+  if (p.history_valid < 0.5f || bw >= 1.0f) {  // bootstrap: the current sample as is
+    p.out_l[i] = cl;
+    p.out_t[i] = ct;
+    return;
+  }
+  // reproject_uv (cloud_taa.wgsl:84-110): view direction of this pixel,
+  // projected with w = 0 (infinite depth) into the previous frame.  In FP64,
+  // as the march's ray set-up: the direction is the near-plane point (0.1 m
+  // ahead) minus the camera position, which cancels in FP32 and would move
+  // the history sample by hundredths of a pixel.
+  const double u = ((double)x + 0.5) / (double)w, v = ((double)y + 0.5) / (double)h;
+  const double nx = u * 2.0 - 1.0, ny = 1.0 - v * 2.0;
+  double nh[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    nh[r] = (((double)p.inv_vp[0][r] * nx + (double)p.inv_vp[1][r] * ny) + (double)p.inv_vp[2][r]) +
+            (double)p.inv_vp[3][r];
+  double d[3] = {nh[0] / nh[3] - (double)p.cam[0], nh[1] / nh[3] - (double)p.cam[1],
+                 nh[2] / nh[3] - (double)p.cam[2]};
+  const double il = 1.0 / sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  d[0] *= il;
+  d[1] *= il;
+  d[2] *= il;
+  double pc[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    pc[r] = ((double)p.prev_vp[0][r] * d[0] + (double)p.prev_vp[1][r] * d[1]) + (double)p.prev_vp[2][r] * d[2];
+  float pu = 0.0f, pv = 0.0f, inside = 0.0f;
+  if (pc[3] > 1e-4) {
+    const double du = (pc[0] / pc[3]) * 0.5 + 0.5, dv = 1.0 - ((pc[1] / pc[3]) * 0.5 + 0.5);
+    inside = (du >= 0.0 && dv >= 0.0 && du <= 1.0 && dv <= 1.0) ? 1.0f : 0.0f;
+    pu = (float)du;
+    pv = (float)dv;
+  }
+  float4 hl = bilinear_clamp(p.hist_l, w, h, pu, pv);
+  float4 ht = bilinear_clamp(p.hist_t, w, h, pu, pv);
+  // 3x3 neighbourhood AABB of the current frame (clamp_to_neighbourhood)
+  float4 mnl = f4(1e10f), mxl = f4(-1e10f), mnt = f4(1e10f), mxt = f4(-1e10f);
+#pragma unroll
+  for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int j = clampi((int)y + dy, h) * w + clampi((int)x + dx, w);
+      const float4 sl = __ldg(p.cur_l + j), st = __ldg(p.cur_t + j);
+      mnl = min4(mnl, sl);
+      mxl = max4(mxl, sl);
+      mnt = min4(mnt, st);
+      mxt = max4(mxt, st);
+    }
+  hl = clamp4(hl, mnl, mxl);
+  ht = clamp4(ht, mnt, mxt);
+  const float eb = 1.0f * (1.0f - inside) + bw * inside;  // mix(1, w, inside)
+  const float4 rl = add4(mul4(hl, 1.0f - eb), mul4(cl, eb));
+  const float4 rt = add4(mul4(ht, 1.0f - eb), mul4(ct, eb));
+  p.out_l[i] = max4(rl, f4(0.0f));
+  p.out_t[i] = clamp4(rt, f4(0.0f), f4(1.0f));
+}
+
+// Catmull-Rom weights of one axis at fraction f in [0, 1).
+__device__ __forceinline__ void cr_weights(float f, float w[4]) {
+  w[0] = f * (-0.5f + f * (1.0f - 0.5f * f));
+  w[1] = 1.0f + f * f * (-2.5f + 1.5f * f);
+  w[2] = f * (0.5f + f * (2.0f - 1.5f * f));
+  w[3] = f * f * (-0.5f + 0.5f * f);
+}
+
+__global__ void k_composite_halfres(const float4* __restrict__ l, const float4* __restrict__ t,
+                                    uint32_t rw, uint32_t rh, float4* __restrict__ hdr, uint32_t W,
+                                    uint32_t H) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  const float spx = ((float)x + 0.5f) / (float)W * (float)rw;
+  const float spy = ((float)y + 0.5f) / (float)H * (float)rh;
+  const float bx = floorf(spx - 0.5f), by = floorf(spy - 0.5f);
+  float wx[4], wy[4];
+  cr_weights(spx - (bx + 0.5f), wx);
+  cr_weights(spy - (by + 0.5f), wy);
+  int ix[4], iy[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    ix[k] = clampi((int)bx - 1 + k, (int)rw);
+    iy[k] = clampi((int)by - 1 + k, (int)rh);
+  }
+  float4 sl = f4(0.0f), st = f4(0.0f);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    float4 rl = f4(0.0f), rt = f4(0.0f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int idx = iy[j] * (int)rw + ix[k];
+      rl = fma4(__ldg(l + idx), wx[k], rl);
+      rt = fma4(__ldg(t + idx), wx[k], rt);
+    }
+    sl = fma4(rl, wy[j], sl);
+    st = fma4(rt, wy[j], st);
+  }
+  const float4 L = max4(sl, f4(0.0f)), T = clamp4(st, f4(0.0f), f4(1.0f));
+  const size_t o = (size_t)y * W + x;
+  const float4 d = hdr[o];
+  hdr[o] = make_float4(fmaf(d.x, T.x, L.x), fmaf(d.y, T.y, L.y), fmaf(d.z, T.z, L.z), fmaf(d.w, T.w, L.w));
+}
+
+dim3 grid16(uint32_t w, uint32_t h) { return dim3((w + 15u) / 16u, (h + 15u) / 16u); }
+
+}  // namespace
+
+int launch_depth_halfres(const float* depth, uint32_t W, uint32_t H, float* out, uint32_t rw,
+                         uint32_t rh, cudaStream_t s) {
+  k_depth_halfres<<<grid16(rw, rh), dim3(16, 16), 0, s>>>(depth, W, H, out, rw, rh);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
+
+int launch_taa_resolve(const TaaParams& p, cudaStream_t s) {
+  k_taa_resolve<<<grid16(p.w, p.h), dim3(16, 16), 0, s>>>(p);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
+
+int launch_composite_halfres(const float4* l, const float4* t, uint32_t rw, uint32_t rh, float4* hdr,
+                             uint32_t W, uint32_t H, cudaStream_t s) {
+  k_composite_halfres<<<grid16(W, H), dim3(16, 16), 0, s>>>(l, t, rw, rh, hdr, W, H);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
+
+}  // namespace psc

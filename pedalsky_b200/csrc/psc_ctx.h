@@ -35,6 +35,7 @@ struct psc_ctx {
 
   float* d_weather = nullptr;
   uint32_t weather_w = 0, weather_h = 0;
+  float4* d_weather_quad = nullptr;  // FAST schedule: 2x2 footprints (power-of-two maps <= 1024^2)
   uint8_t* d_type = nullptr;
   uint32_t type_w = 0, type_h = 0;
   std::vector<uint16_t> h_wind;    // 32x16x32 RGBA16F
@@ -63,6 +64,25 @@ struct psc_ctx {
   cudaArray_t arr_sky = nullptr;
 
   uint64_t launches = 0;
+
+  // cloud RT of the half-res / TAA forms of psc_render (grow-only scratch)
+  float4* d_rt_l = nullptr;
+  float4* d_rt_t = nullptr;
+  size_t rt_cap = 0;          // texels
+  float* d_rt_depth = nullptr;
+  size_t rt_depth_cap = 0;
+  // per-view TAA history (crates/ps-clouds/src/lib.rs:776-825): ping-pong
+  // resolved pairs at the cloud-RT size
+  struct TaaView {
+    float4* l[2] = {nullptr, nullptr};
+    float4* t[2] = {nullptr, nullptr};
+    uint32_t w = 0, h = 0;
+    uint32_t write_slot = 0;
+    bool valid = false;                 // history holds a previous resolve
+    uint64_t marches = 0;               // psc_render calls while this view was active
+    uint64_t resolved_at = UINT64_MAX;  // `marches` at the last resolve
+  } taa[PSC_MAX_CLOUD_VIEWS];
+  uint32_t active_view = 0;
 
   // batching (psc_render_batch)
   PscBatchTuning batch_tuning{128, 16, 0, 0};

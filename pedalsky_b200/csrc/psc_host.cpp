@@ -311,6 +311,22 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
     o.alpha = std::exp(3.62489f - 8.29288f / (d + 5.52825f));
     o.w_d = std::exp(-0.599085f / (d - 0.641583f) - 0.665888f);
     o.ice = smoothstep_h(35.0f, 50.0f, d);
+    // the FAST schedule's ndf coefficients (march_fast_body.cuh:ndf_coef,
+    // cloud_density_common.wgsl:49-91): smoothstep(0, a) times a rising or
+    // falling second smoothstep, for every type but Cumulonimbus
+    static const float kA[7] = {0.07f, 0.10f, 0.15f, 0.20f, 0.30f, 0.40f, 0.50f};
+    static const float kE1[7] = {1.0f, 0.6f, 1.0f, 1.0f, 0.7f, 0.6f, 0.8f};
+    static const float kW1[7] = {-0.8f, 0.4f, -0.6f, -0.7f, 0.3f, 0.4f, 0.2f};
+    static const uint32_t kMode[7] = {1, 2, 1, 1, 2, 2, 2};
+    if (L.cloud_type < 7) {
+      o.ndf_inv_a = 1.0f / kA[L.cloud_type];
+      o.ndf_e1 = kE1[L.cloud_type];
+      o.ndf_inv_w1 = 1.0f / kW1[L.cloud_type];
+      o.ndf_mode = kMode[L.cloud_type];
+    } else {
+      o.ndf_inv_a = o.ndf_e1 = o.ndf_inv_w1 = 0.0f;
+      o.ndf_mode = 0;
+    }
     o.r_bottom = (double)w.planet_radius_m + (double)L.base_m;
     o.r_top = (double)w.planet_radius_m + (double)L.top_m;
   }
@@ -321,6 +337,7 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
   u.curl = c->d_curl;
   u.blue = c->d_blue;
   u.weather = c->d_weather;
+  u.weather_quad = c->d_weather_quad;
   u.weather_w = c->weather_w;
   u.weather_h = c->weather_h;
   u.type_grid = c->d_type;
@@ -648,6 +665,135 @@ int upload_lut_float4(psc_ctx* c, int kind, const uint16_t* h16) {
   return PSC_OK;
 }
 
+// Grow-only device scratch of `n` elements of T.
+template <class T>
+int grow(T** p, size_t* cap, size_t n, const char* what) {
+  if (*cap >= n && *p) return PSC_OK;
+  dfree(*p);
+  *cap = 0;
+  PSC_CUDA(cudaMalloc(p, n * sizeof(T)), what);
+  *cap = n;
+  return PSC_OK;
+}
+
+void half_res_dims(uint32_t w, uint32_t h, uint32_t* rw, uint32_t* rh) {
+  *rw = std::max(1u, (uint32_t)((float)w * 0.5f));  // lib.rs:751-758
+  *rh = std::max(1u, (uint32_t)((float)h * 0.5f));
+}
+
+void free_taa_view(psc_ctx::TaaView& tv) {
+  for (int k = 0; k < 2; ++k) {
+    dfree(tv.l[k]);
+    dfree(tv.t[k]);
+  }
+  tv.w = tv.h = 0;
+  tv.valid = false;
+}
+
+// One TAA frame of the active view (lib.rs:776-825 bookkeeping, then the
+// resolve pass): on the first active frame (the view's previous march was
+// not resolved), after a resize or an invalidation the history is not valid
+// and the resolve is the current sample; otherwise the write slot flips and
+// the current sample weighs 1/8.  *res_l / *res_t point at the resolved pair
+// (the new history slot).
+int taa_step(psc_ctx* c, const float4* cur_l, const float4* cur_t, uint32_t w, uint32_t h,
+             cudaStream_t s, const float4** res_l, const float4** res_t) {
+  psc_ctx::TaaView& tv = c->taa[c->active_view];
+  const bool just_enabled = tv.marches == 0 || tv.resolved_at != tv.marches - 1;
+  tv.resolved_at = tv.marches;
+  if (tv.w != w || tv.h != h || !tv.l[0]) {
+    free_taa_view(tv);
+    for (int k = 0; k < 2; ++k) {
+      PSC_CUDA(cudaMalloc(&tv.l[k], (size_t)w * h * sizeof(float4)), "cudaMalloc TAA history");
+      PSC_CUDA(cudaMalloc(&tv.t[k], (size_t)w * h * sizeof(float4)), "cudaMalloc TAA history");
+    }
+    tv.w = w;
+    tv.h = h;
+    tv.valid = false;
+  }
+  if (just_enabled) tv.valid = false;
+  tv.write_slot = tv.valid ? (tv.write_slot ^ 1u) : 0u;
+  const uint32_t ws = tv.write_slot;
+  psc::TaaParams p{};
+  for (int col = 0; col < 4; ++col)
+    for (int row = 0; row < 4; ++row) {
+      p.inv_vp[col][row] = c->frame.inv_view_proj[col][row];
+      p.prev_vp[col][row] = c->frame.prev_view_proj[col][row];
+    }
+  for (int k = 0; k < 3; ++k) p.cam[k] = c->frame.camera_position_world[k];
+  p.blend_weight = tv.valid ? 1.0f / 8.0f : 1.0f;  // TAA_BLEND_WEIGHT, lib.rs:42
+  p.history_valid = tv.valid ? 1.0f : 0.0f;
+  p.w = w;
+  p.h = h;
+  p.cur_l = cur_l;
+  p.cur_t = cur_t;
+  p.hist_l = tv.l[ws ^ 1u];
+  p.hist_t = tv.t[ws ^ 1u];
+  p.out_l = tv.l[ws];
+  p.out_t = tv.t[ws];
+  if (psc::launch_taa_resolve(p, s)) return fail(PSC_ERR_CUDA, "TAA launch failed");
+  ++c->launches;
+  tv.valid = true;
+  *res_l = tv.l[ws];
+  *res_t = tv.t[ws];
+  return PSC_OK;
+}
+
+// The half-res / TAA form of psc_render for one whole-viewport view: march
+// into the cloud RT, resolve, copy out, composite.
+int render_rt_view(psc_ctx* c, const PscView& v, cudaStream_t s) {
+  const uint32_t W = v.width, H = v.height;
+  uint32_t rw = W, rh = H;
+  if (c->opts.half_res) half_res_dims(W, H, &rw, &rh);
+  const size_t n_rt = (size_t)rw * rh;
+  if (c->rt_cap < n_rt || !c->d_rt_l || !c->d_rt_t) {  // L and T grow together
+    dfree(c->d_rt_l);
+    dfree(c->d_rt_t);
+    c->rt_cap = 0;
+    PSC_CUDA(cudaMalloc(&c->d_rt_l, n_rt * sizeof(float4)), "cudaMalloc cloud RT");
+    PSC_CUDA(cudaMalloc(&c->d_rt_t, n_rt * sizeof(float4)), "cudaMalloc cloud RT");
+    c->rt_cap = n_rt;
+  }
+  int rc = PSC_OK;
+  const float* depth = v.depth;
+  if (c->opts.half_res && v.depth) {
+    rc = grow(&c->d_rt_depth, &c->rt_depth_cap, n_rt, "cudaMalloc cloud-RT depth");
+    if (rc) return rc;
+    if (psc::launch_depth_halfres(v.depth, W, H, c->d_rt_depth, rw, rh, s))
+      return fail(PSC_ERR_CUDA, "half-res depth launch failed");
+    ++c->launches;
+    depth = c->d_rt_depth;
+  }
+  psc::MarchUniforms u;
+  build_uniforms(c, rw, rh, u);
+  u.composite = 0;
+  psc::ViewDev vd{rw, rh, 0, 0, depth, c->d_rt_l, c->d_rt_t, nullptr};
+  rc = PSC_ERR_UNSUPPORTED;
+  if (c->opts.schedule == PSC_SCHED_FAST) rc = psc::launch_march_fast(u, vd, c->opts, s);
+  if (rc == PSC_ERR_UNSUPPORTED) rc = psc::launch_march(u, vd, c->opts, s);
+  if (rc) return fail(rc, "march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  ++c->launches;
+  const float4 *src_l = c->d_rt_l, *src_t = c->d_rt_t;
+  if (c->opts.taa) {
+    rc = taa_step(c, c->d_rt_l, c->d_rt_t, rw, rh, s, &src_l, &src_t);
+    if (rc) return rc;
+  }
+  if (v.out_luminance)
+    PSC_CUDA(cudaMemcpyAsync(v.out_luminance, src_l, n_rt * sizeof(float4), cudaMemcpyDeviceToDevice, s),
+             "cloud RT copy");
+  if (v.out_transmittance)
+    PSC_CUDA(cudaMemcpyAsync(v.out_transmittance, src_t, n_rt * sizeof(float4), cudaMemcpyDeviceToDevice, s),
+             "cloud RT copy");
+  if (c->opts.composite) {
+    const int e = c->opts.half_res
+                      ? psc::launch_composite_halfres(src_l, src_t, rw, rh, reinterpret_cast<float4*>(v.hdr), W, H, s)
+                      : psc::launch_composite(src_l, src_t, reinterpret_cast<float4*>(v.hdr), W * H, s);
+    if (e) return fail(PSC_ERR_CUDA, "composite launch failed");
+    ++c->launches;
+  }
+  return PSC_OK;
+}
+
 }  // namespace
 
 namespace psc {
@@ -661,6 +807,8 @@ int validate_batch(psc_ctx* c, const PscBatchView* views, uint32_t n) {
     return fail(PSC_ERR_MISSING_INPUT, "transmittance/multi-scatter LUTs missing (psc_bake_luts or psc_upload_lut)");
   if (c->opts.schedule != PSC_SCHED_FAST)
     return fail(PSC_ERR_UNSUPPORTED, "the batched kernel implements the FAST schedule (options.schedule)");
+  if (c->opts.half_res || c->opts.taa)
+    return fail(PSC_ERR_UNSUPPORTED, "the batched kernel renders full-resolution views without TAA");
   for (uint32_t i = 0; i < n; ++i) {
     const PscBatchView& v = views[i];
     if (!v.width || !v.height || v.width > 32768 || v.height > 32768)
@@ -1118,8 +1266,13 @@ int psc_destroy(psc_ctx* c) {
   dfree(c->d_detail_quad);
   dfree(c->d_curl_quad);
   dfree(c->d_curl);
+  dfree(c->d_rt_l);
+  dfree(c->d_rt_t);
+  dfree(c->d_rt_depth);
+  for (auto& tv : c->taa) free_taa_view(tv);
   dfree(c->d_blue);
   dfree(c->d_weather);
+  dfree(c->d_weather_quad);
   dfree(c->d_type);
   for (int k = 0; k < 4; ++k) {
     if (c->tex_lut[k]) cudaDestroyTextureObject(c->tex_lut[k]);
@@ -1196,6 +1349,7 @@ int psc_set_options(psc_ctx* c, const PscMarchOptions* o) {
     return fail(PSC_ERR_UNSUPPORTED, "texture filtering reads RGBA8 or RGBA16F volumes only");
   if (o->filter == PSC_FILTER_TEXTURE && o->storage == PSC_STORAGE_F16 && o->schedule != PSC_SCHED_FAST)
     return fail(PSC_ERR_UNSUPPORTED, "F16 texture volumes are read by the FAST schedule only");
+  if (o->half_res > 1 || o->taa > 1) return fail(PSC_ERR_INVALID_ARGUMENT, "half_res and taa are 0 or 1");
   const float hv[] = {o->hg_g_forward, o->hg_g_backward, o->hg_blend};
   if (!all_finite(hv, 3)) return fail(PSC_ERR_NOT_FINITE, "non-finite HG lobe");
   if (o->storage != c->opts.storage || o->filter != c->opts.filter) c->tex_dirty = true;
@@ -1286,6 +1440,23 @@ int psc_upload_weather(psc_ctx* c, const void* texels, uint32_t w, uint32_t h, i
   if (c->d_weather && (c->weather_w != w || c->weather_h != h)) dfree(c->d_weather);
   if (!c->d_weather) PSC_CUDA(cudaMalloc(&c->d_weather, r.size() * 4), "cudaMalloc weather");
   PSC_CUDA(cudaMemcpy(c->d_weather, r.data(), r.size() * 4, cudaMemcpyHostToDevice), "weather upload");
+  dfree(c->d_weather_quad);
+  const bool pow2 = (w & (w - 1)) == 0 && (h & (h - 1)) == 0;
+  if (pow2 && (size_t)w * h <= 1024u * 1024u) {
+    // 2x2 bilinear footprints, repeat-wrapped: one 16-byte load per tap
+    std::vector<float> q(r.size() * 4);
+    for (uint32_t y = 0; y < h; ++y)
+      for (uint32_t x = 0; x < w; ++x) {
+        const uint32_t x1 = (x + 1) & (w - 1), y1 = (y + 1) & (h - 1);
+        float* e = &q[((size_t)y * w + x) * 4];
+        e[0] = r[(size_t)y * w + x];
+        e[1] = r[(size_t)y * w + x1];
+        e[2] = r[(size_t)y1 * w + x];
+        e[3] = r[(size_t)y1 * w + x1];
+      }
+    PSC_CUDA(cudaMalloc(&c->d_weather_quad, q.size() * 4), "cudaMalloc weather quads");
+    PSC_CUDA(cudaMemcpy(c->d_weather_quad, q.data(), q.size() * 4, cudaMemcpyHostToDevice), "weather quads");
+  }
   c->weather_w = w;
   c->weather_h = h;
   return PSC_OK;
@@ -1364,6 +1535,10 @@ int psc_download_lut(psc_ctx* c, int kind, uint16_t* out, size_t count) {
 
 int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
   if (!c || (n && !views)) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  const bool rt_form = c->opts.half_res || c->opts.taa;
+  if (rt_form && n != 1)
+    return fail(PSC_ERR_INVALID_ARGUMENT,
+                "the half-res / TAA forms render one view per call (its march, TAA and composite)");
   if (!c->have_frame) return fail(PSC_ERR_MISSING_INPUT, "psc_set_frame was not called");
   if (!c->have_base || !c->have_detail || !c->have_curl || !c->have_blue)
     return fail(PSC_ERR_MISSING_INPUT, "noise volumes missing (psc_bake_noise or psc_upload_noise)");
@@ -1392,8 +1567,12 @@ int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
     if (!v.out_luminance && !v.out_transmittance && !(c->opts.composite && v.hdr))
       return fail(PSC_ERR_INVALID_ARGUMENT, "view %u has no output buffer", i);
     if (c->opts.composite && !v.hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: composite needs hdr", i);
+    if (rt_form && (v.x_offset || v.y_offset || vw != v.width || vh != v.height))
+      return fail(PSC_ERR_INVALID_ARGUMENT, "the half-res / TAA forms render whole viewports");
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ++c->taa[c->active_view].marches;  // a resolve of this march keeps the view's history going
+  if (rt_form) return render_rt_view(c, views[0], s);
   psc::MarchUniforms u;
   for (uint32_t i = 0; i < n; ++i) {
     const PscView& v = views[i];
@@ -1417,6 +1596,60 @@ int psc_composite(const float* l, const float* t, float* hdr, uint32_t w, uint32
   if (psc::launch_composite(reinterpret_cast<const float4*>(l), reinterpret_cast<const float4*>(t),
                             reinterpret_cast<float4*>(hdr), w * h, static_cast<cudaStream_t>(stream)))
     return fail(PSC_ERR_CUDA, "composite launch failed");
+  return PSC_OK;
+}
+
+int psc_cloud_rt_size(uint32_t w, uint32_t h, uint32_t half_res, uint32_t* rw, uint32_t* rh) {
+  if (!rw || !rh) return fail(PSC_ERR_INVALID_ARGUMENT, "null output");
+  if (!w || !h) return fail(PSC_ERR_INVALID_ARGUMENT, "zero-size target");
+  if (half_res) {
+    half_res_dims(w, h, rw, rh);
+  } else {
+    *rw = w;
+    *rh = h;
+  }
+  return PSC_OK;
+}
+
+int psc_taa_resolve(psc_ctx* c, const float* cur_l, const float* cur_t, uint32_t w, uint32_t h, float* out_l,
+                    float* out_t, void* stream) {
+  if (!c || !cur_l || !cur_t) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (!w || !h || w > 32768 || h > 32768) return fail(PSC_ERR_INVALID_ARGUMENT, "cloud RT %ux%u out of range", w, h);
+  if (!c->have_frame) return fail(PSC_ERR_MISSING_INPUT, "psc_set_frame was not called");
+  int rc = ensure_device(c);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float4 *res_l = nullptr, *res_t = nullptr;
+  rc = taa_step(c, reinterpret_cast<const float4*>(cur_l), reinterpret_cast<const float4*>(cur_t), w, h, s,
+                &res_l, &res_t);
+  if (rc) return rc;
+  const size_t bytes = (size_t)w * h * sizeof(float4);
+  if (out_l) PSC_CUDA(cudaMemcpyAsync(out_l, res_l, bytes, cudaMemcpyDeviceToDevice, s), "TAA output copy");
+  if (out_t) PSC_CUDA(cudaMemcpyAsync(out_t, res_t, bytes, cudaMemcpyDeviceToDevice, s), "TAA output copy");
+  return PSC_OK;
+}
+
+int psc_set_active_view(psc_ctx* c, uint32_t view) {  // lib.rs:722
+  if (!c) return fail(PSC_ERR_INVALID_ARGUMENT, "null context");
+  c->active_view = std::min(view, PSC_MAX_CLOUD_VIEWS - 1u);
+  return PSC_OK;
+}
+
+int psc_invalidate_taa_history(psc_ctx* c) {  // lib.rs:729
+  if (!c) return fail(PSC_ERR_INVALID_ARGUMENT, "null context");
+  for (auto& tv : c->taa) tv.valid = false;
+  return PSC_OK;
+}
+
+int psc_composite_halfres(const float* l, const float* t, uint32_t rw, uint32_t rh, float* hdr, uint32_t w,
+                          uint32_t h, void* stream) {
+  if (!l || !t || !hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "null buffer");
+  if (!w || !h || !rw || !rh) return fail(PSC_ERR_INVALID_ARGUMENT, "zero-size composite");
+  if (w > 32768 || h > 32768 || rw > 32768 || rh > 32768)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "composite size out of range");
+  if (psc::launch_composite_halfres(reinterpret_cast<const float4*>(l), reinterpret_cast<const float4*>(t), rw, rh,
+                                    reinterpret_cast<float4*>(hdr), w, h, static_cast<cudaStream_t>(stream)))
+    return fail(PSC_ERR_CUDA, "half-res composite launch failed");
   return PSC_OK;
 }
 
@@ -1445,6 +1678,8 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
     return fail(PSC_ERR_MISSING_INPUT, "transmittance/multi-scatter LUTs missing (psc_bake_luts or psc_upload_lut)");
   if (c->opts.schedule != PSC_SCHED_FAST)
     return fail(PSC_ERR_UNSUPPORTED, "the batched kernel implements the FAST schedule (options.schedule)");
+  if (c->opts.half_res || c->opts.taa)
+    return fail(PSC_ERR_UNSUPPORTED, "the batched kernel renders full-resolution views without TAA");
   for (uint32_t i = 0; i < n; ++i) {
     const PscBatchView& v = views[i];
     if (!v.width || !v.height || v.width > 32768 || v.height > 32768)

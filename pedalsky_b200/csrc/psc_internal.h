@@ -40,7 +40,11 @@ struct LayerConst {
   // Approx-Mie constants (cloud_phase_constants); exact for every layer
   // type except Cumulonimbus, whose diameter depends on height.
   float g_hg, g_d, alpha, w_d, ice;
-  float _pad;
+  // ndf of types 0..6 as ssr(0, ndf_inv_a, h) * g, g = ssr(ndf_e1,
+  // ndf_inv_w1, h) or 1 - g (ndf_mode 1 / 2); ndf_mode 0: evaluate by type
+  float ndf_inv_a, ndf_e1, ndf_inv_w1;
+  uint32_t ndf_mode;
+  float _pad[2];
   double r_bottom, r_top;  // planet_radius + base/top, FP64
 };
 
@@ -99,6 +103,7 @@ struct alignas(16) MarchUniforms {
   const float* blue;           // 64^2, already v/255
   const float* weather;        // R channel as float, weather_w x weather_h
   uint32_t weather_w, weather_h;
+  const float4* weather_quad;  // power-of-two maps up to 1024^2: 2x2 footprints, else null
   const uint8_t* type_grid;    // may be null (all sentinel)
   uint32_t type_w, type_h;
   const float4* lut_trans;     // 256x64
@@ -144,6 +149,27 @@ struct GridDev {
 };
 int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g, bool adjoint,
                       cudaStream_t stream);
+
+// TAA resolve of one cloud RT (post.cu, shaders/clouds/cloud_taa.wgsl).
+struct TaaParams {
+  float inv_vp[4][4];      // current inv_view_proj, [col][row]
+  float prev_vp[4][4];     // previous frame's view_proj, [col][row]
+  float cam[3];
+  float blend_weight;      // weight of the current sample (1/8, 1 on bootstrap)
+  float history_valid;     // 0: output = current sample
+  uint32_t w, h;
+  const float4* cur_l;
+  const float4* cur_t;
+  const float4* hist_l;
+  const float4* hist_t;
+  float4* out_l;
+  float4* out_t;
+};
+int launch_taa_resolve(const TaaParams& p, cudaStream_t stream);
+int launch_depth_halfres(const float* depth, uint32_t W, uint32_t H, float* out, uint32_t rw,
+                         uint32_t rh, cudaStream_t stream);
+int launch_composite_halfres(const float4* l, const float4* t, uint32_t rw, uint32_t rh, float4* hdr,
+                             uint32_t W, uint32_t H, cudaStream_t stream);
 
 // Launchers (march.cu).
 int launch_march(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,

@@ -106,6 +106,7 @@ class CloudsSubsystem:
         self._cloud_rt = None
         self.active_view = 0
         self.options = options or self._default_options()
+        self.options.half_res, self.options.taa = self._rt_flags(self._tuning)
         call("psc_set_options", self._ctx, C.byref(self.options))
         if bake_noise:
             call("psc_bake_noise", self._ctx)   # CloudNoise::bake (noise.rs:71)
@@ -164,7 +165,10 @@ class CloudsSubsystem:
         if pass_id == PASS_MARCH:
             self._dispatch_march(ctx)
         elif pass_id == PASS_TAA:
-            return  # TAA off unless enabled (lib.rs:1000-1050); history path not built here
+            # With TAA active the march call already resolved the cloud RT
+            # against the active view's history (psc_render's TAA form), so
+            # this pass has nothing left to do (lib.rs:1000-1050).
+            return
         elif pass_id == PASS_COMPOSITE:
             self._dispatch_composite(ctx)
         else:
@@ -174,6 +178,11 @@ class CloudsSubsystem:
         self._tuning = tuning
         self._apply_tuning(tuning)
         self._push_params()
+        half, taa = self._rt_flags(tuning)
+        if (self.options.half_res, self.options.taa) != (half, taa):
+            o = capi.MarchOptions.from_buffer_copy(self.options)
+            o.half_res, o.taa = half, taa
+            self.set_options(o)
 
     # -- CloudsSubsystem API -----------------------------------------------
     def noise(self, kind: int) -> np.ndarray:
@@ -206,9 +215,10 @@ class CloudsSubsystem:
 
     def set_active_view(self, view: int) -> None:  # lib.rs:722
         self.active_view = min(int(view), MAX_CLOUD_VIEWS - 1)
+        call("psc_set_active_view", self._ctx, self.active_view)
 
     def invalidate_taa_history(self) -> None:  # lib.rs:729
-        return None
+        call("psc_invalidate_taa_history", self._ctx)
 
     def set_options(self, options: capi.MarchOptions) -> None:
         call("psc_set_options", self._ctx, C.byref(options))
@@ -244,13 +254,25 @@ class CloudsSubsystem:
     def _push_params(self) -> None:
         call("psc_set_params", self._ctx, C.byref(self._params))
 
+    @staticmethod
+    def _rt_flags(t: CloudsTuning) -> tuple[int, int]:
+        """(half_res, taa) options: TAA is active when enabled and time is not
+        frozen (lib.rs:776)."""
+        return int(t.half_res_render), int(t.temporal_taa and not t.freeze_time)
+
     def _dispatch_march(self, ctx: RenderContext) -> None:
+        """March into the cloud RT (half size with half_res_render, lib.rs:
+        746-758); with TAA the same call resolves it against the active
+        view's history."""
         import torch
         h, w = int(ctx.color.shape[0]), int(ctx.color.shape[1])
-        if self._cloud_rt is None or self._cloud_rt[0].shape[:2] != (h, w):
+        rw, rh = C.c_uint32(), C.c_uint32()
+        call("psc_cloud_rt_size", w, h, self.options.half_res, C.byref(rw), C.byref(rh))
+        rw, rh = rw.value, rh.value
+        if self._cloud_rt is None or self._cloud_rt[0].shape[:2] != (rh, rw):
             dev = ctx.color.device
-            self._cloud_rt = (torch.zeros((h, w, 4), dtype=torch.float32, device=dev),
-                              torch.ones((h, w, 4), dtype=torch.float32, device=dev))
+            self._cloud_rt = (torch.zeros((rh, rw, 4), dtype=torch.float32, device=dev),
+                              torch.ones((rh, rw, 4), dtype=torch.float32, device=dev))
         lum, tr = self._cloud_rt
         view = capi.View(w, h, ptr(ctx.depth).value, lum.data_ptr(), tr.data_ptr(), None)
         call("psc_render", self._ctx, C.byref(view), 1, _stream_handle(ctx.stream))
@@ -260,7 +282,12 @@ class CloudsSubsystem:
             return
         lum, tr = self._cloud_rt
         h, w = int(ctx.color.shape[0]), int(ctx.color.shape[1])
-        call("psc_composite", ptr(lum), ptr(tr), ptr(ctx.color), w, h, _stream_handle(ctx.stream))
+        rh, rw = int(lum.shape[0]), int(lum.shape[1])
+        if (rh, rw) != (h, w):  # half-res RT: Catmull-Rom upsample (lib.rs:1054-1097)
+            call("psc_composite_halfres", ptr(lum), ptr(tr), rw, rh, ptr(ctx.color), w, h,
+                 _stream_handle(ctx.stream))
+        else:
+            call("psc_composite", ptr(lum), ptr(tr), ptr(ctx.color), w, h, _stream_handle(ctx.stream))
 
     @property
     def cloud_rt(self):
