@@ -40,6 +40,9 @@ FRAME_WORKLOADS = {
     "precision_1080p": ((1920, 1080), 1, {"layers": "Cu 1500-2300 cov 0.5; As 4000-5000 cov 0.7; "
                                                     "Ci 8000-9000 cov 0.3", "primary_steps": 128,
                                           "light_steps": 6}),
+    "plain_320x180": ((320, 180), 1, {"layers": "Cu 1500-2300 cov 0.5", "primary_steps": 64,
+                                      "light_steps": 6, "phase": "dual-lobe HG 0.8/-0.2 w 0.5",
+                                      "octaves": 3}),
     "stress_2160p": ((3840, 2160), 8, {"layers": "Cb 600-12000 cov 0.8 x 2048^2 f32 coverage grid",
                                        "primary_steps": 256, "light_steps": 8,
                                        "frames": "8, simulated_seconds 0..7, 15 m/s wind"}),
@@ -51,6 +54,8 @@ def frame_scenes(workload, W, H, **kw):
     from pedalsky_b200 import scenes
     if workload == "stress_2160p":
         return [scenes.stress_2160p(W, H, frame_index=k, **kw) for k in range(8)]
+    if workload == "plain_320x180":
+        return [scenes.plain_320x180(W, H, **kw)]
     return [scenes.precision_1080p(W, H, **kw)]
 
 
@@ -69,7 +74,8 @@ def parse():
     ap.add_argument("--height", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="precision_1080p",
-                    choices=["precision_1080p", "stress_2160p", "batch_64", "grid_512"],
+                    choices=["precision_1080p", "plain_320x180", "stress_2160p", "batch_64",
+                             "grid_512"],
                     help="stress_2160p: eight 4K frames of a Cumulonimbus over a 2048^2 coverage "
                          "grid; batch_64: the 64-view uneven batch in one persistent kernel")
     ap.add_argument("--batch-views", type=int, default=64)
@@ -170,7 +176,7 @@ def bytes_per_ray(storage: str, schedule: str = "fast", workload: str = WORKLOAD
 
 # DRAM bytes (read + write) per launch of the timed kernel, from one ncu
 # capture of the benchmark command (profiles/k_march_fast_f16_hybrid_1080p.md).
-DRAM_TRAFFIC_PER_LAUNCH = {("precision_1080p", "fast", "f16", "hybrid", 1920, 1080): 112875520}
+DRAM_TRAFFIC_PER_LAUNCH = {("precision_1080p", "fast", "f16", "hybrid", 1920, 1080): 176828416}
 
 
 def fetch_peaks(device: int) -> dict:
