@@ -381,6 +381,39 @@ def run_ours(args):
         plain = {"value": world * rays_step / (ms_plain * 1e-3) / 1e6, "ms_per_step": ms_plain,
                  "config": "plain schedule, f32 storage, exact filtering"}
 
+    # the same frames through the persistent batched kernel (psc_render_batch,
+    # one launch per step replayed from a CUDA graph, per-view LUT bakes
+    # included), the form the north-star ratio is stated for
+    batched = None
+    if not args.no_plain_reference and schedule == capi.SCHED_FAST:
+        from pedalsky_b200 import batch as B
+        bt = B.Batch(frames, dev)
+        B.set_tuning(sub.handle, 128, 16, use_graph=1)
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                bt.reset_hdr()
+                bt.render(sub.handle, stream)
+        torch.cuda.synchronize()
+        bevs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(args.steps)]
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.zero_()
+                bt.reset_hdr()
+                bevs[i][0].record(stream)
+                bt.render(sub.handle, stream)
+                bevs[i][1].record(stream)
+        torch.cuda.synchronize()
+        ms_b = float(np.mean([a.elapsed_time(b) for a, b in bevs]))
+        if world > 1:
+            tb = torch.tensor([ms_b], dtype=torch.float64, device=dev)
+            dist.all_reduce(tb, op=dist.ReduceOp.MAX)
+            ms_b = float(tb.item())
+        batched = {"value": world * rays_step / (ms_b * 1e-3) / 1e6, "ms_per_step": ms_b,
+                   "config": "psc_render_batch: persistent kernel from a captured CUDA graph, "
+                             "per-view LUT bakes included"}
+        del bt
+
     # end to end through the C ABI with host buffers: pinned H2D of the
     # depth and background, march + composite, D2H of the composited frame.
     h_bg = torch.from_numpy(s.background).pin_memory()
@@ -467,6 +500,9 @@ def run_ours(args):
             "roofline": roof,
             "plain_fp32_dropin": plain,
             "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
+            "batched_fp16": batched,
+            "batched_speedup_vs_plain_fp32": (batched["value"] / plain["value"])
+            if (batched and plain) else None,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "step_ms": [round(x, 4) for x in step_ms],

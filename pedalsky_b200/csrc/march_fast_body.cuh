@@ -27,8 +27,9 @@
 //     taps and issues their fetches before it combines any of them, so the
 //     fetches overlap instead of each waiting for the previous one;
 //   * in the primary step the weather, type and base-shape fetches are
-//     independent of each other and are issued together; the curl tile is
-//     read as 2x2 quads (one 16-byte load per tap);
+//     independent of each other and are issued together, with the curl
+//     fetch of the detail erosion (a 2x2 quad, one 16-byte load); a uniform
+//     weather map (the reference's synthesis writes R = 1) is not sampled;
 //   * in the filtered forms (HYBRID, TEXTURE) the transmittance and sky-view
 //     LUTs go through the texture unit, as the reference's linear sampler
 //     does; EXACT keeps FP32 weights for them.
@@ -139,15 +140,36 @@ __device__ __forceinline__ float detail_quad_tap(const uint2* q, float x, float 
   return lerpf(s.x, s.y, wz) * (1.0f / 2040.0f);
 }
 
-// Bilinear curl tap (128^2, repeat) from the quad form: one 16-byte load,
-// FP32 weights; returns (R, G) in [0, 1].
-__device__ __forceinline__ float2 curl_quad_tap(const uint4* q, float x, float y) {
+// Read-only 16-byte load that stays where it is written: the compiler may not
+// sink it into the branch that consumes it, so it is in flight while the
+// code before that branch runs.
+__device__ __forceinline__ uint4 ldg_v4_early(const uint4* p) {
+  uint4 r;
+  asm volatile("ld.global.nc.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p));
+  return r;
+}
+
+// Bilinear curl tap (128^2, repeat) from the quad form, in two halves: the
+// fetch (issued with the base-shape fetch, before it is known whether the
+// detail erosion needs it) and the FP32-weight blend; (R, G) in [0, 1].
+struct CurlFetch {
+  uint4 q;
+  float wx, wy;
+};
+__device__ __forceinline__ CurlFetch curl_fetch(const uint4* q, float x, float y) {
   const float fx = floorf(x), fy = floorf(y);
-  const int ix = (int)fx, iy = (int)fy;
-  const float wx = x - fx, wy = y - fy;
-  const uint4 c = __ldg(q + ((uint32_t)iy & 127u) * 128u + ((uint32_t)ix & 127u));
-  const float2 tx = make_float2(wx, wx);
-  const float2 v = lerp2(lerp2(h2f(c.x), h2f(c.y), tx), lerp2(h2f(c.z), h2f(c.w), tx), make_float2(wy, wy));
+  CurlFetch c;
+  c.q = ldg_v4_early(q + ((uint32_t)(int)fy & 127u) * 128u + ((uint32_t)(int)fx & 127u));
+  c.wx = x - fx;
+  c.wy = y - fy;
+  return c;
+}
+__device__ __forceinline__ float2 curl_blend(const CurlFetch& c) {
+  const float2 tx = make_float2(c.wx, c.wx);
+  const float2 v = lerp2(lerp2(h2f(c.q.x), h2f(c.q.y), tx), lerp2(h2f(c.q.z), h2f(c.q.w), tx),
+                         make_float2(c.wy, c.wy));
   return make_float2(v.x * (1.0f / 255.0f), v.y * (1.0f / 255.0f));
 }
 
@@ -509,10 +531,12 @@ __device__ __forceinline__ float3 sky_fast(const MarchUniforms& u, float alt, fl
   return make_float3(s.x * u.sun_illum[0], s.y * u.sun_illum[1], s.z * u.sun_illum[2]);
 }
 
-// Weather R channel, repeat + bilinear; power-of-two sizes wrap with a mask,
-// and up to 1024^2 read one 16-byte 2x2 footprint per tap.
+// Weather R channel, repeat + bilinear; a uniform map is its value, power-of-
+// two sizes wrap with a mask, and up to 1024^2 read one 16-byte 2x2
+// footprint per tap.
 __device__ __forceinline__ float weather_fast(const MarchUniforms& u, float uu, float vv) {
   const uint32_t W = u.weather_w, H = u.weather_h;
+  if (u.weather_uniform) return u.weather_value;  // bilinear of a constant is the constant
   if (u.weather_quad) {
     const float x = fmaf(uu, (float)W, -0.5f), y = fmaf(vv, (float)H, -0.5f);
     const float fx = floorf(x), fy = floorf(y);
@@ -631,6 +655,8 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
                                       fmaf(wsz, u.inv_weather_scale, 0.5f));
         const uint32_t type = effective_type(u, wsx, wsz, L.cloud_type);
         const float2 bs = base_tap<ST, FILT, false>(u, ax, py3, az);
+        const CurlFetch cf = curl_fetch(u.curl_quad, fmaf(ax, u.curl_texel_scale, -0.5f),
+                                        fmaf(az, u.curl_texel_scale, -0.5f));
         const float eff = clamp01(wr * L.coverage);
         const float nd = (!u.type_grid && L.ndf_mode)
                              ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_e1, L.ndf_inv_w1, L.ndf_mode == 2u}, h)
@@ -638,8 +664,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
         float cloud = shape_from(bs, L.lf_bias, nd, 1.0f - eff);
         if (eff >= 0.01f) {  // coverage gate (cloud_march.wgsl:450-451)
           if (cloud > 0.0f) {  // curl-perturbed detail erosion (:502-527)
-            const float2 c2 = curl_quad_tap(u.curl_quad, fmaf(ax, u.curl_texel_scale, -0.5f),
-                                            fmaf(az, u.curl_texel_scale, -0.5f));
+            const float2 c2 = curl_blend(cf);
             const float ddx = fmaf(fmaf(c2.x, 2.0f, -1.0f), u.curl_offset_scale, ax);
             const float ddz = fmaf(fmaf(c2.y, 2.0f, -1.0f), u.curl_offset_scale, az);
             const float hf = detail_tap<ST, FILT>(u, ddx, py3, ddz);

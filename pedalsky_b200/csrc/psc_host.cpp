@@ -338,6 +338,8 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
   u.blue = c->d_blue;
   u.weather = c->d_weather;
   u.weather_quad = c->d_weather_quad;
+  u.weather_uniform = c->weather_uniform ? 1u : 0u;
+  u.weather_value = c->weather_value;
   u.weather_w = c->weather_w;
   u.weather_h = c->weather_h;
   u.type_grid = c->d_type;
@@ -1441,6 +1443,11 @@ int psc_upload_weather(psc_ctx* c, const void* texels, uint32_t w, uint32_t h, i
   if (!c->d_weather) PSC_CUDA(cudaMalloc(&c->d_weather, r.size() * 4), "cudaMalloc weather");
   PSC_CUDA(cudaMemcpy(c->d_weather, r.data(), r.size() * 4, cudaMemcpyHostToDevice), "weather upload");
   dfree(c->d_weather_quad);
+  // a uniform map (the reference's synthesis writes R = 1 wherever layers
+  // exist): lerp(c, c, w) = fma(w, 0, c) = c exactly, so the FAST schedule
+  // skips the tap
+  c->weather_uniform = std::all_of(r.begin(), r.end(), [&](float v) { return v == r[0]; });
+  c->weather_value = r[0];
   const bool pow2 = (w & (w - 1)) == 0 && (h & (h - 1)) == 0;
   if (pow2 && (size_t)w * h <= 1024u * 1024u) {
     // 2x2 bilinear footprints, repeat-wrapped: one 16-byte load per tap

@@ -104,6 +104,8 @@ struct alignas(16) MarchUniforms {
   const float* weather;        // R channel as float, weather_w x weather_h
   uint32_t weather_w, weather_h;
   const float4* weather_quad;  // power-of-two maps up to 1024^2: 2x2 footprints, else null
+  uint32_t weather_uniform;    // every texel equal: bilinear sampling returns weather_value
+  float weather_value;
   const uint8_t* type_grid;    // may be null (all sentinel)
   uint32_t type_w, type_h;
   const float4* lut_trans;     // 256x64
