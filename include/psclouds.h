@@ -206,7 +206,13 @@ typedef struct PscMarchOptions {
   uint32_t schedule;        /* PSC_SCHED_*                                */
   uint32_t kahan;           /* 1: compensated optical-depth sums          */
   uint32_t composite;       /* 1: fuse `hdr = L + hdr*T` into the march   */
-  uint32_t debug_checks;    /* 1: bounds-check every texel index          */
+  uint32_t debug_checks;    /* 1: debug march — the PLAIN schedule (exact
+                               filtering unless U8 texture) with every
+                               texel, LUT, blue-noise, layer and pixel
+                               index compared with its buffer; a bad index
+                               is skipped and psc_render returns
+                               PSC_ERR_DEVICE_CHECK naming it (the call
+                               waits for the kernel); batches reject it  */
   uint32_t tile_w;          /* CTA tile width in pixels (0 = default)     */
   uint32_t tile_h;          /* CTA tile height in pixels (0 = default)    */
   uint32_t half_res;        /* 1: half-res march + Catmull-Rom composite

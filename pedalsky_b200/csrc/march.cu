@@ -43,7 +43,7 @@ __device__ __forceinline__ float max3f(float a, float b, float c) { return fmaxf
 template <int ST, int FILT, bool LIGHT>
 __device__ __forceinline__ float density_at(const MarchUniforms& u, const LayerConst& L, float px,
                                             float py, float pz, float alt, float wr,
-                                            uint32_t type) {
+                                            uint32_t type, int* chk) {
   const float h = (alt - L.base_m) / fmaxf(L.top_m - L.base_m, 1.0f);
   if (h < 0.0f || h > 1.0f) return 0.0f;
   const float eff = clamp01(wr * L.coverage);
@@ -52,19 +52,19 @@ __device__ __forceinline__ float density_at(const MarchUniforms& u, const LayerC
   const float ax = (px - L.wind_off_x) - L.skew_x * sk;
   const float ay = py;
   const float az = (pz - L.wind_off_z) - L.skew_z * sk;
-  const float4 b = Noise<ST, FILT>::base(u, ax / u.base_scale, ay / u.base_scale, az / u.base_scale);
+  const float4 b = Noise<ST, FILT>::base(u, ax / u.base_scale, ay / u.base_scale, az / u.base_scale, chk);
   const float lf = clamp01(((b.y * 0.625f + b.z * 0.25f) + b.w * 0.125f) + L.lf_bias);
   const float base_cloud = remapf(b.x, -(1.0f - lf), 1.0f, 0.0f, 1.0f);
   float cloud = base_cloud * ndf(h, type, L.anvil_bias);
   cloud = remapf(cloud, 1.0f - eff, 1.0f, 0.0f, 1.0f) * eff;
   if (!LIGHT && cloud > 0.0f) {
-    const float2 c2 = Noise<ST, FILT>::curl(u, ax / u.detail_scale, az / u.detail_scale);
+    const float2 c2 = Noise<ST, FILT>::curl(u, ax / u.detail_scale, az / u.detail_scale, chk);
     const float cx = c2.x * 2.0f - 1.0f, cz = c2.y * 2.0f - 1.0f;
     const float dx = ax + (cx * u.curl_strength) * u.detail_scale;
     const float dy = ay + (0.0f * u.curl_strength) * u.detail_scale;
     const float dz = az + (cz * u.curl_strength) * u.detail_scale;
     const float4 det = Noise<ST, FILT>::detail(u, dx / u.detail_scale, dy / u.detail_scale,
-                                               dz / u.detail_scale);
+                                               dz / u.detail_scale, chk);
     const float hf = (det.x * 0.625f + det.y * 0.25f) + det.z * 0.125f;
     const float dmod = mixf(hf, 1.0f - hf, clamp01(h * 10.0f));
     cloud = remapf(cloud, dmod * L.layer_detail, 1.0f, 0.0f, 1.0f);
@@ -83,7 +83,7 @@ __device__ __forceinline__ float altitude_from_entry(const MarchUniforms& u, flo
 
 template <int ST, int FILT>
 __device__ float march_to_light(const MarchUniforms& u, const LayerConst& L, float px, float py,
-                                float pz, float alt, float wr, uint32_t type) {
+                                float pz, float alt, float wr, uint32_t type, int* chk) {
   const float sx = u.sun[0], sy = u.sun[1], sz = u.sun[2];
   const float r0 = u.planet_r + alt;
   const float inv = 1.0f / fmaxf(r0, 1.0f);
@@ -107,14 +107,14 @@ __device__ float march_to_light(const MarchUniforms& u, const LayerConst& L, flo
       const float qy = fmaf(sy, t, py) + K[i][1] * sc;
       const float qz = fmaf(sz, t, pz) + K[i][2] * sc;
       const float a = altitude_from_entry(u, qx, qy, qz, r0, cv, alt, t);
-      od += density_at<ST, FILT, true>(u, L, qx, qy, qz, a, wr, type) * step;
+      od += density_at<ST, FILT, true>(u, L, qx, qy, qz, a, wr, type, chk) * step;
     }
     const float tf = dist * 3.0f;
     const float qx = fmaf(sx, tf, px) + K[5][0] * (step * 3.0f);
     const float qy = fmaf(sy, tf, py) + K[5][1] * (step * 3.0f);
     const float qz = fmaf(sz, tf, pz) + K[5][2] * (step * 3.0f);
     const float a = altitude_from_entry(u, qx, qy, qz, r0, cv, alt, tf);
-    od += density_at<ST, FILT, true>(u, L, qx, qy, qz, a, wr, type) * step * 3.0f;
+    od += density_at<ST, FILT, true>(u, L, qx, qy, qz, a, wr, type, chk) * step * 3.0f;
     return od;
   }
   const float step = dist / (float)u.light_steps;
@@ -122,7 +122,7 @@ __device__ float march_to_light(const MarchUniforms& u, const LayerConst& L, flo
     const float t = ((float)i + 0.5f) * step;
     const float qx = fmaf(sx, t, px), qy = fmaf(sy, t, py), qz = fmaf(sz, t, pz);
     const float a = altitude_from_entry(u, qx, qy, qz, r0, cv, alt, t);
-    const float term = density_at<ST, FILT, true>(u, L, qx, qy, qz, a, wr, type) * step;
+    const float term = density_at<ST, FILT, true>(u, L, qx, qy, qz, a, wr, type, chk) * step;
     if (u.kahan) {  // compensated sum
       const float y = term - comp;
       const float tt = od + y;
@@ -136,7 +136,7 @@ __device__ float march_to_light(const MarchUniforms& u, const LayerConst& L, flo
 }
 
 // cloud_march.wgsl:328-354
-__device__ float3 sun_transmittance_at(const MarchUniforms& u, float px, float py, float pz) {
+__device__ float3 sun_transmittance_at(const MarchUniforms& u, float px, float py, float pz, int* chk) {
   const float R = u.planet_r;
   const float ay = py + R;
   const float len = sqrtf((px * px + ay * ay) + pz * pz);
@@ -153,13 +153,14 @@ __device__ float3 sun_transmittance_at(const MarchUniforms& u, float px, float p
   const float d_min = ht - r, d_max = rho + bh;
   const float xm = clamp01((d - d_min) / fmaxf(d_max - d_min, 1.0f));
   const float xr = rho / fmaxf(bh, 1.0f);
-  const float4 t = lut2d(u.lut_trans, 256, 64, xm, xr);
+  const float4 t = lut2d(u.lut_trans, 256, 64, xm, xr, chk, kChkTrans);
   return make_float3(t.x, t.y, t.z);
 }
 
 // cloud_march.wgsl:672-700.  The zenith angle uses atan2(|xz|, y), the
 // well-conditioned form of acos(y) for directions near local up.
-__device__ float3 sky_ambient(const MarchUniforms& u, float px, float py, float pz, float sun_az) {
+__device__ float3 sky_ambient(const MarchUniforms& u, float px, float py, float pz, float sun_az,
+                              int* chk) {
   const float ay = py + u.planet_r;
   const float cam_r = sqrtf((px * px + ay * ay) + pz * pz);
   const float ux = px / cam_r, uy = ay / cam_r, uz = pz / cam_r;
@@ -176,16 +177,19 @@ __device__ float3 sky_ambient(const MarchUniforms& u, float px, float py, float 
   const float vaz = atan2f(ux, uz);
   float du = (vaz - sun_az) / (2.0f * kPi);
   du = du - floorf(du);
-  const float4 s = lut2d(u.lut_sky, 192, 108, du, vv);
+  const float4 s = lut2d(u.lut_sky, 192, 108, du, vv, chk, kChkSky);
   return make_float3(s.x * u.sun_illum[0], s.y * u.sun_illum[1], s.z * u.sun_illum[2]);
 }
 
-template <int ST, int FILT>
+// CK: options.debug_checks — every index is compared with its buffer's
+// extent (march_common.cuh:idx_ok); without it the checks compile away.
+template <int ST, int FILT, bool CK>
 __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant__ MarchUniforms u,
                                                           const __grid_constant__ ViewDev v) {
   uint32_t px, py;
   pixel_of(px, py);
   if (px >= v.width || py >= v.height) return;
+  int* const chk = CK ? u.error_word : nullptr;
 
   RaySetup rs;
   setup_ray(u, v, px, py, rs);
@@ -202,7 +206,7 @@ __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant_
     sx = (sx ^ ((ph * 11u + 7u) & 63u)) & 63u;
     sy = (sy ^ ((ph * 23u + 13u) & 63u)) & 63u;
   }
-  const float jitter = __ldg(u.blue + sy * 64u + sx);
+  const float jitter = idx_ok(chk, sy < 64u && sx < 64u, kChkBlue) ? __ldg(u.blue + sy * 64u + sx) : 0.0f;
 
   float Lr = 0.0f, Lg = 0.0f, Lb = 0.0f;
   float Tr = 1.0f, Tg = 1.0f, Tb = 1.0f;
@@ -214,6 +218,7 @@ __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant_
     if (max3f(Tr, Tg, Tb) < 0.01f) break;
     const uint32_t li = (rs.order >> (4u * k)) & 15u;
     if (!((rs.hit_mask >> li) & 1u)) continue;
+    if (!idx_ok(chk, li < 8u && li < u.layer_count, kChkLayer)) continue;
     float t0 = 0.0f, t1 = 0.0f;
 #pragma unroll
     for (int j = 0; j < 8; ++j)
@@ -233,12 +238,12 @@ __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant_
       const float alt = altitude_from_entry(u, px3, py3, pz3, rs.r0, rs.cos_view, rs.h0, t);
       const float wsx = px3 - L.wind_off_x, wsz = pz3 - L.wind_off_z;
       const float wr = Noise<ST, FILT>::weather(u, wsx / u.weather_scale + 0.5f,
-                                                wsz / u.weather_scale + 0.5f);
-      const uint32_t type = effective_type(u, wsx, wsz, L.cloud_type);
-      const float density = density_at<ST, FILT, false>(u, L, px3, py3, pz3, alt, wr, type);
+                                                wsz / u.weather_scale + 0.5f, chk);
+      const uint32_t type = effective_type(u, wsx, wsz, L.cloud_type, chk);
+      const float density = density_at<ST, FILT, false>(u, L, px3, py3, pz3, alt, wr, type, chk);
 
       if (density > 1e-3f) {
-        const float od = march_to_light<ST, FILT>(u, L, px3, py3, pz3, alt, wr, type);
+        const float od = march_to_light<ST, FILT>(u, L, px3, py3, pz3, alt, wr, type, chk);
         const float br = expf(-st_r * od), bg = expf(-st_g * od), bb = expf(-st_b * od);
         const float pr = 1.0f - expf(-2.0f * st_r * od), pg = 1.0f - expf(-2.0f * st_g * od),
                     pb = 1.0f - expf(-2.0f * st_b * od);
@@ -253,7 +258,7 @@ __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant_
         } else {
           pc = PhaseConst{L.g_hg, L.g_d, L.alpha, L.w_d, L.ice};
         }
-        const float3 st = sun_transmittance_at(u, px3, py3, pz3);
+        const float3 st = sun_transmittance_at(u, px3, py3, pz3, chk);
         float sr = 0.0f, sg = 0.0f, sb = 0.0f;
         float a = 1.0f, b = 1.0f, c = 1.0f;
         for (uint32_t o = 0; o < u.octaves; ++o) {
@@ -271,7 +276,7 @@ __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant_
           sg *= f;
           sb *= f;
         }
-        const float3 sky = sky_ambient(u, px3, py3, pz3, sun_az);
+        const float3 sky = sky_ambient(u, px3, py3, pz3, sun_az, chk);
         const float ag = mixf(0.3f, 1.0f, hn) * u.ambient;
         float lr = 0.0f, lg = 0.0f, lb = 0.0f;
         if (u.lightning_radius > 0.0f) {
@@ -328,12 +333,13 @@ __global__ void __launch_bounds__(kThreads) k_march_plain(const __grid_constant_
     const float ds = fmaxf(t_cloud, 50.0f);
     const float az = clamp01(logf(ds / 50.0f) / logf(100000.0f / 50.0f));
     const float4 ap = lut_ap(u.lut_ap, ((float)(px + v.x_off) + 0.5f) / u.vp_w,
-                             ((float)(py + v.y_off) + 0.5f) / u.vp_h, az);
+                             ((float)(py + v.y_off) + 0.5f) / u.vp_h, az, chk);
     Or = Lr * ap.w + ap.x * opacity;
     Og = Lg * ap.w + ap.y * opacity;
     Ob = Lb * ap.w + ap.z * opacity;
   }
   const size_t idx = (size_t)py * v.width + px;
+  if (!idx_ok(chk, px < v.width && py < v.height, kChkPixel)) return;
   const float4 lo = make_float4(Or, Og, Ob, 1.0f);
   const float4 to = make_float4(Tr, Tg, Tb, 1.0f);
   if (v.out_l) v.out_l[idx] = lo;
@@ -356,7 +362,10 @@ __global__ void k_composite(const float4* __restrict__ l, const float4* __restri
 template <int ST, int FILT>
 cudaError_t launch_plain(const MarchUniforms& u, const ViewDev& v, cudaStream_t s) {
   const dim3 grid((v.width + kTileW - 1) / kTileW, (v.height + kTileH - 1) / kTileH);
-  k_march_plain<ST, FILT><<<grid, kThreads, 0, s>>>(u, v);
+  if (u.debug_checks && u.error_word)
+    k_march_plain<ST, FILT, true><<<grid, kThreads, 0, s>>>(u, v);
+  else
+    k_march_plain<ST, FILT, false><<<grid, kThreads, 0, s>>>(u, v);
   return cudaGetLastError();
 }
 
@@ -365,7 +374,9 @@ cudaError_t launch_plain(const MarchUniforms& u, const ViewDev& v, cudaStream_t 
 int launch_march(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
                  cudaStream_t s) {
   cudaError_t e = cudaErrorInvalidValue;
-  if (o.filter == PSC_FILTER_HYBRID) return PSC_ERR_UNSUPPORTED;  // FAST schedule only
+  // the hybrid filter belongs to the FAST schedule; the checked debug form
+  // runs it with exact filtering
+  if (o.filter == PSC_FILTER_HYBRID && !(o.debug_checks && u.error_word)) return PSC_ERR_UNSUPPORTED;
   if (o.filter == PSC_FILTER_TEXTURE) {
     if (o.storage != PSC_STORAGE_U8) return PSC_ERR_UNSUPPORTED;
     e = launch_plain<PSC_STORAGE_U8, PSC_FILTER_TEXTURE>(u, v, s);

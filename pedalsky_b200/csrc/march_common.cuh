@@ -75,6 +75,23 @@ __device__ __forceinline__ int wrap_mod(int i, int n) {
 }
 __device__ __forceinline__ int clamp_idx(int i, int n) { return min(max(i, 0), n - 1); }
 
+// ---------------------------------------------------- debug index checks
+// options.debug_checks: every index the PLAIN kernel forms is compared with
+// its buffer's extent; a violation records its site code in the device
+// word (first one wins) and the access is skipped.  With chk == nullptr
+// (every other caller) the test folds away at compile time.
+enum CheckSite : int {
+  kChkBase = 1, kChkDetail = 2, kChkCurl = 3, kChkWeather = 4, kChkType = 5, kChkTrans = 6,
+  kChkSky = 7, kChkAerial = 8, kChkBlue = 9, kChkPixel = 10, kChkLayer = 11
+};
+__device__ __forceinline__ bool idx_ok(int* chk, bool ok, int site) {
+  if (chk != nullptr && !ok) {
+    atomicCAS(chk, 0, site);
+    return false;
+  }
+  return true;
+}
+
 // ---------------------------------------------------- texel decoding
 // Exact unorm8 -> float: the byte placed in the mantissa of 2^23.
 __device__ __forceinline__ float byte_to_float(uint32_t word, uint32_t sel) {
@@ -128,7 +145,8 @@ __device__ __forceinline__ float storage_scale(float volume_scale) {
 // Trilinear, repeat addressing, N a power of two; texel centre at u*N - 0.5.
 template <int ST, int N>
 __device__ __forceinline__ float4 trilinear_repeat(const void* vol, float u, float v, float w,
-                                                   float volume_scale) {
+                                                   float volume_scale, int* chk = nullptr,
+                                                   int site = 0) {
   const float x = u * (float)N - 0.5f, y = v * (float)N - 0.5f, z = w * (float)N - 0.5f;
   const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
   const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
@@ -136,6 +154,8 @@ __device__ __forceinline__ float4 trilinear_repeat(const void* vol, float u, flo
   const uint32_t x0 = (uint32_t)ix & (N - 1), x1 = (uint32_t)(ix + 1) & (N - 1);
   const uint32_t y0 = (uint32_t)iy & (N - 1), y1 = (uint32_t)(iy + 1) & (N - 1);
   const uint32_t z0 = (uint32_t)iz & (N - 1), z1 = (uint32_t)(iz + 1) & (N - 1);
+  if (!idx_ok(chk, x0 < N && x1 < N && y0 < N && y1 < N && z0 < N && z1 < N, site))
+    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const uint32_t r00 = (z0 * N + y0) * N, r10 = (z0 * N + y1) * N;
   const uint32_t r01 = (z1 * N + y0) * N, r11 = (z1 * N + y1) * N;
   const float4 c000 = load_texel<ST>(vol, r00 + x0), c100 = load_texel<ST>(vol, r00 + x1);
@@ -154,13 +174,16 @@ __device__ __forceinline__ float4 trilinear_repeat(const void* vol, float u, flo
 }
 
 // Curl: 128^2 RG8, repeat, bilinear.
-__device__ __forceinline__ float2 curl_sample(const uint8_t* curl, float u, float v) {
+__device__ __forceinline__ float2 curl_sample(const uint8_t* curl, float u, float v,
+                                              int* chk = nullptr) {
   const float x = u * 128.0f - 0.5f, y = v * 128.0f - 0.5f;
   const float fx = floorf(x), fy = floorf(y);
   const int ix = (int)fx, iy = (int)fy;
   const float wx = x - fx, wy = y - fy;
   const uint32_t x0 = (uint32_t)ix & 127u, x1 = (uint32_t)(ix + 1) & 127u;
   const uint32_t y0 = (uint32_t)iy & 127u, y1 = (uint32_t)(iy + 1) & 127u;
+  if (!idx_ok(chk, x0 < 128u && x1 < 128u && y0 < 128u && y1 < 128u, kChkCurl))
+    return make_float2(0.5f, 0.5f);
   const uint16_t* c = reinterpret_cast<const uint16_t*>(curl);
   const uint32_t t00 = __ldg(c + y0 * 128 + x0), t10 = __ldg(c + y0 * 128 + x1);
   const uint32_t t01 = __ldg(c + y1 * 128 + x0), t11 = __ldg(c + y1 * 128 + x1);
@@ -173,33 +196,39 @@ __device__ __forceinline__ float2 curl_sample(const uint8_t* curl, float u, floa
 
 // Weather R channel: W x H floats, repeat, bilinear.
 __device__ __forceinline__ float weather_sample(const float* wm, uint32_t W, uint32_t H, float u,
-                                                float v) {
+                                                float v, int* chk = nullptr) {
   const float x = u * (float)W - 0.5f, y = v * (float)H - 0.5f;
   const float fx = floorf(x), fy = floorf(y);
   const int ix = (int)fx, iy = (int)fy;
   const float wx = x - fx, wy = y - fy;
   const int x0 = wrap_mod(ix, (int)W), x1 = wrap_mod(ix + 1, (int)W);
   const int y0 = wrap_mod(iy, (int)H), y1 = wrap_mod(iy + 1, (int)H);
+  if (!idx_ok(chk, x0 >= 0 && x1 >= 0 && y0 >= 0 && y1 >= 0 && (uint32_t)x0 < W && (uint32_t)x1 < W &&
+                       (uint32_t)y0 < H && (uint32_t)y1 < H, kChkWeather))
+    return 0.0f;
   const float a = lerpf(__ldg(wm + y0 * W + x0), __ldg(wm + y0 * W + x1), wx);
   const float b = lerpf(__ldg(wm + y1 * W + x0), __ldg(wm + y1 * W + x1), wx);
   return lerpf(a, b, wy);
 }
 
 // RGBA LUT (float4), clamp-to-edge, bilinear.
-__device__ __forceinline__ float4 lut2d(const float4* lut, int W, int H, float u, float v) {
+__device__ __forceinline__ float4 lut2d(const float4* lut, int W, int H, float u, float v,
+                                        int* chk = nullptr, int site = 0) {
   const float x = u * (float)W - 0.5f, y = v * (float)H - 0.5f;
   const float fx = floorf(x), fy = floorf(y);
   const int ix = (int)fx, iy = (int)fy;
   const float wx = x - fx, wy = y - fy;
   const int x0 = clamp_idx(ix, W), x1 = clamp_idx(ix + 1, W);
   const int y0 = clamp_idx(iy, H), y1 = clamp_idx(iy + 1, H);
+  if (!idx_ok(chk, x0 >= 0 && x1 < W && y0 >= 0 && y1 < H, site)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const float4 a = lerp4(__ldg(lut + y0 * W + x0), __ldg(lut + y0 * W + x1), wx);
   const float4 b = lerp4(__ldg(lut + y1 * W + x0), __ldg(lut + y1 * W + x1), wx);
   return lerp4(a, b, wy);
 }
 
 // Aerial perspective 32x32x64, clamp-to-edge, trilinear.
-__device__ __forceinline__ float4 lut_ap(const float4* lut, float u, float v, float w) {
+__device__ __forceinline__ float4 lut_ap(const float4* lut, float u, float v, float w,
+                                         int* chk = nullptr) {
   const float x = u * 32.0f - 0.5f, y = v * 32.0f - 0.5f, z = w * 64.0f - 0.5f;
   const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
   const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
@@ -207,6 +236,8 @@ __device__ __forceinline__ float4 lut_ap(const float4* lut, float u, float v, fl
   const int x0 = clamp_idx(ix, 32), x1 = clamp_idx(ix + 1, 32);
   const int y0 = clamp_idx(iy, 32), y1 = clamp_idx(iy + 1, 32);
   const int z0 = clamp_idx(iz, 64), z1 = clamp_idx(iz + 1, 64);
+  if (!idx_ok(chk, x0 >= 0 && x1 < 32 && y0 >= 0 && y1 < 32 && z0 >= 0 && z1 < 64, kChkAerial))
+    return make_float4(0.0f, 0.0f, 0.0f, 1.0f);
   auto at = [&](int xx, int yy, int zz) { return __ldg(lut + (zz * 32 + yy) * 32 + xx); };
   const float4 a = lerp4(lerp4(at(x0, y0, z0), at(x1, y0, z0), wx),
                          lerp4(at(x0, y1, z0), at(x1, y1, z0), wx), wy);
@@ -288,39 +319,45 @@ __device__ __forceinline__ float phase_with(const MarchUniforms& u, float cos_t,
 // ---------------------------------------------------- noise access
 template <int ST, int FILT>
 struct Noise {
-  __device__ __forceinline__ static float4 base(const MarchUniforms& u, float x, float y, float z) {
+  __device__ __forceinline__ static float4 base(const MarchUniforms& u, float x, float y, float z,
+                                                int* chk = nullptr) {
     if constexpr (FILT == PSC_FILTER_TEXTURE) {
       return tex3D<float4>(u.tex_base, x, y, z);
     } else {
-      return trilinear_repeat<ST, 128>(u.noise_base, x, y, z, u.noise_scale);
+      return trilinear_repeat<ST, 128>(u.noise_base, x, y, z, u.noise_scale, chk, kChkBase);
     }
   }
-  __device__ __forceinline__ static float4 detail(const MarchUniforms& u, float x, float y, float z) {
+  __device__ __forceinline__ static float4 detail(const MarchUniforms& u, float x, float y, float z,
+                                                  int* chk = nullptr) {
     if constexpr (FILT == PSC_FILTER_TEXTURE) {
       return tex3D<float4>(u.tex_detail, x, y, z);
     } else {
-      return trilinear_repeat<ST, 32>(u.noise_detail, x, y, z, u.noise_scale);
+      return trilinear_repeat<ST, 32>(u.noise_detail, x, y, z, u.noise_scale, chk, kChkDetail);
     }
   }
   // The 2D curl tile and the weather map are small and read at most once per
   // step; they always use the exact FP32-weight path.
-  __device__ __forceinline__ static float2 curl(const MarchUniforms& u, float x, float y) {
-    return curl_sample(u.curl, x, y);
+  __device__ __forceinline__ static float2 curl(const MarchUniforms& u, float x, float y,
+                                                int* chk = nullptr) {
+    return curl_sample(u.curl, x, y, chk);
   }
-  __device__ __forceinline__ static float weather(const MarchUniforms& u, float x, float y) {
-    return weather_sample(u.weather, u.weather_w, u.weather_h, x, y);
+  __device__ __forceinline__ static float weather(const MarchUniforms& u, float x, float y,
+                                                  int* chk = nullptr) {
+    return weather_sample(u.weather, u.weather_w, u.weather_h, x, y, chk);
   }
 };
 
 // cloud_density_common.wgsl:233-251; the grid spans 32 km centred on the
 // origin, any size, double-modulo wrap, 255 = layer type.
 __device__ __forceinline__ uint32_t effective_type(const MarchUniforms& u, float px, float pz,
-                                                   uint32_t layer_type) {
+                                                   uint32_t layer_type, int* chk = nullptr) {
   if (!u.type_grid) return layer_type;
   const float uu = (px + 16000.0f) / 32000.0f;
   const float vv = (pz + 16000.0f) / 32000.0f;
   const int tx = wrap_mod((int)floorf(uu * (float)u.type_w), (int)u.type_w);
   const int ty = wrap_mod((int)floorf(vv * (float)u.type_h), (int)u.type_h);
+  if (!idx_ok(chk, tx >= 0 && ty >= 0 && (uint32_t)tx < u.type_w && (uint32_t)ty < u.type_h, kChkType))
+    return layer_type;
   const uint32_t t = __ldg(u.type_grid + (uint32_t)ty * u.type_w + (uint32_t)tx);
   return t == PSC_TYPE_SENTINEL ? layer_type : t;
 }

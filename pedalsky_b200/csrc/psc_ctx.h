@@ -66,6 +66,7 @@ struct psc_ctx {
   cudaArray_t arr_sky = nullptr;
 
   uint64_t launches = 0;
+  int* d_check = nullptr;  // options.debug_checks: first out-of-range index site
 
   // cloud RT of the half-res / TAA forms of psc_render (grow-only scratch)
   float4* d_rt_l = nullptr;

@@ -250,6 +250,7 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
   u.kahan = c->opts.kahan;
   u.composite = c->opts.composite;
   u.debug_checks = c->opts.debug_checks;
+  u.error_word = nullptr;  // set by launch_view_march in the debug form
 
   u.base_texel_scale = 128.0f / u.base_scale;
   u.detail_texel_scale = 32.0f / u.detail_scale;
@@ -741,6 +742,42 @@ int taa_step(psc_ctx* c, const float4* cur_l, const float4* cur_t, uint32_t w, u
   return PSC_OK;
 }
 
+const char* check_site_name(int site) {
+  static const char* names[] = {"?",         "base noise", "detail noise",     "curl",
+                                "weather",   "type grid",  "transmittance LUT", "sky-view LUT",
+                                "aerial LUT", "blue noise", "pixel",            "layer"};
+  return (site > 0 && site < (int)(sizeof(names) / sizeof(names[0]))) ? names[site] : names[0];
+}
+
+// One view's march.  options.debug_checks runs the PLAIN schedule's checked
+// kernel (exact filtering unless U8 texture): every index is compared with
+// its buffer, the first violation is recorded in a device word and the call
+// waits for the kernel to report it.
+int launch_view_march(psc_ctx* c, psc::MarchUniforms& u, const psc::ViewDev& vd, cudaStream_t s) {
+  if (c->opts.debug_checks) {
+    if (!c->d_check) PSC_CUDA(cudaMalloc(&c->d_check, sizeof(int)), "cudaMalloc check word");
+    PSC_CUDA(cudaMemsetAsync(c->d_check, 0, sizeof(int), s), "check word reset");
+    u.error_word = c->d_check;
+    PscMarchOptions o = c->opts;
+    o.schedule = PSC_SCHED_PLAIN;
+    if (!(o.filter == PSC_FILTER_TEXTURE && o.storage == PSC_STORAGE_U8)) o.filter = PSC_FILTER_EXACT;
+    const int rc = psc::launch_march(u, vd, o, s);
+    if (rc) return fail(rc, "checked march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    ++c->launches;
+    int site = 0;
+    PSC_CUDA(cudaMemcpyAsync(&site, c->d_check, sizeof(int), cudaMemcpyDeviceToHost, s), "check word read");
+    PSC_CUDA(cudaStreamSynchronize(s), "checked march");
+    if (site) return fail(PSC_ERR_DEVICE_CHECK, "debug check: out-of-range %s index (skipped)", check_site_name(site));
+    return PSC_OK;
+  }
+  int rc = PSC_ERR_UNSUPPORTED;
+  if (c->opts.schedule == PSC_SCHED_FAST) rc = psc::launch_march_fast(u, vd, c->opts, s);
+  if (rc == PSC_ERR_UNSUPPORTED) rc = psc::launch_march(u, vd, c->opts, s);
+  if (rc) return fail(rc, "march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  ++c->launches;
+  return PSC_OK;
+}
+
 // The half-res / TAA form of psc_render for one whole-viewport view: march
 // into the cloud RT, resolve, copy out, composite.
 int render_rt_view(psc_ctx* c, const PscView& v, cudaStream_t s) {
@@ -770,11 +807,8 @@ int render_rt_view(psc_ctx* c, const PscView& v, cudaStream_t s) {
   build_uniforms(c, rw, rh, u);
   u.composite = 0;
   psc::ViewDev vd{rw, rh, 0, 0, depth, c->d_rt_l, c->d_rt_t, nullptr};
-  rc = PSC_ERR_UNSUPPORTED;
-  if (c->opts.schedule == PSC_SCHED_FAST) rc = psc::launch_march_fast(u, vd, c->opts, s);
-  if (rc == PSC_ERR_UNSUPPORTED) rc = psc::launch_march(u, vd, c->opts, s);
-  if (rc) return fail(rc, "march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-  ++c->launches;
+  rc = launch_view_march(c, u, vd, s);
+  if (rc) return rc;
   const float4 *src_l = c->d_rt_l, *src_t = c->d_rt_t;
   if (c->opts.taa) {
     rc = taa_step(c, c->d_rt_l, c->d_rt_t, rw, rh, s, &src_l, &src_t);
@@ -809,8 +843,9 @@ int validate_batch(psc_ctx* c, const PscBatchView* views, uint32_t n) {
     return fail(PSC_ERR_MISSING_INPUT, "transmittance/multi-scatter LUTs missing (psc_bake_luts or psc_upload_lut)");
   if (c->opts.schedule != PSC_SCHED_FAST)
     return fail(PSC_ERR_UNSUPPORTED, "the batched kernel implements the FAST schedule (options.schedule)");
-  if (c->opts.half_res || c->opts.taa)
-    return fail(PSC_ERR_UNSUPPORTED, "the batched kernel renders full-resolution views without TAA");
+  if (c->opts.half_res || c->opts.taa || c->opts.debug_checks)
+    return fail(PSC_ERR_UNSUPPORTED,
+                "the batched kernel renders full-resolution views without TAA or debug checks");
   for (uint32_t i = 0; i < n; ++i) {
     const PscBatchView& v = views[i];
     if (!v.width || !v.height || v.width > 32768 || v.height > 32768)
@@ -1271,6 +1306,7 @@ int psc_destroy(psc_ctx* c) {
   dfree(c->d_rt_l);
   dfree(c->d_rt_t);
   dfree(c->d_rt_depth);
+  dfree(c->d_check);
   for (auto& tv : c->taa) free_taa_view(tv);
   dfree(c->d_blue);
   dfree(c->d_weather);
@@ -1588,11 +1624,8 @@ int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
     psc::ViewDev vd{v.width, v.height, v.x_offset, v.y_offset, v.depth,
                     reinterpret_cast<float4*>(v.out_luminance),
                     reinterpret_cast<float4*>(v.out_transmittance), reinterpret_cast<float4*>(v.hdr)};
-    rc = PSC_ERR_UNSUPPORTED;
-    if (c->opts.schedule == PSC_SCHED_FAST) rc = psc::launch_march_fast(u, vd, c->opts, s);
-    if (rc == PSC_ERR_UNSUPPORTED) rc = psc::launch_march(u, vd, c->opts, s);
-    if (rc) return fail(rc, "march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-    ++c->launches;
+    rc = launch_view_march(c, u, vd, s);
+    if (rc) return rc;
   }
   return PSC_OK;
 }
@@ -1685,8 +1718,9 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
     return fail(PSC_ERR_MISSING_INPUT, "transmittance/multi-scatter LUTs missing (psc_bake_luts or psc_upload_lut)");
   if (c->opts.schedule != PSC_SCHED_FAST)
     return fail(PSC_ERR_UNSUPPORTED, "the batched kernel implements the FAST schedule (options.schedule)");
-  if (c->opts.half_res || c->opts.taa)
-    return fail(PSC_ERR_UNSUPPORTED, "the batched kernel renders full-resolution views without TAA");
+  if (c->opts.half_res || c->opts.taa || c->opts.debug_checks)
+    return fail(PSC_ERR_UNSUPPORTED,
+                "the batched kernel renders full-resolution views without TAA or debug checks");
   for (uint32_t i = 0; i < n; ++i) {
     const PscBatchView& v = views[i];
     if (!v.width || !v.height || v.width > 32768 || v.height > 32768)

@@ -141,6 +141,46 @@ def test_texture_filter_path(c1, oracle_noise, sched, storage, filt):
     assert st["ssim"] >= 0.99 and st["mean"] < 5e-2 and np.isfinite(hdr).all()
 
 
+@pytest.mark.parametrize("sched,storage,filt", [
+    ("fast", "f16", "hybrid"), ("plain", "u8", "exact"), ("fast", "bf16", "exact"),
+    ("plain", "u8", "texture")])
+def test_debug_checks_find_no_bad_index_and_keep_the_image(c1, oracle_noise, sched, storage, filt):
+    """options.debug_checks runs the index-checked PLAIN kernel: no site
+    reports an out-of-range index (psc_render would raise), and the image is
+    the PLAIN kernel's (exact filtering unless U8 texture)."""
+    s, luts, ref = c1
+    kw = dict(storage=capi.STORAGE_NAMES[storage], filt=capi.FILTER_NAMES[filt],
+              schedule=SCHEDULES[sched])
+    checked = scenes.plain_320x180(**kw)
+    checked.options.debug_checks = 1
+    L, T, hdr = _gpu.render(checked, oracle_noise, luts, composite_bg=s.background)
+    plain_filt = filt if (filt == "texture" and storage == "u8") else "exact"
+    base = scenes.plain_320x180(storage=capi.STORAGE_NAMES[storage],
+                                filt=capi.FILTER_NAMES[plain_filt], schedule=capi.SCHED_PLAIN)
+    L0, T0, hdr0 = _gpu.render(base, oracle_noise, luts, composite_bg=s.background)
+    # the checked kernel is its own instantiation and may round differently
+    st = rel_stats(hdr, hdr0)
+    assert st["p999"] < 1e-4 and st["max"] < 1e-3, st
+    if plain_filt == "exact":
+        _check(f"plain_320x180/debug_checks/{storage}", hdr, ref)
+
+
+def test_debug_checks_are_rejected_by_the_batched_kernel(oracle_noise):
+    from pedalsky_b200 import batch as B
+    from pedalsky_b200.subsystem import subsystem_for_scene
+    views = scenes.batch_views(2, seed=1, size_scale=0.03, storage=capi.STORAGE_F16,
+                               filt=capi.FILTER_HYBRID)
+    sub = subsystem_for_scene(views[0], luts=None, noise=oracle_noise)
+    o = capi.MarchOptions.from_buffer_copy(sub.options)
+    o.debug_checks = 1
+    sub.set_options(o)
+    b = B.Batch(views, "cuda:0")
+    with pytest.raises(PscError) as e:
+        b.render(sub.handle)
+    assert e.value.code == -8  # PSC_ERR_UNSUPPORTED
+    sub.close()
+
+
 @pytest.mark.parametrize("sched", sorted(SCHEDULES))
 def test_fused_composite_equals_two_pass(c1, oracle_noise, sched):
     s, luts, ref = c1
