@@ -228,10 +228,12 @@ __device__ __forceinline__ float detail_tap(const MarchUniforms& u, float dx, fl
 
 // smoothstep with the reciprocal of (e1 - e0) precomputed (a multiply, not
 // a division); e0 > e1 gives the reversed ramps of cloud_density_common.wgsl.
-__device__ __forceinline__ float ssr(float e0, float inv_w, float x) {
-  const float t = clamp01((x - e0) * inv_w);
+// t = clamp01(x * inv_w + b) with b = -e0 * inv_w is one saturating FMA.
+__device__ __forceinline__ float ssr_b(float inv_w, float b, float x) {
+  const float t = __saturatef(fmaf(x, inv_w, b));
   return t * t * fmaf(-2.0f, t, 3.0f);
 }
+__device__ __forceinline__ float ssr(float e0, float inv_w, float x) { return ssr_b(inv_w, -e0 * inv_w, x); }
 // ndf (cloud_density_common.wgsl:49-91) with reciprocal smoothsteps.
 __device__ __forceinline__ float ndf_fast(float h, uint32_t t, float anvil_bias) {
   switch (t) {
@@ -260,7 +262,7 @@ __device__ __forceinline__ float ndf_fast(float h, uint32_t t, float anvil_bias)
 // density is not gated off (eff >= 0.01), and 2 - lf >= 1, so neither
 // needs its guard.
 __device__ __forceinline__ float shape_from(float2 b, float lf_bias, float nd, float one_minus_eff) {
-  const float lf = clamp01(b.y + lf_bias);
+  const float lf = __saturatef(b.y + lf_bias);
   const float base_cloud = __fdividef(b.x + (1.0f - lf), 2.0f - lf);
   return fmaf(base_cloud, nd, -one_minus_eff);
 }
@@ -268,25 +270,32 @@ __device__ __forceinline__ float shape_from(float2 b, float lf_bias, float nd, f
 // ndf_fast for types 0..6 as two reciprocal smoothsteps with per-type
 // constants: ssr(0, inv_a, h) * g, g = ssr(e1, inv_w1, h) or 1 - that.
 // Chosen once per dense sample, so the light taps carry no switch.
+// b1 = -e1 * inv_w1 (the saturating-FMA form of ssr).  For these types the
+// profile is exactly 0 outside h in [0, 1] (the rising ramp starts at 0 and
+// the second factor reaches 0 at h = 1).
 struct NdfCoef {
-  float inv_a, e1, inv_w1;
+  float inv_a, b1, inv_w1;
   bool flip;
 };
+__device__ __forceinline__ NdfCoef ndf_row(float a, float e1, float w1, bool flip) {
+  const float inv_w1 = 1.0f / w1;
+  return {1.0f / a, -e1 * inv_w1, inv_w1, flip};
+}
 __device__ __forceinline__ NdfCoef ndf_coef(uint32_t t) {
   switch (t) {
-    case 0: return {1.0f / 0.07f, 1.0f, 1.0f / -0.8f, false};
-    case 1: return {1.0f / 0.10f, 0.6f, 1.0f / 0.4f, true};
-    case 2: return {1.0f / 0.15f, 1.0f, 1.0f / -0.6f, false};
-    case 3: return {1.0f / 0.20f, 1.0f, 1.0f / -0.7f, false};
-    case 4: return {1.0f / 0.30f, 0.7f, 1.0f / 0.3f, true};
-    case 5: return {1.0f / 0.40f, 0.6f, 1.0f / 0.4f, true};
-    case 6: return {1.0f / 0.50f, 0.8f, 1.0f / 0.2f, true};
+    case 0: return ndf_row(0.07f, 1.0f, -0.8f, false);
+    case 1: return ndf_row(0.10f, 0.6f, 0.4f, true);
+    case 2: return ndf_row(0.15f, 1.0f, -0.6f, false);
+    case 3: return ndf_row(0.20f, 1.0f, -0.7f, false);
+    case 4: return ndf_row(0.30f, 0.7f, 0.3f, true);
+    case 5: return ndf_row(0.40f, 0.6f, 0.4f, true);
+    case 6: return ndf_row(0.50f, 0.8f, 0.2f, true);
     default: return {0.0f, 0.0f, 0.0f, false};  // unknown types: ndf = 0
   }
 }
 __device__ __forceinline__ float ndf_eval(const NdfCoef& k, float h) {
-  const float g = ssr(k.e1, k.inv_w1, h);
-  return ssr(0.0f, k.inv_a, h) * (k.flip ? 1.0f - g : g);
+  const float g = ssr_b(k.inv_w1, k.b1, h);
+  return ssr_b(k.inv_a, 0.0f, h) * (k.flip ? 1.0f - g : g);
 }
 
 template <int ST, int FILT>
@@ -384,15 +393,18 @@ __device__ __forceinline__ float2 light_tex_tap(const MarchUniforms& u, float x,
   }
 }
 
-template <int ST, class Prof, uint32_t NB>
+// HCHECK: zero taps outside the layer's height range (Cumulonimbus; the
+// other profiles are exactly 0 there already).
+template <int ST, class Prof, bool HCHECK, uint32_t NB>
 __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerConst& L,
                                            const LightRay& lr, const Prof& prof, uint32_t i0,
                                            float& od, float& comp) {
   float2 bt[NB];
   float hh[NB];
+  const float tb = ((float)i0 + 0.5f) * lr.step;
 #pragma unroll
   for (uint32_t j = 0; j < NB; ++j) {
-    const float t = ((float)(i0 + j) + 0.5f) * lr.step;
+    const float t = fmaf((float)j, lr.step, tb);
     const float bt_t = lr.B + t;
     const float r = sqrtf(fmaf(t, bt_t, lr.A));
     const float alt = lr.h0 + __fdividef(t * bt_t, lr.r0 + r);
@@ -401,36 +413,35 @@ __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerCo
     bt[j] = light_tex_tap<ST>(u, fmaf(-lr.kx, h, fmaf(lr.sx, t, lr.px)), fmaf(lr.sy, t, lr.py),
                               fmaf(-lr.kz, h, fmaf(lr.sz, t, lr.pz)));
   }
+  const float ds_step = L.density_scale * lr.step;
 #pragma unroll
   for (uint32_t j = 0; j < NB; ++j) {
     const float h = hh[j];
-    const float d = (h >= 0.0f && h <= 1.0f)
-                        ? clamp01(shape_from(bt[j], L.lf_bias, prof(h), lr.one_minus_eff)) * L.density_scale
-                        : 0.0f;
-    const float term = d * lr.step;
+    float d = __saturatef(shape_from(bt[j], L.lf_bias, prof(h), lr.one_minus_eff));
+    if (HCHECK && !(h >= 0.0f && h <= 1.0f)) d = 0.0f;
     if (u.kahan) {
-      const float y = term - comp;
+      const float y = d * ds_step - comp;
       const float tt = od + y;
       comp = (tt - od) - y;
       od = tt;
     } else {
-      od += term;
+      od = fmaf(d, ds_step, od);
     }
   }
 }
 
-template <int ST, class Prof>
+template <int ST, class Prof, bool HCHECK>
 __device__ __forceinline__ float light_march_tex(const MarchUniforms& u, const LayerConst& L,
                                                  const LightRay& lr, const Prof& prof) {
   const uint32_t n = u.light_steps;
   float od = 0.0f, comp = 0.0f;
   uint32_t i = 0;
-  for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, 4>(u, L, lr, prof, i, od, comp);
+  for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, HCHECK, 4>(u, L, lr, prof, i, od, comp);
   if (i + 2u <= n) {
-    light_taps<ST, Prof, 2>(u, L, lr, prof, i, od, comp);
+    light_taps<ST, Prof, HCHECK, 2>(u, L, lr, prof, i, od, comp);
     i += 2u;
   }
-  if (i < n) light_taps<ST, Prof, 1>(u, L, lr, prof, i, od, comp);
+  if (i < n) light_taps<ST, Prof, HCHECK, 1>(u, L, lr, prof, i, od, comp);
   return od;
 }
 
@@ -463,11 +474,11 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
     lr.kz = L.skew_z * L.skew_thickness * k;
     lr.step = step;
     lr.one_minus_eff = 1.0f - eff;
-    if (type == 7u) return light_march_tex<ST>(u, L, lr, NdfCb{L.anvil_bias});
-    return light_march_tex<ST>(
+    if (type == 7u) return light_march_tex<ST, NdfCb, true>(u, L, lr, NdfCb{L.anvil_bias});
+    return light_march_tex<ST, NdfGeneral, false>(
         u, L, lr,
         NdfGeneral{u.type_grid ? ndf_coef(type)
-                               : NdfCoef{L.ndf_inv_a, L.ndf_e1, L.ndf_inv_w1, L.ndf_mode == 2u}});
+                               : NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1, L.ndf_mode == 2u}});
   }
   float od = 0.0f, comp = 0.0f;
   for (uint32_t i = 0; i < u.light_steps; ++i) {
@@ -659,7 +670,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
                                         fmaf(az, u.curl_texel_scale, -0.5f));
         const float eff = clamp01(wr * L.coverage);
         const float nd = (!u.type_grid && L.ndf_mode)
-                             ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_e1, L.ndf_inv_w1, L.ndf_mode == 2u}, h)
+                             ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1, L.ndf_mode == 2u}, h)
                              : ndf_fast(h, type, L.anvil_bias);
         float cloud = shape_from(bs, L.lf_bias, nd, 1.0f - eff);
         if (eff >= 0.01f) {  // coverage gate (cloud_march.wgsl:450-451)

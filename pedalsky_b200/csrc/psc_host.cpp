@@ -321,11 +321,11 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
     static const uint32_t kMode[7] = {1, 2, 1, 1, 2, 2, 2};
     if (L.cloud_type < 7) {
       o.ndf_inv_a = 1.0f / kA[L.cloud_type];
-      o.ndf_e1 = kE1[L.cloud_type];
       o.ndf_inv_w1 = 1.0f / kW1[L.cloud_type];
+      o.ndf_b1 = -kE1[L.cloud_type] * o.ndf_inv_w1;
       o.ndf_mode = kMode[L.cloud_type];
     } else {
-      o.ndf_inv_a = o.ndf_e1 = o.ndf_inv_w1 = 0.0f;
+      o.ndf_inv_a = o.ndf_b1 = o.ndf_inv_w1 = 0.0f;
       o.ndf_mode = 0;
     }
     o.r_bottom = (double)w.planet_radius_m + (double)L.base_m;

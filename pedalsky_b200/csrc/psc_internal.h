@@ -40,9 +40,10 @@ struct LayerConst {
   // Approx-Mie constants (cloud_phase_constants); exact for every layer
   // type except Cumulonimbus, whose diameter depends on height.
   float g_hg, g_d, alpha, w_d, ice;
-  // ndf of types 0..6 as ssr(0, ndf_inv_a, h) * g, g = ssr(ndf_e1,
-  // ndf_inv_w1, h) or 1 - g (ndf_mode 1 / 2); ndf_mode 0: evaluate by type
-  float ndf_inv_a, ndf_e1, ndf_inv_w1;
+  // ndf of types 0..6 as ssr(0, ndf_inv_a, h) * g, g = smoothstep ramp
+  // clamp01(h * ndf_inv_w1 + ndf_b1) or 1 - that (ndf_mode 1 / 2);
+  // ndf_mode 0: evaluate by type
+  float ndf_inv_a, ndf_b1, ndf_inv_w1;
   uint32_t ndf_mode;
   float _pad[2];
   double r_bottom, r_top;  // planet_radius + base/top, FP64
