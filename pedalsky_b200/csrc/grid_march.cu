@@ -147,11 +147,11 @@ __device__ __forceinline__ void lighting(const MarchUniforms& u, const LayerCons
 #pragma unroll
     for (int n = 0; n < kMaxOct; ++n) l.cf[n] = coef[n];
   }
-  const float3 ts = sun_trans_fast(u, alt, ux, uy, uz);
+  float3 ts, sky;
+  lut_lookups(u, alt, ux, uy, uz, ts, sky);
   l.sun[0] = u.sun_illum[0] * ts.x;
   l.sun[1] = u.sun_illum[1] * ts.y;
   l.sun[2] = u.sun_illum[2] * ts.z;
-  const float3 sky = sky_fast(u, alt, ux, uy, uz);
   const float ag = mixf(0.3f, 1.0f, h) * u.ambient;
   float lr = 0.0f, lg = 0.0f, lb = 0.0f;
   if (u.lightning_radius > 0.0f) {

@@ -8,9 +8,10 @@
 //   * per dense sample: the octave exponentials exp(-sigma*od*b^n) for
 //     b = 1/2 come from one exponential and repeated squaring, which also
 //     yields Beer (n = 0) and the powder term exp(-2*sigma*od);
-//   * the transmittance-LUT and sky-view lookups use well-conditioned forms
-//     (r = R + alt, rho = sqrt(alt*(2R + alt)), zenith angles via atan2) with
-//     a polynomial arctangent;
+//   * the transmittance-LUT and sky-view lookups share one altitude geometry
+//     in well-conditioned forms (r = R + alt, rho = sqrt(alt*(2R + alt)),
+//     zenith angles via atan2) with a polynomial arctangent;
+//   * texel floors and indices come from one round-down add (floor_bits);
 //   * weather/type fetches are skipped where the height gate already
 //     returns zero density;
 //   * texel coordinates are formed with one FMA per axis.
@@ -100,6 +101,20 @@ __device__ __forceinline__ float4 trilinear_texel(const void* vol, float x, floa
   return r;
 }
 
+// floor(x) and its integer bits for |x| < 2^22: one round-down add puts
+// 1.5 * 2^23 + floor(x) in a float whose low mantissa bits are floor(x)
+// (two's complement, so masks wrap negative indices), and subtracting the
+// constant back is exact.  Larger |x| (millions of texels, far beyond any
+// ray here) still yields masked, in-bounds indices.
+struct FloorBits {
+  float f;
+  uint32_t i;
+};
+__device__ __forceinline__ FloorBits floor_bits(float x) {
+  const float s = __fadd_rd(x, 12582912.0f);
+  return {s - 12582912.0f, __float_as_uint(s)};
+}
+
 __device__ __forceinline__ float2 h2f(uint32_t w) {
   return __half22float2(*reinterpret_cast<const __half2*>(&w));
 }
@@ -108,11 +123,10 @@ __device__ __forceinline__ float2 h2f(uint32_t w) {
 // coordinates in texel units: one 16-byte quad load per slab, FP32 weights.
 // Returns (R, 0.625G + 0.25B + 0.125A), both in [0, 1].
 __device__ __forceinline__ float2 base_quad_tap(const uint4* q, float x, float y, float z) {
-  const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
-  const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
-  const float wx = x - fx, wy = y - fy, wz = z - fz;
-  const uint32_t r = ((uint32_t)iy & 127u) * 128u + ((uint32_t)ix & 127u);
-  const uint32_t z0 = (uint32_t)iz & 127u, z1 = (uint32_t)(iz + 1) & 127u;
+  const FloorBits bx = floor_bits(x), by = floor_bits(y), bz = floor_bits(z);
+  const float wx = x - bx.f, wy = y - by.f, wz = z - bz.f;
+  const uint32_t r = (by.i & 127u) * 128u + (bx.i & 127u);
+  const uint32_t z0 = bz.i & 127u, z1 = (bz.i + 1u) & 127u;
   const uint4 a = __ldg(q + z0 * 16384u + r);
   const uint4 b = __ldg(q + z1 * 16384u + r);
   const float2 tx = make_float2(wx, wx), ty = make_float2(wy, wy);
@@ -126,11 +140,10 @@ __device__ __forceinline__ float2 base_quad_tap(const uint4* q, float x, float y
 // one 8-byte quad load per slab; the two slabs ride the two FP32x2 lanes.
 // Returns 0.625R + 0.25G + 0.125B in [0, 1].
 __device__ __forceinline__ float detail_quad_tap(const uint2* q, float x, float y, float z) {
-  const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
-  const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
-  const float wx = x - fx, wy = y - fy, wz = z - fz;
-  const uint32_t r = ((uint32_t)iy & 31u) * 32u + ((uint32_t)ix & 31u);
-  const uint32_t z0 = (uint32_t)iz & 31u, z1 = (uint32_t)(iz + 1) & 31u;
+  const FloorBits bx = floor_bits(x), by = floor_bits(y), bz = floor_bits(z);
+  const float wx = x - bx.f, wy = y - by.f, wz = z - bz.f;
+  const uint32_t r = (by.i & 31u) * 32u + (bx.i & 31u);
+  const uint32_t z0 = bz.i & 31u, z1 = (bz.i + 1u) & 31u;
   const uint2 a = __ldg(q + z0 * 1024u + r);
   const uint2 b = __ldg(q + z1 * 1024u + r);
   const float2 a0 = h2f(a.x), a1 = h2f(a.y), b0 = h2f(b.x), b1 = h2f(b.y);
@@ -159,11 +172,11 @@ struct CurlFetch {
   float wx, wy;
 };
 __device__ __forceinline__ CurlFetch curl_fetch(const uint4* q, float x, float y) {
-  const float fx = floorf(x), fy = floorf(y);
+  const FloorBits bx = floor_bits(x), by = floor_bits(y);
   CurlFetch c;
-  c.q = ldg_v4_early(q + ((uint32_t)(int)fy & 127u) * 128u + ((uint32_t)(int)fx & 127u));
-  c.wx = x - fx;
-  c.wy = y - fy;
+  c.q = ldg_v4_early(q + (by.i & 127u) * 128u + (bx.i & 127u));
+  c.wx = x - bx.f;
+  c.wy = y - by.f;
   return c;
 }
 __device__ __forceinline__ float2 curl_blend(const CurlFetch& c) {
@@ -499,47 +512,57 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
   return od;
 }
 
-// Transmittance-LUT lookup (cloud_march.wgsl:328-354) with r = R + alt and
-// rho = sqrt(alt*(2R + alt)) instead of differences of squares at 6e6 m.
-__device__ __forceinline__ float3 sun_trans_fast(const MarchUniforms& u, float alt, float ux,
-                                                 float uy, float uz) {
-  const float R = u.planet_r;
-  const float a = fmaxf(alt, 1.0f);
-  const float r = R + a;
-  const float rho = sqrtf(a * (2.0f * R + a));
-  const float mu = clampf(fmaf(ux, u.sun[0], fmaf(uy, u.sun[1], uz * u.sun[2])), -1.0f, 1.0f);
-  if (mu <= -__fdividef(rho, r)) return make_float3(0.0f, 0.0f, 0.0f);
-  const float top = u.atmo_top;
-  const float rm = r * mu;
-  const float disc = fmaf(rm, rm, (top - r) * (top + r));
-  const float d = fmaxf(sqrtf(fmaxf(disc, 0.0f)) - rm, 0.0f);
-  const float d_min = top - r, d_max = rho + u.big_h;
-  const float xm = clamp01(__fdividef(d - d_min, fmaxf(d_max - d_min, 1.0f)));
-  const float xr = __fdividef(rho, fmaxf(u.big_h, 1.0f));
-  const float4 t = u.tex_trans ? tex2D<float4>(u.tex_trans, xm, xr) : lut2d(u.lut_trans, 256, 64, xm, xr);
-  return make_float3(t.x, t.y, t.z);
+// atan2(y, x) for y >= 0 (the zenith angle of a direction), as fast_atan2.
+__device__ __forceinline__ float atan2_upper(float y, float x) {
+  const float ax = fabsf(x);
+  const float a = __fdividef(fminf(ax, y), fmaxf(fmaxf(ax, y), 1e-30f));
+  float r = atan01(a);
+  if (y > ax) r = 1.57079632679f - r;
+  return x < 0.0f ? 3.14159265359f - r : r;
 }
 
-// Sky-view ambient (cloud_march.wgsl:672-700): local up, zenith angle and
-// horizon angle through atan2 (pi - asin(R/r) = pi/2 + atan2(rho, R)).
-__device__ __forceinline__ float3 sky_fast(const MarchUniforms& u, float alt, float ux, float uy,
-                                           float uz) {
+// The two LUT lookups of a dense sample, sharing the altitude geometry
+// (r = R + alt and rho = sqrt(alt (2R + alt)) instead of differences of
+// squares at 6e6 m):
+//  * transmittance toward the sun (cloud_march.wgsl:328-354): earth shadow,
+//    then the Bruneton uv with a = max(alt, 1);
+//  * sky-view ambient at the local up (cloud_march.wgsl:672-700): zenith
+//    angle, horizon angle pi/2 + atan2(rho, R) (rho < R below 2600 km) and
+//    azimuth; scaled by the sun illuminance.
+__device__ __forceinline__ void lut_lookups(const MarchUniforms& u, float alt, float ux, float uy,
+                                            float uz, float3& trans, float3& sky) {
   const float R = u.planet_r;
-  const float a = fmaxf(alt, 0.0f);
-  const float rho = sqrtf(a * (2.0f * R + a));
-  const float vza = fast_atan2(sqrtf(fmaf(ux, ux, uz * uz)), uy);
-  // pi/2 + atan2(rho, R) with rho < R (altitudes below 2600 km)
-  const float zha = 1.57079632679f + atan01(fminf(__fdividef(rho, R), 1.0f));
-  float vv;
-  if (vza < zha) {
-    vv = sqrtf(clamp01(__fdividef(vza, fmaxf(zha, 1e-6f)))) * 0.5f;
+  const float a0 = fmaxf(alt, 0.0f);
+  const float rho0 = sqrtf(a0 * (2.0f * R + a0));
+  // transmittance
+  const float a = fmaxf(alt, 1.0f);
+  const float r = R + a;
+  const float rho = alt >= 1.0f ? rho0 : u.rho_1m;
+  const float mu = clampf(fmaf(ux, u.sun[0], fmaf(uy, u.sun[1], uz * u.sun[2])), -1.0f, 1.0f);
+  if (mu <= -__fdividef(rho, r)) {
+    trans = make_float3(0.0f, 0.0f, 0.0f);
   } else {
-    vv = 0.5f + sqrtf(clamp01(__fdividef(vza - zha, fmaxf(kPi - zha, 1e-6f)))) * 0.5f;
+    const float top = u.atmo_top;
+    const float rm = r * mu;
+    const float disc = fmaf(rm, rm, (top - r) * (top + r));
+    const float d = fmaxf(sqrtf(fmaxf(disc, 0.0f)) - rm, 0.0f);
+    const float d_min = top - r, d_max = rho + u.big_h;
+    const float xm = __saturatef(__fdividef(d - d_min, fmaxf(d_max - d_min, 1.0f)));
+    const float xr = rho * u.inv_big_h;
+    const float4 t = u.tex_trans ? tex2D<float4>(u.tex_trans, xm, xr) : lut2d(u.lut_trans, 256, 64, xm, xr);
+    trans = make_float3(t.x, t.y, t.z);
   }
+  // sky view
+  const float vza = atan2_upper(sqrtf(fmaf(ux, ux, uz * uz)), uy);
+  const float zha = 1.57079632679f + atan01(fminf(rho0 * u.inv_planet_r, 1.0f));
+  const bool below = vza < zha;
+  const float num = below ? vza : vza - zha;
+  const float den = below ? zha : kPi - zha;
+  const float vv = fmaf(0.5f, sqrtf(__saturatef(__fdividef(num, fmaxf(den, 1e-6f)))), below ? 0.0f : 0.5f);
   float du = (fast_atan2(ux, uz) - u.sun_az) * (1.0f / (2.0f * kPi));
   du = du - floorf(du);
-  const float4 s = u.tex_sky ? tex2D<float4>(u.tex_sky, du, vv) : lut2d(u.lut_sky, 192, 108, du, vv);
-  return make_float3(s.x * u.sun_illum[0], s.y * u.sun_illum[1], s.z * u.sun_illum[2]);
+  const float4 sk = u.tex_sky ? tex2D<float4>(u.tex_sky, du, vv) : lut2d(u.lut_sky, 192, 108, du, vv);
+  sky = make_float3(sk.x * u.sun_illum[0], sk.y * u.sun_illum[1], sk.z * u.sun_illum[2]);
 }
 
 // Weather R channel, repeat + bilinear; a uniform map is its value, power-of-
@@ -550,10 +573,9 @@ __device__ __forceinline__ float weather_fast(const MarchUniforms& u, float uu, 
   if (u.weather_uniform) return u.weather_value;  // bilinear of a constant is the constant
   if (u.weather_quad) {
     const float x = fmaf(uu, (float)W, -0.5f), y = fmaf(vv, (float)H, -0.5f);
-    const float fx = floorf(x), fy = floorf(y);
-    const float wx = x - fx, wy = y - fy;
-    const float4 q = __ldg(u.weather_quad + ((uint32_t)(int)fy & (H - 1)) * W + ((uint32_t)(int)fx & (W - 1)));
-    return lerpf(lerpf(q.x, q.y, wx), lerpf(q.z, q.w, wx), wy);
+    const FloorBits bx = floor_bits(x), by = floor_bits(y);
+    const float4 q = __ldg(u.weather_quad + (by.i & (H - 1)) * W + (bx.i & (W - 1)));
+    return lerpf(lerpf(q.x, q.y, x - bx.f), lerpf(q.z, q.w, x - bx.f), y - by.f);
   }
   if (((W & (W - 1)) | (H & (H - 1))) != 0) return weather_sample(u.weather, W, H, uu, vv);
   const float x = fmaf(uu, (float)W, -0.5f), y = fmaf(vv, (float)H, -0.5f);
@@ -687,29 +709,26 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
 
           if (density > 1e-3f) {
             const float yy = py3 + u.planet_r;
-            const float inv_r = __frcp_rn(u.planet_r + alt);
+            const float inv_r = __fdividef(1.0f, u.planet_r + alt);
             const float ux = px3 * inv_r, uy = yy * inv_r, uz = pz3 * inv_r;
             const float od = light_od<ST, FILT>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
             const float st_r = L.sigma_t[0], st_g = L.sigma_t[1], st_b = L.sigma_t[2];
             const float xr = st_r * od, xg = st_g * od, xb = st_b * od;
-            // e[n] = exp(-x * b^n); with b = 1/2 one exponential at the last live
-            // octave m and repeated squaring give every lower octave.
+            // e[n] = exp(-x * b^n); with b = 1/2 one exponential at n = 3 and
+            // repeated squaring give every lower octave (octaves past the
+            // count carry zero coefficients).
             float er[kMaxOct], eg[kMaxOct], eb[kMaxOct];
             const int m = (int)noct - 1;
             if (u.b_half) {
-              const float bl = u.bpow[m];
-              float vr = __expf(-xr * bl), vg = __expf(-xg * bl), vb = __expf(-xb * bl);
+              float vr = __expf(xr * -0.125f), vg = __expf(xg * -0.125f), vb = __expf(xb * -0.125f);
 #pragma unroll
               for (int n = kMaxOct - 1; n >= 0; --n) {
-                const bool live = n <= m;
-                er[n] = live ? vr : 0.0f;
-                eg[n] = live ? vg : 0.0f;
-                eb[n] = live ? vb : 0.0f;
-                if (live) {
-                  vr *= vr;
-                  vg *= vg;
-                  vb *= vb;
-                }
+                er[n] = vr;
+                eg[n] = vg;
+                eb[n] = vb;
+                vr *= vr;
+                vg *= vg;
+                vb *= vb;
               }
             } else {
 #pragma unroll
@@ -720,11 +739,11 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
                 eb[n] = live ? __expf(-xb * u.bpow[n]) : 0.0f;
               }
             }
-            const float br = er[0], bg = eg[0], bb = eb[0];  // Beer, n = 0
-            const float pr = 1.0f - br * br, pg = 1.0f - bg * bg, pb = 1.0f - bb * bb;
-            const float enr = mixf(br, br * pr * 2.0f, u.powder);
-            const float eng = mixf(bg, bg * pg * 2.0f, u.powder);
-            const float enb = mixf(bb, bb * pb * 2.0f, u.powder);
+            // Beer-powder mix(b, 2 b (1 - b^2), w) = b (1 + w (1 - 2 b^2)), b = e[0]
+            const float br = er[0], bg = eg[0], bb = eb[0];
+            const float enr = br * fmaf(u.powder, fmaf(-2.0f * br, br, 1.0f), 1.0f);
+            const float eng = bg * fmaf(u.powder, fmaf(-2.0f * bg, bg, 1.0f), 1.0f);
+            const float enb = bb * fmaf(u.powder, fmaf(-2.0f * bb, bb, 1.0f), 1.0f);
             float cf[kMaxOct];
             if (cb) {
               const float mt = smoothstepf(0.60f, 0.85f, h);
@@ -743,11 +762,11 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
               sg = fmaf(cf[n], eg[n], sg);
               sb = fmaf(cf[n], eb[n], sb);
             }
-            const float3 ts = sun_trans_fast(u, alt, ux, uy, uz);
+            float3 ts, sky;
+            lut_lookups(u, alt, ux, uy, uz, ts, sky);
             sr *= u.sun_illum[0] * ts.x;
             sg *= u.sun_illum[1] * ts.y;
             sb *= u.sun_illum[2] * ts.z;
-            const float3 sky = sky_fast(u, alt, ux, uy, uz);
             const float ag = mixf(0.3f, 1.0f, clamp01(h)) * u.ambient;
             float lr = 0.0f, lg = 0.0f, lb = 0.0f;
             if (u.lightning_radius > 0.0f) {

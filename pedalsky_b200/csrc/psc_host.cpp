@@ -263,6 +263,10 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
   {
     const double top = w.atmosphere_top_m, R = w.planet_radius_m;
     u.big_h = (float)std::sqrt(std::max(top * top - R * R, 0.0));
+    u.inv_big_h = 1.0f / std::fmax(u.big_h, 1.0f);
+    u.inv_planet_r = 1.0f / (float)R;
+    const float Rf = (float)R;
+    u.rho_1m = std::sqrt(1.0f * (2.0f * Rf + 1.0f));
   }
   u.inv_cos_sun = 1.0f / std::fmax(f.sun_direction[1], 0.05f);
   u.b_half = p.multi_scatter_b == 0.5f ? 1u : 0u;

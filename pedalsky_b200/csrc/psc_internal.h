@@ -91,6 +91,9 @@ struct alignas(16) MarchUniforms {
   float sun_az;              // atan2(sun.x, sun.z)
   float top_minus_r_sq_unused;
   float big_h;               // sqrt(atmo_top^2 - planet_r^2)
+  float inv_big_h;           // 1 / max(big_h, 1)
+  float inv_planet_r;        // 1 / planet_r
+  float rho_1m;              // sqrt(2 planet_r + 1): rho at 1 m altitude
   float inv_cos_sun;         // 1 / max(sun.y, 0.05)
   uint32_t b_half;           // multi_scatter_b == 0.5 exactly
   float apow[8], bpow[8], cpow[8];  // a^n, b^n, c^n
