@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
   __shared__ MarchUniforms su;
   __shared__ ViewDev sv;
   __shared__ uint32_t s_tile;
-  __shared__ float s_t0[8 * NT], s_t1[8 * NT];
+  __shared__ float s_t0[8 * NT], s_t1[8 * NT], s_aux[kAuxWords * NT];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t warps_x = tile_w >> 3;  // 8x4-pixel warp tiles per tile row
   uint32_t cur = 0xffffffffu;
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
     const uint32_t px = tx * tile_w + (warp % warps_x) * 8u + (lane & 7u);
     const uint32_t py = ty * tile_h + (warp / warps_x) * 4u + (lane >> 3);
     if (px < sv.width && py < sv.height)
-      march_pixel_fast<ST, FILT>(su, sv, px, py, s_t0, s_t1, NT, threadIdx.x);
+      march_pixel_fast<ST, FILT>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
     __syncthreads();  // su, sv and s_tile are rewritten by the next iteration
   }
 }

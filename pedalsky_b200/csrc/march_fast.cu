@@ -17,12 +17,12 @@ constexpr int kThreads = 128;
 template <int ST, int FILT>
 __global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constant__ MarchUniforms u,
                                                             const __grid_constant__ ViewDev v) {
-  __shared__ float s_t0[8 * kThreads], s_t1[8 * kThreads];
+  __shared__ float s_t0[8 * kThreads], s_t1[8 * kThreads], s_aux[kAuxWords * kThreads];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t px = blockIdx.x * kTileW + (warp & 1u) * 8u + (lane & 7u);
   const uint32_t py = blockIdx.y * kTileH + (warp >> 1) * 4u + (lane >> 3);
   if (px >= v.width || py >= v.height) return;
-  march_pixel_fast<ST, FILT>(u, v, px, py, s_t0, s_t1, kThreads, threadIdx.x);
+  march_pixel_fast<ST, FILT>(u, v, px, py, s_t0, s_t1, s_aux, kThreads, threadIdx.x);
 }
 
 template <int ST, int FILT>

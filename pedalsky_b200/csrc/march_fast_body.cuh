@@ -595,12 +595,19 @@ __device__ __forceinline__ float one_minus_exp_neg(float y, float e) {
                    : 1.0f - e;
 }
 
+// Per-thread shared-memory words of march_pixel_fast beyond the layer
+// intervals: the per-layer octave coefficients (read once per dense sample)
+// and the compensated optical depths of the Kahan form, kept out of the
+// registers the step loop needs.
+constexpr uint32_t kAuxWords = kMaxOct + 6;
+
 // One primary ray of the FAST schedule.  `s_t0/s_t1` are this CTA's shared
 // arrays of per-layer entry/exit distances, laid out [layer][slot] with
-// `stride` slots; `slot` is this thread's column.
+// `stride` slots; `slot` is this thread's column.  `s_aux` holds kAuxWords
+// words per thread, laid out the same way.
 template <int ST, int FILT>
 __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const ViewDev& v, uint32_t px,
-                                                 uint32_t py, float* s_t0, float* s_t1,
+                                                 uint32_t py, float* s_t0, float* s_t1, float* s_aux,
                                                  uint32_t stride, uint32_t slot) {
 
   // Per-lane layer intervals live in shared memory for the march, so the 16
@@ -631,21 +638,14 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
   const float jitter = __ldg(u.blue + sy * 64u + sx);
   const uint32_t noct = u.octaves;
 
-  // Dual-lobe HG lobes do not depend on the layer: evaluate once per ray.
-  float hg_coef[kMaxOct];
-  if (u.phase_mode == PSC_PHASE_DUAL_LOBE_HG) {
+  float* const s_coef = s_aux;                // [kMaxOct][stride]
+  float* const s_kahan = s_aux + kMaxOct * stride;  // od r,g,b then comp r,g,b
+  if (u.kahan) {
 #pragma unroll
-    for (int n = 0; n < kMaxOct; ++n) {
-      const float c = u.cpow[n];
-      hg_coef[n] = (n < (int)noct) ? u.apow[n] * fwd_gain *
-                                         mixf(hg_phase(cos_theta, u.hg_f * c),
-                                              hg_phase(cos_theta, u.hg_b * c), u.hg_w)
-                                   : 0.0f;
-    }
+    for (int c = 0; c < 6; ++c) s_kahan[c * stride + slot] = 0.0f;
   }
 
   float Lr = 0.0f, Lg = 0.0f, Lb = 0.0f, Tr = 1.0f, Tg = 1.0f, Tb = 1.0f;
-  float odr = 0.0f, odg = 0.0f, odb = 0.0f, kr = 0.0f, kg = 0.0f, kb = 0.0f;
   float tw = 0.0f, twn = 0.0f;
   const uint32_t nl = u.layer_count;
 
@@ -660,16 +660,22 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
     const float step = __fdividef(segment, (float)u.cloud_steps);
     const bool cb = L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE;
 
-    // per ray and layer: a^n * phase_n * forward gain
-    float coef[kMaxOct];
+    // per ray and layer: a^n * phase_n * forward gain (shared memory)
     if (u.phase_mode == PSC_PHASE_DUAL_LOBE_HG) {
 #pragma unroll
-      for (int n = 0; n < kMaxOct; ++n) coef[n] = hg_coef[n];
+      for (int n = 0; n < kMaxOct; ++n) {
+        const float c = u.cpow[n];
+        s_coef[n * stride + slot] =
+            (n < (int)noct) ? u.apow[n] * fwd_gain *
+                                  mixf(hg_phase(cos_theta, u.hg_f * c), hg_phase(cos_theta, u.hg_b * c), u.hg_w)
+                            : 0.0f;
+      }
     } else if (!cb) {
       const PhaseConst pc{L.g_hg, L.g_d, L.alpha, L.w_d, L.ice};
 #pragma unroll
       for (int n = 0; n < kMaxOct; ++n)
-        coef[n] = (n < (int)noct) ? u.apow[n] * fwd_gain * phase_with(u, cos_theta, u.cpow[n], pc) : 0.0f;
+        s_coef[n * stride + slot] =
+            (n < (int)noct) ? u.apow[n] * fwd_gain * phase_with(u, cos_theta, u.cpow[n], pc) : 0.0f;
     }
 
     for (uint32_t s = 0; s < u.cloud_steps; ++s) {
@@ -753,7 +759,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
                 cf[n] = (n < (int)noct) ? u.apow[n] * fwd_gain * phase_with(u, cos_theta, u.cpow[n], pc) : 0.0f;
             } else {
 #pragma unroll
-              for (int n = 0; n < kMaxOct; ++n) cf[n] = coef[n];
+              for (int n = 0; n < kMaxOct; ++n) cf[n] = s_coef[n * stride + slot];
             }
             float sr = 0.0f, sg = 0.0f, sb = 0.0f;
 #pragma unroll
@@ -793,18 +799,21 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             Lb += slb;
             tw = fmaf(sw, t, tw);
             twn += sw;
-            if (u.kahan) {
-              const float ar = yr - kr, ag2 = yg - kg, ab = yb - kb;
-              const float nr = odr + ar, ng = odg + ag2, nb = odb + ab;
-              kr = (nr - odr) - ar;
-              kg = (ng - odg) - ag2;
-              kb = (nb - odb) - ab;
-              odr = nr;
-              odg = ng;
-              odb = nb;
-              Tr = __expf(-odr);
-              Tg = __expf(-odg);
-              Tb = __expf(-odb);
+            if (u.kahan) {  // T = exp(-sum), the sum compensated (shared memory)
+              const float y3[3] = {yr, yg, yb};
+              float T3[3];
+#pragma unroll
+              for (int c = 0; c < 3; ++c) {
+                const float od = s_kahan[c * stride + slot], kc = s_kahan[(3 + c) * stride + slot];
+                const float a = y3[c] - kc;
+                const float nsum = od + a;
+                s_kahan[(3 + c) * stride + slot] = (nsum - od) - a;
+                s_kahan[c * stride + slot] = nsum;
+                T3[c] = __expf(-nsum);
+              }
+              Tr = T3[0];
+              Tg = T3[1];
+              Tb = T3[2];
             } else {
               Tr *= smr;
               Tg *= smg;
