@@ -14,10 +14,16 @@ constexpr int kTileW = 16;
 constexpr int kTileH = 8;
 constexpr int kThreads = 128;
 
+// Shared memory per CTA: the entry/exit distances of each of the view's
+// layers and kAuxWords more words, per thread (dynamic, sized at launch).
 template <int ST, int FILT>
 __global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constant__ MarchUniforms u,
                                                             const __grid_constant__ ViewDev v) {
-  __shared__ float s_t0[8 * kThreads], s_t1[8 * kThreads], s_aux[kAuxWords * kThreads];
+  extern __shared__ float s_dyn[];
+  const uint32_t nl = u.layer_count;
+  float* const s_t0 = s_dyn;
+  float* const s_t1 = s_dyn + nl * kThreads;
+  float* const s_aux = s_dyn + 2u * nl * kThreads;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t px = blockIdx.x * kTileW + (warp & 1u) * 8u + (lane & 7u);
   const uint32_t py = blockIdx.y * kTileH + (warp >> 1) * 4u + (lane >> 3);
@@ -28,7 +34,8 @@ __global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constan
 template <int ST, int FILT>
 cudaError_t launch_fast(const MarchUniforms& u, const ViewDev& v, cudaStream_t s) {
   const dim3 grid((v.width + kTileW - 1) / kTileW, (v.height + kTileH - 1) / kTileH);
-  k_march_fast<ST, FILT><<<grid, kThreads, 0, s>>>(u, v);
+  const size_t smem = (2u * u.layer_count + kAuxWords) * kThreads * sizeof(float);
+  k_march_fast<ST, FILT><<<grid, kThreads, smem, s>>>(u, v);
   return cudaGetLastError();
 }
 

@@ -596,10 +596,11 @@ __device__ __forceinline__ float one_minus_exp_neg(float y, float e) {
 }
 
 // Per-thread shared-memory words of march_pixel_fast beyond the layer
-// intervals: the per-layer octave coefficients (read once per dense sample)
-// and the compensated optical depths of the Kahan form, kept out of the
-// registers the step loop needs.
-constexpr uint32_t kAuxWords = kMaxOct + 6;
+// intervals, all touched at most once per dense sample and so kept out of
+// the registers the step loop needs: the per-layer octave coefficients,
+// the compensated optical depths of the Kahan form, the radiance and the
+// aerial-perspective distance weights.
+constexpr uint32_t kAuxWords = kMaxOct + 6 + 5;
 
 // One primary ray of the FAST schedule.  `s_t0/s_t1` are this CTA's shared
 // arrays of per-layer entry/exit distances, laid out [layer][slot] with
@@ -616,8 +617,10 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
   setup_ray(u, v, px, py, rs);
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    s_t0[j * stride + slot] = rs.t0[j];
-    s_t1[j * stride + slot] = rs.t1[j];
+    if ((uint32_t)j < u.layer_count) {  // the arrays hold layer_count rows
+      s_t0[j * stride + slot] = rs.t0[j];
+      s_t1[j * stride + slot] = rs.t1[j];
+    }
   }
   const uint32_t order = rs.order, hit_mask = rs.hit_mask;
   const float ray_r0 = rs.r0, ray_h0 = rs.h0;
@@ -638,15 +641,17 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
   const float jitter = __ldg(u.blue + sy * 64u + sx);
   const uint32_t noct = u.octaves;
 
-  float* const s_coef = s_aux;                // [kMaxOct][stride]
+  float* const s_coef = s_aux;                      // [kMaxOct][stride]
   float* const s_kahan = s_aux + kMaxOct * stride;  // od r,g,b then comp r,g,b
+  float* const s_acc = s_kahan + 6 * stride;        // L r,g,b, sum(w t), sum(w)
   if (u.kahan) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) s_kahan[c * stride + slot] = 0.0f;
   }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) s_acc[c * stride + slot] = 0.0f;
 
-  float Lr = 0.0f, Lg = 0.0f, Lb = 0.0f, Tr = 1.0f, Tg = 1.0f, Tb = 1.0f;
-  float tw = 0.0f, twn = 0.0f;
+  float Tr = 1.0f, Tg = 1.0f, Tb = 1.0f;
   const uint32_t nl = u.layer_count;
 
   for (uint32_t k = 0; k < nl; ++k) {
@@ -794,11 +799,11 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             const float slg = Tg * isg * __fdividef(one_minus_exp_neg(yg, smg), lsg);
             const float slb = Tb * isb * __fdividef(one_minus_exp_neg(yb, smb), lsb);
             const float sw = fmaf(slb, 0.0722f, fmaf(slg, 0.7152f, slr * 0.2126f));
-            Lr += slr;
-            Lg += slg;
-            Lb += slb;
-            tw = fmaf(sw, t, tw);
-            twn += sw;
+            s_acc[0 * stride + slot] += slr;
+            s_acc[1 * stride + slot] += slg;
+            s_acc[2 * stride + slot] += slb;
+            s_acc[3 * stride + slot] = fmaf(sw, t, s_acc[3 * stride + slot]);
+            s_acc[4 * stride + slot] += sw;
             if (u.kahan) {  // T = exp(-sum), the sum compensated (shared memory)
               const float y3[3] = {yr, yg, yb};
               float T3[3];
@@ -828,6 +833,8 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
 
   const float t_lum = fmaf(Tb, 0.0722f, fmaf(Tg, 0.7152f, Tr * 0.2126f));
   const float opacity = 1.0f - t_lum;
+  const float Lr = s_acc[0 * stride + slot], Lg = s_acc[1 * stride + slot], Lb = s_acc[2 * stride + slot];
+  const float tw = s_acc[3 * stride + slot], twn = s_acc[4 * stride + slot];
   float Or = Lr, Og = Lg, Ob = Lb;
   if (opacity > 1e-4f) {
     const float t_cloud = __fdividef(tw, fmaxf(twn, 1e-6f));
