@@ -25,8 +25,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include")]
 CUDA_UNITS = {
     "march.cu": [],
-    "march_fast.cu": ["-prec-div=false", "-prec-sqrt=false"],
-    "march_batch.cu": ["-prec-div=false", "-prec-sqrt=false"],
+    "march_fast.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+    "march_batch.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "march_noalloc.cu": [],
     "grid_march.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "noise_bake.cu": ["-fmad=false"],

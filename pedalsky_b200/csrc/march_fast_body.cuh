@@ -121,7 +121,8 @@ __device__ __forceinline__ float2 h2f(uint32_t w) {
 
 // Exact trilinear tap of the folded base volume (128^3 quads, repeat),
 // coordinates in texel units: one 16-byte quad load per slab, FP32 weights.
-// Returns (R, 0.625G + 0.25B + 0.125A), both in [0, 1].
+// Returns the stored scale (255 R, 2040 (0.625G + 0.25B + 0.125A)); the
+// shape function folds the 1/255 and 1/2040 into its FMAs.
 __device__ __forceinline__ float2 base_quad_tap(const uint4* q, float x, float y, float z) {
   const FloorBits bx = floor_bits(x), by = floor_bits(y), bz = floor_bits(z);
   const float wx = x - bx.f, wy = y - by.f, wz = z - bz.f;
@@ -132,8 +133,7 @@ __device__ __forceinline__ float2 base_quad_tap(const uint4* q, float x, float y
   const float2 tx = make_float2(wx, wx), ty = make_float2(wy, wy);
   const float2 sa = lerp2(lerp2(h2f(a.x), h2f(a.y), tx), lerp2(h2f(a.z), h2f(a.w), tx), ty);
   const float2 sb = lerp2(lerp2(h2f(b.x), h2f(b.y), tx), lerp2(h2f(b.z), h2f(b.w), tx), ty);
-  const float2 v = lerp2(sa, sb, make_float2(wz, wz));
-  return make_float2(v.x * (1.0f / 255.0f), v.y * (1.0f / 2040.0f));
+  return lerp2(sa, sb, make_float2(wz, wz));
 }
 
 // Exact trilinear tap of the folded detail volume (32^3 quads, repeat):
@@ -186,16 +186,23 @@ __device__ __forceinline__ float2 curl_blend(const CurlFetch& c) {
   return make_float2(v.x * (1.0f / 255.0f), v.y * (1.0f / 255.0f));
 }
 
-// Base-noise tap: (R, 0.625G + 0.25B + 0.125A).  LIGHT taps use the texture
-// unit in the HYBRID form.
+// Scale of a base tap's two values: F16 taps return the stored integers
+// (255 R, 2040 fbm), the other forms the values themselves.
+template <int ST>
+struct BaseScale {
+  static constexpr float x = ST == PSC_STORAGE_F16 ? 1.0f / 255.0f : 1.0f;
+  static constexpr float y = ST == PSC_STORAGE_F16 ? 1.0f / 2040.0f : 1.0f;
+};
+
+// Base-noise tap: (R, 0.625G + 0.25B + 0.125A) times BaseScale's inverse.
+// LIGHT taps use the texture unit in the HYBRID form.
 template <int ST, int FILT, bool LIGHT>
 __device__ __forceinline__ float2 base_tap(const MarchUniforms& u, float ax, float ay, float az) {
   constexpr bool kTex = FILT == PSC_FILTER_TEXTURE || (FILT == PSC_FILTER_HYBRID && LIGHT);
   if constexpr (ST == PSC_STORAGE_F16) {
     if constexpr (kTex) {
-      const float2 r = tex3D<float2>(u.tex_base, ax * u.inv_base_scale, ay * u.inv_base_scale,
-                                     az * u.inv_base_scale);
-      return make_float2(r.x * (1.0f / 255.0f), r.y * (1.0f / 2040.0f));
+      return tex3D<float2>(u.tex_base, ax * u.inv_base_scale, ay * u.inv_base_scale,
+                           az * u.inv_base_scale);
     } else {
       const float k = u.base_texel_scale;
       return base_quad_tap(u.base_quad, fmaf(ax, k, -0.5f), fmaf(ay, k, -0.5f), fmaf(az, k, -0.5f));
@@ -270,29 +277,32 @@ __device__ __forceinline__ float ndf_fast(float h, uint32_t t, float anvil_bias)
 
 // Base-shape part shared by the primary and light densities
 // (cloud_march.wgsl:463-494) from a base tap `b` = (R, low-frequency fbm)
-// and the profile value `nd` = ndf(h, type).  The coverage remap
-// remap(cloud, 1 - eff, 1, 0, 1) * eff equals cloud - (1 - eff) wherever the
-// density is not gated off (eff >= 0.01), and 2 - lf >= 1, so neither
-// needs its guard.
-__device__ __forceinline__ float shape_from(float2 b, float lf_bias, float nd, float one_minus_eff) {
-  const float lf = __saturatef(b.y + lf_bias);
-  const float base_cloud = __fdividef(b.x + (1.0f - lf), 2.0f - lf);
+// scaled by 1/(sx, sy) and the profile value `nd` = ndf(h, type).  With
+// c = 1 - lf = clamp01(lf_c - fbm), lf_c = 1 - lf_bias, the remapped base is
+// (R + c) / (1 + c).  The coverage remap remap(cloud, 1 - eff, 1, 0, 1) * eff
+// equals cloud - (1 - eff) wherever the density is not gated off
+// (eff >= 0.01), and 1 + c >= 1, so neither needs its guard.
+template <int ST>
+__device__ __forceinline__ float shape_from(float2 b, float lf_c, float nd, float one_minus_eff) {
+  const float c = __saturatef(fmaf(b.y, -BaseScale<ST>::y, lf_c));
+  const float base_cloud = __fdividef(fmaf(b.x, BaseScale<ST>::x, c), c + 1.0f);
   return fmaf(base_cloud, nd, -one_minus_eff);
 }
 
 // ndf_fast for types 0..6 as two reciprocal smoothsteps with per-type
 // constants: ssr(0, inv_a, h) * g, g = ssr(e1, inv_w1, h) or 1 - that.
 // Chosen once per dense sample, so the light taps carry no switch.
-// b1 = -e1 * inv_w1 (the saturating-FMA form of ssr).  For these types the
-// profile is exactly 0 outside h in [0, 1] (the rising ramp starts at 0 and
-// the second factor reaches 0 at h = 1).
+// b1 = -e1 * inv_w1 (the saturating-FMA form of ssr); the falling form
+// 1 - S(t) is S(1 - t), the ramp with slope -inv_w1 and offset 1 - b1.  For
+// these types the profile is exactly 0 outside h in [0, 1] (the rising ramp
+// starts at 0 and the second factor reaches 0 at h = 1).
 struct NdfCoef {
   float inv_a, b1, inv_w1;
-  bool flip;
 };
 __device__ __forceinline__ NdfCoef ndf_row(float a, float e1, float w1, bool flip) {
   const float inv_w1 = 1.0f / w1;
-  return {1.0f / a, -e1 * inv_w1, inv_w1, flip};
+  const float b1 = -e1 * inv_w1;
+  return flip ? NdfCoef{1.0f / a, 1.0f - b1, -inv_w1} : NdfCoef{1.0f / a, b1, inv_w1};
 }
 __device__ __forceinline__ NdfCoef ndf_coef(uint32_t t) {
   switch (t) {
@@ -303,12 +313,11 @@ __device__ __forceinline__ NdfCoef ndf_coef(uint32_t t) {
     case 4: return ndf_row(0.30f, 0.7f, 0.3f, true);
     case 5: return ndf_row(0.40f, 0.6f, 0.4f, true);
     case 6: return ndf_row(0.50f, 0.8f, 0.2f, true);
-    default: return {0.0f, 0.0f, 0.0f, false};  // unknown types: ndf = 0
+    default: return {0.0f, 0.0f, 0.0f};  // unknown types: ndf = 0
   }
 }
 __device__ __forceinline__ float ndf_eval(const NdfCoef& k, float h) {
-  const float g = ssr_b(k.inv_w1, k.b1, h);
-  return ssr_b(k.inv_a, 0.0f, h) * (k.flip ? 1.0f - g : g);
+  return ssr_b(k.inv_a, 0.0f, h) * ssr_b(k.inv_w1, k.b1, h);
 }
 
 template <int ST, int FILT>
@@ -317,11 +326,10 @@ __device__ __forceinline__ float density_light(const MarchUniforms& u, const Lay
                                                uint32_t type) {
   const float h = (alt - L.base_m) * L.inv_thickness;
   if (h < 0.0f || h > 1.0f) return 0.0f;
-  const float sk = h * L.skew_thickness;
-  const float ax = fmaf(-L.skew_x, sk, qx - L.wind_off_x);
-  const float az = fmaf(-L.skew_z, sk, qz - L.wind_off_z);
+  const float ax = fmaf(-L.skew_kx, h, qx - L.wind_off_x);
+  const float az = fmaf(-L.skew_kz, h, qz - L.wind_off_z);
   const float2 b = base_tap<ST, FILT, true>(u, ax, qy, az);
-  return clamp01(shape_from(b, L.lf_bias, ndf_fast(h, type, L.anvil_bias), 1.0f - eff)) *
+  return clamp01(shape_from<ST>(b, L.lf_c, ndf_fast(h, type, L.anvil_bias), 1.0f - eff)) *
          L.density_scale;
 }
 
@@ -394,12 +402,12 @@ struct NdfCb {
   __device__ __forceinline__ float operator()(float h) const { return ndf_fast(h, 7u, anvil_bias); }
 };
 
-// Base-noise tap of the light march at normalised texture coordinates.
+// Base-noise tap of the light march at normalised texture coordinates
+// (scaled as base_tap's).
 template <int ST>
 __device__ __forceinline__ float2 light_tex_tap(const MarchUniforms& u, float x, float y, float z) {
   if constexpr (ST == PSC_STORAGE_F16) {
-    const float2 r = tex3D<float2>(u.tex_base, x, y, z);
-    return make_float2(r.x * (1.0f / 255.0f), r.y * (1.0f / 2040.0f));
+    return tex3D<float2>(u.tex_base, x, y, z);
   } else {
     const float4 b = tex3D<float4>(u.tex_base, x, y, z);
     return make_float2(b.x, fmaf(b.w, 0.125f, fmaf(b.z, 0.25f, b.y * 0.625f)));
@@ -430,7 +438,7 @@ __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerCo
 #pragma unroll
   for (uint32_t j = 0; j < NB; ++j) {
     const float h = hh[j];
-    float d = __saturatef(shape_from(bt[j], L.lf_bias, prof(h), lr.one_minus_eff));
+    float d = __saturatef(shape_from<ST>(bt[j], L.lf_c, prof(h), lr.one_minus_eff));
     if (HCHECK && !(h >= 0.0f && h <= 1.0f)) d = 0.0f;
     if (u.kahan) {
       const float y = d * ds_step - comp;
@@ -483,15 +491,14 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
     lr.sx = u.sun[0] * k;
     lr.sy = u.sun[1] * k;
     lr.sz = u.sun[2] * k;
-    lr.kx = L.skew_x * L.skew_thickness * k;
-    lr.kz = L.skew_z * L.skew_thickness * k;
+    lr.kx = L.skew_kx * k;
+    lr.kz = L.skew_kz * k;
     lr.step = step;
     lr.one_minus_eff = 1.0f - eff;
     if (type == 7u) return light_march_tex<ST, NdfCb, true>(u, L, lr, NdfCb{L.anvil_bias});
     return light_march_tex<ST, NdfGeneral, false>(
         u, L, lr,
-        NdfGeneral{u.type_grid ? ndf_coef(type)
-                               : NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1, L.ndf_mode == 2u}});
+        NdfGeneral{u.type_grid ? ndf_coef(type) : NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}});
   }
   float od = 0.0f, comp = 0.0f;
   for (uint32_t i = 0; i < u.light_steps; ++i) {
@@ -691,9 +698,8 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
       const float h = (alt - L.base_m) * L.inv_thickness;
       if (h >= 0.0f && h <= 1.0f) {
         const float wsx = px3 - L.wind_off_x, wsz = pz3 - L.wind_off_z;
-        const float sk = h * L.skew_thickness;
-        const float ax = fmaf(-L.skew_x, sk, wsx);
-        const float az = fmaf(-L.skew_z, sk, wsz);
+        const float ax = fmaf(-L.skew_kx, h, wsx);
+        const float az = fmaf(-L.skew_kz, h, wsz);
         // weather, type and base fetches do not depend on each other
         const float wr = weather_fast(u, fmaf(wsx, u.inv_weather_scale, 0.5f),
                                       fmaf(wsz, u.inv_weather_scale, 0.5f));
@@ -703,9 +709,9 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
                                         fmaf(az, u.curl_texel_scale, -0.5f));
         const float eff = clamp01(wr * L.coverage);
         const float nd = (!u.type_grid && L.ndf_mode)
-                             ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1, L.ndf_mode == 2u}, h)
+                             ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}, h)
                              : ndf_fast(h, type, L.anvil_bias);
-        float cloud = shape_from(bs, L.lf_bias, nd, 1.0f - eff);
+        float cloud = shape_from<ST>(bs, L.lf_c, nd, 1.0f - eff);
         if (eff >= 0.01f) {  // coverage gate (cloud_march.wgsl:450-451)
           if (cloud > 0.0f) {  // curl-perturbed detail erosion (:502-527)
             const float2 c2 = curl_blend(cf);

@@ -328,10 +328,17 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
       o.ndf_inv_w1 = 1.0f / kW1[L.cloud_type];
       o.ndf_b1 = -kE1[L.cloud_type] * o.ndf_inv_w1;
       o.ndf_mode = kMode[L.cloud_type];
+      if (o.ndf_mode == 2) {  // 1 - S(t) = S(1 - t)
+        o.ndf_inv_w1 = -o.ndf_inv_w1;
+        o.ndf_b1 = 1.0f - o.ndf_b1;
+      }
     } else {
       o.ndf_inv_a = o.ndf_b1 = o.ndf_inv_w1 = 0.0f;
       o.ndf_mode = 0;
     }
+    o.lf_c = 1.0f - o.lf_bias;
+    o.skew_kx = o.skew_x * o.skew_thickness;
+    o.skew_kz = o.skew_z * o.skew_thickness;
     o.r_bottom = (double)w.planet_radius_m + (double)L.base_m;
     o.r_top = (double)w.planet_radius_m + (double)L.top_m;
   }

@@ -40,12 +40,14 @@ struct LayerConst {
   // Approx-Mie constants (cloud_phase_constants); exact for every layer
   // type except Cumulonimbus, whose diameter depends on height.
   float g_hg, g_d, alpha, w_d, ice;
-  // ndf of types 0..6 as ssr(0, ndf_inv_a, h) * g, g = smoothstep ramp
-  // clamp01(h * ndf_inv_w1 + ndf_b1) or 1 - that (ndf_mode 1 / 2);
-  // ndf_mode 0: evaluate by type
+  // ndf of types 0..6 as ssr(0, ndf_inv_a, h) * g with g the smoothstep of
+  // clamp01(h * ndf_inv_w1 + ndf_b1); a falling second factor 1 - S(t) is
+  // stored as S(1 - t) (negated slope, offset 1 - b), so g needs no flip.
+  // ndf_mode 0: evaluate by type (Cumulonimbus, unknown types)
   float ndf_inv_a, ndf_b1, ndf_inv_w1;
   uint32_t ndf_mode;
-  float _pad[2];
+  float lf_c;              // 1 - lf_bias: 1 - clamp01(fbm + lf_bias) = clamp01(lf_c - fbm)
+  float skew_kx, skew_kz;  // skew_x * skew_thickness, skew_z * skew_thickness
   double r_bottom, r_top;  // planet_radius + base/top, FP64
 };
 
