@@ -377,7 +377,14 @@ __device__ __noinline__ float light_cone(const MarchUniforms& u, const LayerCons
 // is reduced to constants: the distance from the planet centre along the
 // sun ray is r(t)^2 = A + t (B + t) with A = r0^2, B = 2 r0 cos(up, sun),
 // so alt(t) = h0 + t (B + t) / (r0 + r(t)) (the stable form alt_from
-// uses), and the texture coordinates of a tap are affine in t and h.  Taps
+// uses), and the texture coordinates of a tap are affine in t and h.  For
+// light paths up to 20 km (POLY) the normalised height comes instead from
+// the Taylor series of r(t) - r0 in s = t / r0,
+//   t cv + t^2 (1 - cv^2) / (2 r0) - t^3 cv (1 - cv^2) / (2 r0^2) + O(t^4 / (8 r0^3)),
+// cv = cos(up, sun), as a cubic in t: the truncation error is below 1e-4 m at
+// 20 km, smaller than the FP32 rounding of the altitude, and the square root
+// and division per tap are gone.  Longer paths (low sun, thick layers) keep
+// the exact form.  Taps
 // run in batches of 4, then 2, then 1 (no padded slots): every position and
 // fetch of a batch first, then the densities and the optical-depth sum in
 // tap order, plain or compensated as in the one-tap-at-a-time loop.  A tap
@@ -390,6 +397,7 @@ struct LightRay {
   float sx, sy, sz;    // sun direction in texture units per metre
   float kx, kz;        // skew shift in texture units per unit of h
   float step, one_minus_eff;
+  float c0, c1, c2, c3;  // h(t) = c0 + t (c1 + t (c2 + t c3))
 };
 
 // ndf of a non-Cumulonimbus type from its coefficients, and of Cumulonimbus.
@@ -416,7 +424,7 @@ __device__ __forceinline__ float2 light_tex_tap(const MarchUniforms& u, float x,
 
 // HCHECK: zero taps outside the layer's height range (Cumulonimbus; the
 // other profiles are exactly 0 there already).
-template <int ST, class Prof, bool HCHECK, uint32_t NB>
+template <int ST, class Prof, bool HCHECK, uint32_t NB, bool POLY>
 __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerConst& L,
                                            const LightRay& lr, const Prof& prof, uint32_t i0,
                                            float& od, float& comp) {
@@ -426,10 +434,15 @@ __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerCo
 #pragma unroll
   for (uint32_t j = 0; j < NB; ++j) {
     const float t = fmaf((float)j, lr.step, tb);
-    const float bt_t = lr.B + t;
-    const float r = sqrtf(fmaf(t, bt_t, lr.A));
-    const float alt = lr.h0 + __fdividef(t * bt_t, lr.r0 + r);
-    const float h = fmaf(alt, lr.ih, -lr.hb);
+    float h;
+    if constexpr (POLY) {
+      h = fmaf(t, fmaf(t, fmaf(t, lr.c3, lr.c2), lr.c1), lr.c0);
+    } else {
+      const float bt_t = lr.B + t;
+      const float r = sqrtf(fmaf(t, bt_t, lr.A));
+      const float alt = lr.h0 + __fdividef(t * bt_t, lr.r0 + r);
+      h = fmaf(alt, lr.ih, -lr.hb);
+    }
     hh[j] = h;
     bt[j] = light_tex_tap<ST>(u, fmaf(-lr.kx, h, fmaf(lr.sx, t, lr.px)), fmaf(lr.sy, t, lr.py),
                               fmaf(-lr.kz, h, fmaf(lr.sz, t, lr.pz)));
@@ -451,18 +464,18 @@ __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerCo
   }
 }
 
-template <int ST, class Prof, bool HCHECK>
+template <int ST, class Prof, bool HCHECK, bool POLY>
 __device__ __forceinline__ float light_march_tex(const MarchUniforms& u, const LayerConst& L,
                                                  const LightRay& lr, const Prof& prof) {
   const uint32_t n = u.light_steps;
   float od = 0.0f, comp = 0.0f;
   uint32_t i = 0;
-  for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, HCHECK, 4>(u, L, lr, prof, i, od, comp);
+  for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, HCHECK, 4, POLY>(u, L, lr, prof, i, od, comp);
   if (i + 2u <= n) {
-    light_taps<ST, Prof, HCHECK, 2>(u, L, lr, prof, i, od, comp);
+    light_taps<ST, Prof, HCHECK, 2, POLY>(u, L, lr, prof, i, od, comp);
     i += 2u;
   }
-  if (i < n) light_taps<ST, Prof, HCHECK, 1>(u, L, lr, prof, i, od, comp);
+  if (i < n) light_taps<ST, Prof, HCHECK, 1, POLY>(u, L, lr, prof, i, od, comp);
   return od;
 }
 
@@ -495,10 +508,18 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
     lr.kz = L.skew_kz * k;
     lr.step = step;
     lr.one_minus_eff = 1.0f - eff;
-    if (type == 7u) return light_march_tex<ST, NdfCb, true>(u, L, lr, NdfCb{L.anvil_bias});
-    return light_march_tex<ST, NdfGeneral, false>(
-        u, L, lr,
-        NdfGeneral{u.type_grid ? ndf_coef(type) : NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}});
+    const NdfGeneral gen{u.type_grid ? ndf_coef(type) : NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}};
+    if (dist <= 20000.0f) {
+      const float s2 = fmaf(-cv, cv, 1.0f) * __fdividef(0.5f, r0);
+      lr.c0 = fmaf(alt, lr.ih, -lr.hb);
+      lr.c1 = cv * lr.ih;
+      lr.c2 = s2 * lr.ih;
+      lr.c3 = -cv * __fdividef(s2, r0) * lr.ih;
+      if (type == 7u) return light_march_tex<ST, NdfCb, true, true>(u, L, lr, NdfCb{L.anvil_bias});
+      return light_march_tex<ST, NdfGeneral, false, true>(u, L, lr, gen);
+    }
+    if (type == 7u) return light_march_tex<ST, NdfCb, true, false>(u, L, lr, NdfCb{L.anvil_bias});
+    return light_march_tex<ST, NdfGeneral, false, false>(u, L, lr, gen);
   }
   float od = 0.0f, comp = 0.0f;
   for (uint32_t i = 0; i < u.light_steps; ++i) {
