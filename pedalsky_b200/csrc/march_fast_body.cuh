@@ -384,8 +384,8 @@ __device__ __noinline__ float light_cone(const MarchUniforms& u, const LayerCons
 // cv = cos(up, sun), as a cubic in t: the truncation error is below 1e-4 m at
 // 20 km, smaller than the FP32 rounding of the altitude, and the square root
 // and division per tap are gone.  Longer paths (low sun, thick layers) keep
-// the exact form.  Taps
-// run in batches of 4, then 2, then 1 (no padded slots): every position and
+// the exact form.  Six taps (the reference default) run as one batch, other
+// counts in batches of 4, then 2, then 1 (no padded slots): every position and
 // fetch of a batch first, then the densities and the optical-depth sum in
 // tap order, plain or compensated as in the one-tap-at-a-time loop.  A tap
 // outside the layer's height range is fetched but adds zero, as
@@ -470,6 +470,10 @@ __device__ __forceinline__ float light_march_tex(const MarchUniforms& u, const L
   const uint32_t n = u.light_steps;
   float od = 0.0f, comp = 0.0f;
   uint32_t i = 0;
+  if (n == 6u) {  // the reference default: all six fetches in one batch
+    light_taps<ST, Prof, HCHECK, 6, POLY>(u, L, lr, prof, 0u, od, comp);
+    return od;
+  }
   for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, HCHECK, 4, POLY>(u, L, lr, prof, i, od, comp);
   if (i + 2u <= n) {
     light_taps<ST, Prof, HCHECK, 2, POLY>(u, L, lr, prof, i, od, comp);
@@ -749,6 +753,10 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             const float yy = py3 + u.planet_r;
             const float inv_r = __fdividef(1.0f, u.planet_r + alt);
             const float ux = px3 * inv_r, uy = yy * inv_r, uz = pz3 * inv_r;
+            // the two LUT fetches go out before the light march's, so all of
+            // a dense sample's texture fetches are in flight together
+            float3 ts, sky;
+            lut_lookups(u, alt, ux, uy, uz, ts, sky);
             const float od = light_od<ST, FILT>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
             const float st_r = L.sigma_t[0], st_g = L.sigma_t[1], st_b = L.sigma_t[2];
             const float xr = st_r * od, xg = st_g * od, xb = st_b * od;
@@ -800,8 +808,6 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
               sg = fmaf(cf[n], eg[n], sg);
               sb = fmaf(cf[n], eb[n], sb);
             }
-            float3 ts, sky;
-            lut_lookups(u, alt, ux, uy, uz, ts, sky);
             sr *= u.sun_illum[0] * ts.x;
             sg *= u.sun_illum[1] * ts.y;
             sb *= u.sun_illum[2] * ts.z;
