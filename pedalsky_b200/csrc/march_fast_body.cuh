@@ -627,27 +627,6 @@ __device__ __forceinline__ float one_minus_exp_neg(float y, float e) {
                    : 1.0f - e;
 }
 
-// exp(-x b^n) for the octaves n < kMaxOct (zero past the count); with
-// b = 1/2 one exponential at n = 3 and repeated squaring give the others.
-__device__ __forceinline__ void octave_exps(const MarchUniforms& u, float x, int m,
-                                            float (&e)[kMaxOct]) {
-  if (u.b_half) {
-    float v = __expf(x * -0.125f);
-#pragma unroll
-    for (int n = kMaxOct - 1; n >= 0; --n) {
-      e[n] = v;
-      v *= v;
-    }
-  } else {
-#pragma unroll
-    for (int n = 0; n < kMaxOct; ++n) e[n] = n <= m ? __expf(-x * u.bpow[n]) : 0.0f;
-  }
-}
-// Beer-powder mix(b, 2 b (1 - b^2), w) = b (1 + w (1 - 2 b^2))
-__device__ __forceinline__ float beer_powder(float w, float b) {
-  return b * fmaf(w, fmaf(-2.0f * b, b, 1.0f), 1.0f);
-}
-
 // Per-thread shared-memory words of march_pixel_fast beyond the layer
 // intervals, all touched at most once per dense sample and so kept out of
 // the registers the step loop needs: the per-layer octave coefficients,
@@ -780,6 +759,37 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             lut_lookups(u, alt, ux, uy, uz, ts, sky);
             const float od = light_od<ST, FILT>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
             const float st_r = L.sigma_t[0], st_g = L.sigma_t[1], st_b = L.sigma_t[2];
+            const float xr = st_r * od, xg = st_g * od, xb = st_b * od;
+            // e[n] = exp(-x * b^n); with b = 1/2 one exponential at n = 3 and
+            // repeated squaring give every lower octave (octaves past the
+            // count carry zero coefficients).
+            float er[kMaxOct], eg[kMaxOct], eb[kMaxOct];
+            const int m = (int)noct - 1;
+            if (u.b_half) {
+              float vr = __expf(xr * -0.125f), vg = __expf(xg * -0.125f), vb = __expf(xb * -0.125f);
+#pragma unroll
+              for (int n = kMaxOct - 1; n >= 0; --n) {
+                er[n] = vr;
+                eg[n] = vg;
+                eb[n] = vb;
+                vr *= vr;
+                vg *= vg;
+                vb *= vb;
+              }
+            } else {
+#pragma unroll
+              for (int n = 0; n < kMaxOct; ++n) {
+                const bool live = n <= m;
+                er[n] = live ? __expf(-xr * u.bpow[n]) : 0.0f;
+                eg[n] = live ? __expf(-xg * u.bpow[n]) : 0.0f;
+                eb[n] = live ? __expf(-xb * u.bpow[n]) : 0.0f;
+              }
+            }
+            // Beer-powder mix(b, 2 b (1 - b^2), w) = b (1 + w (1 - 2 b^2)), b = e[0]
+            const float br = er[0], bg = eg[0], bb = eb[0];
+            const float enr = br * fmaf(u.powder, fmaf(-2.0f * br, br, 1.0f), 1.0f);
+            const float eng = bg * fmaf(u.powder, fmaf(-2.0f * bg, bg, 1.0f), 1.0f);
+            const float enb = bb * fmaf(u.powder, fmaf(-2.0f * bb, bb, 1.0f), 1.0f);
             float cf[kMaxOct];
             if (cb) {
               const float mt = smoothstepf(0.60f, 0.85f, h);
@@ -791,55 +801,12 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
 #pragma unroll
               for (int n = 0; n < kMaxOct; ++n) cf[n] = s_coef[n * stride + slot];
             }
-            const int m = (int)noct - 1;
-            // Octave sums S_c = sum_n cf[n] exp(-sigma_c od b^n), Beer-powder,
-            // and the step's transmittance exp(-y_c) and (1 - exp(-y_c)) / ls_c
-            // per channel.  A layer without chromatic Mie modulation (droplets
-            // of 20 um and more) has one sigma_t for all channels: one channel
-            // is computed and copied, the same values as three.
-            float sr, sg, sb, enr, eng, enb, yr, yg, yb, smr, smg, smb, fr, fg, fb;
-            if (st_r == st_g && st_g == st_b) {
-              float e[kMaxOct];
-              octave_exps(u, st_r * od, m, e);
-              const float en = beer_powder(u.powder, e[0]);
-              float sum = 0.0f;
+            float sr = 0.0f, sg = 0.0f, sb = 0.0f;
 #pragma unroll
-              for (int n = 0; n < kMaxOct; ++n) sum = fmaf(cf[n], e[n], sum);
-              const float ls = fmaxf(density * st_r, 1e-6f);
-              const float y = ls * step;
-              const float sm = __expf(-y);
-              const float f = __fdividef(one_minus_exp_neg(y, sm), ls);
-              sr = sg = sb = sum;
-              enr = eng = enb = en;
-              yr = yg = yb = y;
-              smr = smg = smb = sm;
-              fr = fg = fb = f;
-            } else {
-              float er[kMaxOct], eg[kMaxOct], eb[kMaxOct];
-              octave_exps(u, st_r * od, m, er);
-              octave_exps(u, st_g * od, m, eg);
-              octave_exps(u, st_b * od, m, eb);
-              enr = beer_powder(u.powder, er[0]);
-              eng = beer_powder(u.powder, eg[0]);
-              enb = beer_powder(u.powder, eb[0]);
-              sr = sg = sb = 0.0f;
-#pragma unroll
-              for (int n = 0; n < kMaxOct; ++n) {
-                sr = fmaf(cf[n], er[n], sr);
-                sg = fmaf(cf[n], eg[n], sg);
-                sb = fmaf(cf[n], eb[n], sb);
-              }
-              const float lsr = fmaxf(density * st_r, 1e-6f), lsg = fmaxf(density * st_g, 1e-6f),
-                          lsb = fmaxf(density * st_b, 1e-6f);
-              yr = lsr * step;
-              yg = lsg * step;
-              yb = lsb * step;
-              smr = __expf(-yr);
-              smg = __expf(-yg);
-              smb = __expf(-yb);
-              fr = __fdividef(one_minus_exp_neg(yr, smr), lsr);
-              fg = __fdividef(one_minus_exp_neg(yg, smg), lsg);
-              fb = __fdividef(one_minus_exp_neg(yb, smb), lsb);
+            for (int n = 0; n < kMaxOct; ++n) {
+              sr = fmaf(cf[n], er[n], sr);
+              sg = fmaf(cf[n], eg[n], sg);
+              sb = fmaf(cf[n], eb[n], sb);
             }
             sr *= u.sun_illum[0] * ts.x;
             sg *= u.sun_illum[1] * ts.y;
@@ -857,9 +824,13 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             const float isr = density * u.sigma_s[0] * fmaf(sr, enr, fmaf(sky.x, ag, lr));
             const float isg = density * u.sigma_s[1] * fmaf(sg, eng, fmaf(sky.y, ag, lg));
             const float isb = density * u.sigma_s[2] * fmaf(sb, enb, fmaf(sky.z, ag, lb));
-            const float slr = Tr * isr * fr;
-            const float slg = Tg * isg * fg;
-            const float slb = Tb * isb * fb;
+            const float lsr = fmaxf(density * st_r, 1e-6f), lsg = fmaxf(density * st_g, 1e-6f),
+                        lsb = fmaxf(density * st_b, 1e-6f);
+            const float yr = lsr * step, yg = lsg * step, yb = lsb * step;
+            const float smr = __expf(-yr), smg = __expf(-yg), smb = __expf(-yb);
+            const float slr = Tr * isr * __fdividef(one_minus_exp_neg(yr, smr), lsr);
+            const float slg = Tg * isg * __fdividef(one_minus_exp_neg(yg, smg), lsg);
+            const float slb = Tb * isb * __fdividef(one_minus_exp_neg(yb, smb), lsb);
             const float sw = fmaf(slb, 0.0722f, fmaf(slg, 0.7152f, slr * 0.2126f));
             s_acc[0 * stride + slot] += slr;
             s_acc[1 * stride + slot] += slg;
