@@ -721,7 +721,19 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
       const float bt = ray_B + t;
       const float alt = ray_h0 + __fdividef(t * bt, ray_r0 + sqrtf(fmaf(t, bt, ray_A)));
       const float h = (alt - L.base_m) * L.inv_thickness;
-      if (h >= 0.0f && h <= 1.0f) {
+      // Profile test before any fetch (no type grid: the profile depends on h
+      // alone).  The base shape is at most 1 and the detail erosion only
+      // lowers it, so the density is at most (nd - (1 - eff)) * density_scale
+      // (up to rounding, which skip_k and the 1.000001 absorb); at or below
+      // the 1e-3 threshold the step adds nothing and its fetches are skipped.
+      bool live = h >= 0.0f && h <= 1.0f;
+      float nd = 0.0f;
+      if (live && !u.type_grid) {
+        nd = L.ndf_mode ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}, h)
+                        : ndf_fast(h, L.cloud_type, L.anvil_bias);
+        live = fmaf(nd, 1.000001f, -L.skip_k) * L.density_scale > 1e-3f;
+      }
+      if (live) {
         const float wsx = px3 - L.wind_off_x, wsz = pz3 - L.wind_off_z;
         const float ax = fmaf(-L.skew_kx, h, wsx);
         const float az = fmaf(-L.skew_kz, h, wsz);
@@ -733,9 +745,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
         const CurlFetch cf = curl_fetch(u.curl_quad, fmaf(ax, u.curl_texel_scale, -0.5f),
                                         fmaf(az, u.curl_texel_scale, -0.5f));
         const float eff = clamp01(wr * L.coverage);
-        const float nd = (!u.type_grid && L.ndf_mode)
-                             ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}, h)
-                             : ndf_fast(h, type, L.anvil_bias);
+        if (u.type_grid) nd = ndf_fast(h, type, L.anvil_bias);
         float cloud = shape_from<ST>(bs, L.lf_c, nd, 1.0f - eff);
         if (eff >= 0.01f) {  // coverage gate (cloud_march.wgsl:450-451)
           if (cloud > 0.0f) {  // curl-perturbed detail erosion (:502-527)

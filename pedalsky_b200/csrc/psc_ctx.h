@@ -38,6 +38,7 @@ struct psc_ctx {
   float4* d_weather_quad = nullptr;  // FAST schedule: 2x2 footprints (power-of-two maps <= 1024^2)
   bool weather_uniform = false;      // every texel holds weather_value
   float weather_value = 0.0f;
+  float weather_min = 0.0f, weather_max = 0.0f;  // extremes of the R channel
   uint8_t* d_type = nullptr;
   uint32_t type_w = 0, type_h = 0;
   std::vector<uint16_t> h_wind;    // 32x16x32 RGBA16F

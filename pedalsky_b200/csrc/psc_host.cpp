@@ -337,6 +337,13 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
       o.ndf_mode = 0;
     }
     o.lf_c = 1.0f - o.lf_bias;
+    {
+      // the largest eff any weather sample can give: bilinear taps stay
+      // within the map's extremes, and eff = clamp01(weather * coverage)
+      const float wext = L.coverage >= 0.0f ? c->weather_max : c->weather_min;
+      const float eff_max = std::fmin(std::fmax(wext * L.coverage, 0.0f), 1.0f);
+      o.skip_k = eff_max < 0.01f ? 4.0f : (1.0f - eff_max) - 1e-6f;
+    }
     o.skew_kx = o.skew_x * o.skew_thickness;
     o.skew_kz = o.skew_z * o.skew_thickness;
     o.r_bottom = (double)w.planet_radius_m + (double)L.base_m;
@@ -1495,6 +1502,9 @@ int psc_upload_weather(psc_ctx* c, const void* texels, uint32_t w, uint32_t h, i
   // skips the tap
   c->weather_uniform = std::all_of(r.begin(), r.end(), [&](float v) { return v == r[0]; });
   c->weather_value = r[0];
+  const auto mm = std::minmax_element(r.begin(), r.end());
+  c->weather_min = *mm.first;
+  c->weather_max = *mm.second;
   const bool pow2 = (w & (w - 1)) == 0 && (h & (h - 1)) == 0;
   if (pow2 && (size_t)w * h <= 1024u * 1024u) {
     // 2x2 bilinear footprints, repeat-wrapped: one 16-byte load per tap

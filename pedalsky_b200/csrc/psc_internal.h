@@ -47,6 +47,11 @@ struct LayerConst {
   float ndf_inv_a, ndf_b1, ndf_inv_w1;
   uint32_t ndf_mode;
   float lf_c;              // 1 - lf_bias: 1 - clamp01(fbm + lf_bias) = clamp01(lf_c - fbm)
+  // Lower bound of 1 - eff over the weather map (eff = clamp01(weather *
+  // coverage)) less 1e-6 for rounding; 4 (above every profile) when eff
+  // never reaches the 0.01 coverage gate.  A primary step whose profile
+  // value nd has (nd - skip_k) * density_scale <= 1e-3 cannot be dense.
+  float skip_k;
   float skew_kx, skew_kz;  // skew_x * skew_thickness, skew_z * skew_thickness
   double r_bottom, r_top;  // planet_radius + base/top, FP64
 };
