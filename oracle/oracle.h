@@ -123,6 +123,13 @@ int oracle_render_pixel(const OracleScene* scene, uint32_t width,
                         int precision, int filter, double* lum4,
                         double* trans4);
 
+/* One FP64 primary density sample at world point p3 / altitude alt in layer
+ * li with weather R value weather_r, and the layer profile ndf(h) there
+ * (test support for the density bound of the GPU march's step skip). */
+int oracle_density_sample(const OracleScene* scene, uint32_t li, const double* p3,
+                          double alt, double weather_r, double* density,
+                          double* profile);
+
 /* ---- voxel-grid form (no reference counterpart; see oracle_grid.cpp) ----
  * Images are width x height = the scene's viewport; bg / target are
  * width*height*4 floats; the loss is sum((L + bg*T - target)^2) / (3*w*h). */

@@ -108,6 +108,26 @@ int oracle_render_pixel(const OracleScene* s, uint32_t w, uint32_t h, uint32_t x
   return 0;
 }
 
+// Test support: one primary density sample (sample_density,
+// cloud_march.wgsl:432-530) in FP64 at world point p3 and altitude `alt`, in
+// layer `li`, with weather R channel `weather_r`; also the layer's profile
+// ndf(h) (cloud_density_common.wgsl:49-91) there.  The tests use it to check
+// density <= max(ndf(h) - (1 - eff), 0) * density_scale, the bound the GPU
+// march relies on to skip the fetches of steps that cannot be dense.
+int oracle_density_sample(const OracleScene* s, uint32_t li, const double* p3, double alt,
+                          double weather_r, double* density, double* profile) {
+  if (!scene_ok(s) || li >= 8 || !p3 || !density || !profile) return -1;
+  March<double> m;
+  m.init(s, 0);
+  const Layer<double>& L = m.layers[li];
+  const WindCache<double> w = m.wind_cache(L);
+  const uint32_t type = m.effective_type(p3[0], p3[2], L);
+  *density = m.sample_density(mk<double>(p3[0], p3[1], p3[2]), alt, L, weather_r, w, type);
+  const double h = (alt - L.base) / std::fmax(L.top - L.base, 1.0);
+  *profile = m.ndf(h, type, L.anvil_bias);
+  return 0;
+}
+
 int oracle_composite(const float* lum, const float* tr, float* hdr, uint32_t n) {
   if (!lum || !tr || !hdr) return -1;
   for (size_t i = 0; i < (size_t)n * 4; ++i) hdr[i] = lum[i] + hdr[i] * tr[i];

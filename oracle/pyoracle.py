@@ -75,6 +75,7 @@ def lib() -> C.CDLL:
             ("oracle_render", [vp, u32, u32, C.c_int, C.c_int, C.c_int, u32, u32, vp, vp, vp], C.c_int),
             ("oracle_render_pixel", [vp, u32, u32, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
             ("oracle_composite", [vp, vp, vp, u32], C.c_int),
+            ("oracle_density_sample", [vp, u32, vp, C.c_double, C.c_double, vp, vp], C.c_int),
             ("oracle_grid_render", [vp, vp, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
             ("oracle_grid_loss", [vp, vp, u32, u32, vp, vp, vp, u32, C.c_int, vp], C.c_int),
             ("oracle_grid_adjoint", [vp, vp, u32, u32, vp, vp, u32, u32, C.c_int, vp, vp, vp],
@@ -173,6 +174,18 @@ def render(scene, noise, luts, precision=FP64, filt=FILTER_EXACT, threads=0, row
     if counters:
         return L, T, dict(zip(COUNTERS, (int(c) for c in cnt)))
     return L, T
+
+
+def density_sample(scene, noise, luts, layer, p3, alt, weather_r):
+    """FP64 primary density at world point p3 (altitude alt) in `layer` with
+    weather R value `weather_r`, and the layer profile ndf(h) there."""
+    s, keep = make_scene(scene, noise, luts)
+    p = np.ascontiguousarray(p3, np.float64)
+    d, prof = C.c_double(), C.c_double()
+    _ok(lib().oracle_density_sample(C.byref(s), layer, _p(p), float(alt), float(weather_r),
+                                    C.byref(d), C.byref(prof)), "oracle_density_sample")
+    del keep
+    return d.value, prof.value
 
 
 def composite(L, T, bg):
