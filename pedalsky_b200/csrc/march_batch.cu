@@ -23,8 +23,12 @@ __device__ __forceinline__ void unpack_tile(uint32_t w, uint32_t& view, uint32_t
   ty = w & 0xfffu;
 }
 
+// 768 threads per SM (6 CTAs of 128): the shared-memory uniform block turns
+// every uniform operand into a register, and 80 registers per thread remove
+// nearly all spills (measured: 8 CTAs/SM 5.80 ms, 7 5.50, 6 5.35 on a 1080p
+// view; 64 uneven views 224.9 -> 209.4 ms).
 template <int ST, int FILT, int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT)
+__global__ void __launch_bounds__(NT, 768 / NT)
     k_march_batch(const MarchUniforms* __restrict__ views_u, const ViewDev* __restrict__ views_v,
                   const uint32_t* __restrict__ tiles, uint32_t n_tiles, uint32_t* __restrict__ counter,
                   uint32_t tile_w) {
