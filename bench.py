@@ -388,7 +388,9 @@ def run_ours(args):
     if not args.no_plain_reference and schedule == capi.SCHED_FAST:
         from pedalsky_b200 import batch as B
         bt = B.Batch(frames, dev)
-        B.set_tuning(sub.handle, 128, 16, use_graph=1)
+        with torch.cuda.stream(stream):
+            btune = B.autotune(sub.handle, bt, reps=1, stream=stream)
+        B.set_tuning(sub.handle, btune["threads"], btune["tile_w"], use_graph=1)
         with torch.cuda.stream(stream):
             for _ in range(args.warmup):
                 bt.reset_hdr()
@@ -411,7 +413,7 @@ def run_ours(args):
             ms_b = float(tb.item())
         batched = {"value": world * rays_step / (ms_b * 1e-3) / 1e6, "ms_per_step": ms_b,
                    "config": "psc_render_batch: persistent kernel from a captured CUDA graph, "
-                             "per-view LUT bakes included"}
+                             "per-view LUT bakes included", "autotuned": btune}
         del bt
 
     # end to end through the C ABI with host buffers: pinned H2D of the
