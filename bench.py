@@ -466,6 +466,10 @@ def run_ours(args):
                             "are served by L1/TEX and L2, not HBM (DRAM traffic per launch is "
                             "`traffic`); `fetch` relates them to the on-chip ceilings measured on "
                             "this GPU"}
+            if peaks_fetch and batched:
+                b_ach = bpr["bytes_per_ray"] * rays_step / (batched["ms_per_step"] * 1e-3) / 1e9
+                batched["fetch_gbs"] = b_ach
+                batched["frac_of_l2_read"] = b_ach / peaks_fetch["l2_read_gbs"]
             if peaks_fetch:
                 light_rate = bpr["light_fetches_per_ray"] * rays_step / (ms_max * 1e-3) / 1e9
                 roof["fetch"] = {
