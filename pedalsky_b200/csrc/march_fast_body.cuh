@@ -35,7 +35,10 @@
 //     LUTs go through the texture unit, as the reference's linear sampler
 //     does; EXACT keeps FP32 weights for them.
 // Octave counts up to 4 are handled here; the host falls back to the plain
-// kernel beyond that.
+// kernel beyond that.  CB = false compiles out the Cumulonimbus paths (the
+// height-dependent phase of the octaves, the anvil profile of the light
+// march); the host uses that form when no layer is of type 7 and there is no
+// cloud-type grid (needs_cb_paths): the hot loop is then shorter.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -484,7 +487,7 @@ __device__ __forceinline__ float light_march_tex(const MarchUniforms& u, const L
 }
 
 // Optical depth toward the sun (cloud_march.wgsl:543-578).
-template <int ST, int FILT>
+template <int ST, int FILT, bool CB = true>
 __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerConst& L, float px,
                                           float py, float pz, float alt, float eff, uint32_t type,
                                           float ux, float uy, float uz) {
@@ -519,10 +522,10 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
       lr.c1 = cv * lr.ih;
       lr.c2 = s2 * lr.ih;
       lr.c3 = -cv * __fdividef(s2, r0) * lr.ih;
-      if (type == 7u) return light_march_tex<ST, NdfCb, true, true>(u, L, lr, NdfCb{L.anvil_bias});
+      if (CB && type == 7u) return light_march_tex<ST, NdfCb, true, true>(u, L, lr, NdfCb{L.anvil_bias});
       return light_march_tex<ST, NdfGeneral, false, true>(u, L, lr, gen);
     }
-    if (type == 7u) return light_march_tex<ST, NdfCb, true, false>(u, L, lr, NdfCb{L.anvil_bias});
+    if (CB && type == 7u) return light_march_tex<ST, NdfCb, true, false>(u, L, lr, NdfCb{L.anvil_bias});
     return light_march_tex<ST, NdfGeneral, false, false>(u, L, lr, gen);
   }
   float od = 0.0f, comp = 0.0f;
@@ -638,7 +641,7 @@ constexpr uint32_t kAuxWords = kMaxOct + 6 + 5;
 // arrays of per-layer entry/exit distances, laid out [layer][slot] with
 // `stride` slots; `slot` is this thread's column.  `s_aux` holds kAuxWords
 // words per thread, laid out the same way.
-template <int ST, int FILT>
+template <int ST, int FILT, bool CB = true>
 __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const ViewDev& v, uint32_t px,
                                                  uint32_t py, float* s_t0, float* s_t1, float* s_aux,
                                                  uint32_t stride, uint32_t slot) {
@@ -695,7 +698,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
     const float segment = t1 - t0;
     if (segment <= 0.0f) continue;
     const float step = __fdividef(segment, (float)u.cloud_steps);
-    const bool cb = L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE;
+    const bool cb = CB && L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE;
 
     // per ray and layer: a^n * phase_n * forward gain (shared memory)
     if (u.phase_mode == PSC_PHASE_DUAL_LOBE_HG) {
@@ -767,7 +770,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             // a dense sample's texture fetches are in flight together
             float3 ts, sky;
             lut_lookups(u, alt, ux, uy, uz, ts, sky);
-            const float od = light_od<ST, FILT>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
+            const float od = light_od<ST, FILT, CB>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
             const float st_r = L.sigma_t[0], st_g = L.sigma_t[1], st_b = L.sigma_t[2];
             const float xr = st_r * od, xg = st_g * od, xb = st_b * od;
             // e[n] = exp(-x * b^n); with b = 1/2 one exponential at n = 3 and
