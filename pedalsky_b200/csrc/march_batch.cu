@@ -27,7 +27,7 @@ __device__ __forceinline__ void unpack_tile(uint32_t w, uint32_t& view, uint32_t
 // every uniform operand into a register, and 80 registers per thread remove
 // nearly all spills (measured: 8 CTAs/SM 5.80 ms, 7 5.50, 6 5.35 on a 1080p
 // view; 64 uneven views 224.9 -> 209.4 ms).
-template <int ST, int FILT, int NT, bool CB>
+template <int ST, int FILT, int NT, bool FULL>
 __global__ void __launch_bounds__(NT, 768 / NT)
     k_march_batch(const MarchUniforms* __restrict__ views_u, const ViewDev* __restrict__ views_v,
                   const uint32_t* __restrict__ tiles, uint32_t n_tiles, uint32_t* __restrict__ counter,
@@ -58,40 +58,40 @@ __global__ void __launch_bounds__(NT, 768 / NT)
     const uint32_t px = tx * tile_w + (warp % warps_x) * 8u + (lane & 7u);
     const uint32_t py = ty * tile_h + (warp / warps_x) * 4u + (lane >> 3);
     if (px < sv.width && py < sv.height)
-      march_pixel_fast<ST, FILT, CB>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
+      march_pixel_fast<ST, FILT, FULL>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
     __syncthreads();  // su, sv and s_tile are rewritten by the next iteration
   }
 }
 
-template <int ST, int FILT, int NT, bool CB>
-int launch_batch_cb(const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles, uint32_t n_tiles,
+template <int ST, int FILT, int NT, bool FULL>
+int launch_batch_full(const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles, uint32_t n_tiles,
                     uint32_t* counter, uint32_t tile_w, int sms, cudaStream_t s) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march_batch<ST, FILT, NT, CB>, NT, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march_batch<ST, FILT, NT, FULL>, NT, 0) !=
       cudaSuccess)
     return PSC_ERR_CUDA;
   per_sm = per_sm < 1 ? 1 : per_sm;
   uint32_t grid = (uint32_t)(sms * per_sm);
   if (grid > n_tiles) grid = n_tiles ? n_tiles : 1;
-  k_march_batch<ST, FILT, NT, CB><<<grid, NT, 0, s>>>(u, v, tiles, n_tiles, counter, tile_w);
+  k_march_batch<ST, FILT, NT, FULL><<<grid, NT, 0, s>>>(u, v, tiles, n_tiles, counter, tile_w);
   return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
 }
 
 template <int ST, int FILT, int NT>
 int launch_batch_t(const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles, uint32_t n_tiles,
-                   uint32_t* counter, uint32_t tile_w, int sms, bool cb, cudaStream_t s) {
-  return cb ? launch_batch_cb<ST, FILT, NT, true>(u, v, tiles, n_tiles, counter, tile_w, sms, s)
-            : launch_batch_cb<ST, FILT, NT, false>(u, v, tiles, n_tiles, counter, tile_w, sms, s);
+                   uint32_t* counter, uint32_t tile_w, int sms, bool full, cudaStream_t s) {
+  return full ? launch_batch_full<ST, FILT, NT, true>(u, v, tiles, n_tiles, counter, tile_w, sms, s)
+            : launch_batch_full<ST, FILT, NT, false>(u, v, tiles, n_tiles, counter, tile_w, sms, s);
 }
 
 template <int ST, int FILT>
 int launch_batch_nt(int nt, const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles,
-                    uint32_t n_tiles, uint32_t* counter, uint32_t tile_w, int sms, bool cb,
+                    uint32_t n_tiles, uint32_t* counter, uint32_t tile_w, int sms, bool full,
                     cudaStream_t s) {
   switch (nt) {
-    case 64: return launch_batch_t<ST, FILT, 64>(u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
-    case 128: return launch_batch_t<ST, FILT, 128>(u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
-    case 256: return launch_batch_t<ST, FILT, 256>(u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
+    case 64: return launch_batch_t<ST, FILT, 64>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
+    case 128: return launch_batch_t<ST, FILT, 128>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
+    case 256: return launch_batch_t<ST, FILT, 256>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
     default: return PSC_ERR_INVALID_ARGUMENT;
   }
 }
@@ -100,22 +100,22 @@ int launch_batch_nt(int nt, const MarchUniforms* u, const ViewDev* v, const uint
 
 int launch_march_batch(const PscMarchOptions& o, int threads, uint32_t tile_w,
                        const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles,
-                       uint32_t n_tiles, uint32_t* counter, int sms, bool cb, cudaStream_t s) {
+                       uint32_t n_tiles, uint32_t* counter, int sms, bool full, cudaStream_t s) {
   if (o.filter == PSC_FILTER_HYBRID) {
     if (o.storage == PSC_STORAGE_F16)
-      return launch_batch_nt<PSC_STORAGE_F16, PSC_FILTER_HYBRID>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
+      return launch_batch_nt<PSC_STORAGE_F16, PSC_FILTER_HYBRID>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
     if (o.storage == PSC_STORAGE_U8)
-      return launch_batch_nt<PSC_STORAGE_U8, PSC_FILTER_HYBRID>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
+      return launch_batch_nt<PSC_STORAGE_U8, PSC_FILTER_HYBRID>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
   } else if (o.filter == PSC_FILTER_EXACT) {
     if (o.storage == PSC_STORAGE_F16)
-      return launch_batch_nt<PSC_STORAGE_F16, PSC_FILTER_EXACT>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
+      return launch_batch_nt<PSC_STORAGE_F16, PSC_FILTER_EXACT>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
     if (o.storage == PSC_STORAGE_U8)
-      return launch_batch_nt<PSC_STORAGE_U8, PSC_FILTER_EXACT>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
+      return launch_batch_nt<PSC_STORAGE_U8, PSC_FILTER_EXACT>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
     if (o.storage == PSC_STORAGE_F32)
-      return launch_batch_nt<PSC_STORAGE_F32, PSC_FILTER_EXACT>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
+      return launch_batch_nt<PSC_STORAGE_F32, PSC_FILTER_EXACT>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
   } else if (o.filter == PSC_FILTER_TEXTURE) {
     if (o.storage == PSC_STORAGE_U8)
-      return launch_batch_nt<PSC_STORAGE_U8, PSC_FILTER_TEXTURE>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, cb, s);
+      return launch_batch_nt<PSC_STORAGE_U8, PSC_FILTER_TEXTURE>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
   }
   return PSC_ERR_UNSUPPORTED;
 }

@@ -16,7 +16,7 @@ constexpr int kThreads = 128;
 
 // Shared memory per CTA: the entry/exit distances of each of the view's
 // layers and kAuxWords more words, per thread (dynamic, sized at launch).
-template <int ST, int FILT, bool CB>
+template <int ST, int FILT, bool FULL>
 __global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constant__ MarchUniforms u,
                                                             const __grid_constant__ ViewDev v) {
   extern __shared__ float s_dyn[];
@@ -28,14 +28,14 @@ __global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constan
   const uint32_t px = blockIdx.x * kTileW + (warp & 1u) * 8u + (lane & 7u);
   const uint32_t py = blockIdx.y * kTileH + (warp >> 1) * 4u + (lane >> 3);
   if (px >= v.width || py >= v.height) return;
-  march_pixel_fast<ST, FILT, CB>(u, v, px, py, s_t0, s_t1, s_aux, kThreads, threadIdx.x);
+  march_pixel_fast<ST, FILT, FULL>(u, v, px, py, s_t0, s_t1, s_aux, kThreads, threadIdx.x);
 }
 
 template <int ST, int FILT>
 cudaError_t launch_fast(const MarchUniforms& u, const ViewDev& v, cudaStream_t s) {
   const dim3 grid((v.width + kTileW - 1) / kTileW, (v.height + kTileH - 1) / kTileH);
   const size_t smem = (2u * u.layer_count + kAuxWords) * kThreads * sizeof(float);
-  if (needs_cb_paths(&u, 1))
+  if (needs_full_paths(&u, 1))
     k_march_fast<ST, FILT, true><<<grid, kThreads, smem, s>>>(u, v);
   else
     k_march_fast<ST, FILT, false><<<grid, kThreads, smem, s>>>(u, v);

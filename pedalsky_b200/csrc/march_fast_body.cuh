@@ -35,10 +35,12 @@
 //     LUTs go through the texture unit, as the reference's linear sampler
 //     does; EXACT keeps FP32 weights for them.
 // Octave counts up to 4 are handled here; the host falls back to the plain
-// kernel beyond that.  CB = false compiles out the Cumulonimbus paths (the
-// height-dependent phase of the octaves, the anvil profile of the light
-// march); the host uses that form when no layer is of type 7 and there is no
-// cloud-type grid (needs_cb_paths): the hot loop is then shorter.
+// kernel beyond that.  FULL = false (the lean form) compiles out the paths a
+// common scene does not use: Cumulonimbus (the height-dependent phase of the
+// octaves, the anvil profile of the light march), the cloud-type grid, Kahan
+// sums, cone light sampling and lightning.  The host picks the lean form
+// when none of them is in use (needs_full_paths): the hot loop is shorter and
+// spills less.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -427,7 +429,7 @@ __device__ __forceinline__ float2 light_tex_tap(const MarchUniforms& u, float x,
 
 // HCHECK: zero taps outside the layer's height range (Cumulonimbus; the
 // other profiles are exactly 0 there already).
-template <int ST, class Prof, bool HCHECK, uint32_t NB, bool POLY>
+template <int ST, class Prof, bool HCHECK, uint32_t NB, bool POLY, bool FULL>
 __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerConst& L,
                                            const LightRay& lr, const Prof& prof, uint32_t i0,
                                            float& od, float& comp) {
@@ -456,7 +458,7 @@ __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerCo
     const float h = hh[j];
     float d = __saturatef(shape_from<ST>(bt[j], L.lf_c, prof(h), lr.one_minus_eff));
     if (HCHECK && !(h >= 0.0f && h <= 1.0f)) d = 0.0f;
-    if (u.kahan) {
+    if (FULL && u.kahan) {
       const float y = d * ds_step - comp;
       const float tt = od + y;
       comp = (tt - od) - y;
@@ -467,34 +469,34 @@ __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerCo
   }
 }
 
-template <int ST, class Prof, bool HCHECK, bool POLY>
+template <int ST, class Prof, bool HCHECK, bool POLY, bool FULL>
 __device__ __forceinline__ float light_march_tex(const MarchUniforms& u, const LayerConst& L,
                                                  const LightRay& lr, const Prof& prof) {
   const uint32_t n = u.light_steps;
   float od = 0.0f, comp = 0.0f;
   uint32_t i = 0;
   if (n == 6u) {  // the reference default: all six fetches in one batch
-    light_taps<ST, Prof, HCHECK, 6, POLY>(u, L, lr, prof, 0u, od, comp);
+    light_taps<ST, Prof, HCHECK, 6, POLY, FULL>(u, L, lr, prof, 0u, od, comp);
     return od;
   }
-  for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, HCHECK, 4, POLY>(u, L, lr, prof, i, od, comp);
+  for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, HCHECK, 4, POLY, FULL>(u, L, lr, prof, i, od, comp);
   if (i + 2u <= n) {
-    light_taps<ST, Prof, HCHECK, 2, POLY>(u, L, lr, prof, i, od, comp);
+    light_taps<ST, Prof, HCHECK, 2, POLY, FULL>(u, L, lr, prof, i, od, comp);
     i += 2u;
   }
-  if (i < n) light_taps<ST, Prof, HCHECK, 1, POLY>(u, L, lr, prof, i, od, comp);
+  if (i < n) light_taps<ST, Prof, HCHECK, 1, POLY, FULL>(u, L, lr, prof, i, od, comp);
   return od;
 }
 
 // Optical depth toward the sun (cloud_march.wgsl:543-578).
-template <int ST, int FILT, bool CB = true>
+template <int ST, int FILT, bool FULL = true>
 __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerConst& L, float px,
                                           float py, float pz, float alt, float eff, uint32_t type,
                                           float ux, float uy, float uz) {
   const float r0 = u.planet_r + alt;
   const float cv = fmaf(ux, u.sun[0], fmaf(uy, u.sun[1], uz * u.sun[2]));
   const float dist = fmaxf((L.top_m - alt) * u.inv_cos_sun, 1.0f);
-  if (u.cone) return light_cone<ST, FILT>(u, L, px, py, pz, alt, eff, type, r0, cv, dist);
+  if (FULL && u.cone) return light_cone<ST, FILT>(u, L, px, py, pz, alt, eff, type, r0, cv, dist);
   const float step = __fdividef(dist, (float)u.light_steps);
   if constexpr (FILT != PSC_FILTER_EXACT) {
     const float k = u.inv_base_scale;
@@ -515,18 +517,18 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
     lr.kz = L.skew_kz * k;
     lr.step = step;
     lr.one_minus_eff = 1.0f - eff;
-    const NdfGeneral gen{u.type_grid ? ndf_coef(type) : NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}};
+    const NdfGeneral gen{(FULL && u.type_grid) ? ndf_coef(type) : NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}};
     if (dist <= 20000.0f) {
       const float s2 = fmaf(-cv, cv, 1.0f) * __fdividef(0.5f, r0);
       lr.c0 = fmaf(alt, lr.ih, -lr.hb);
       lr.c1 = cv * lr.ih;
       lr.c2 = s2 * lr.ih;
       lr.c3 = -cv * __fdividef(s2, r0) * lr.ih;
-      if (CB && type == 7u) return light_march_tex<ST, NdfCb, true, true>(u, L, lr, NdfCb{L.anvil_bias});
-      return light_march_tex<ST, NdfGeneral, false, true>(u, L, lr, gen);
+      if (FULL && type == 7u) return light_march_tex<ST, NdfCb, true, true, FULL>(u, L, lr, NdfCb{L.anvil_bias});
+      return light_march_tex<ST, NdfGeneral, false, true, FULL>(u, L, lr, gen);
     }
-    if (CB && type == 7u) return light_march_tex<ST, NdfCb, true, false>(u, L, lr, NdfCb{L.anvil_bias});
-    return light_march_tex<ST, NdfGeneral, false, false>(u, L, lr, gen);
+    if (FULL && type == 7u) return light_march_tex<ST, NdfCb, true, false, FULL>(u, L, lr, NdfCb{L.anvil_bias});
+    return light_march_tex<ST, NdfGeneral, false, false, FULL>(u, L, lr, gen);
   }
   float od = 0.0f, comp = 0.0f;
   for (uint32_t i = 0; i < u.light_steps; ++i) {
@@ -535,7 +537,7 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
     const float term =
         density_light<ST, FILT>(u, L, qx, qy, qz, alt_from(u, qx, qy, qz, r0, cv, alt, t), eff, type) *
         step;
-    if (u.kahan) {
+    if (FULL && u.kahan) {
       const float y = term - comp;
       const float tt = od + y;
       comp = (tt - od) - y;
@@ -641,7 +643,7 @@ constexpr uint32_t kAuxWords = kMaxOct + 6 + 5;
 // arrays of per-layer entry/exit distances, laid out [layer][slot] with
 // `stride` slots; `slot` is this thread's column.  `s_aux` holds kAuxWords
 // words per thread, laid out the same way.
-template <int ST, int FILT, bool CB = true>
+template <int ST, int FILT, bool FULL = true>
 __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const ViewDev& v, uint32_t px,
                                                  uint32_t py, float* s_t0, float* s_t1, float* s_aux,
                                                  uint32_t stride, uint32_t slot) {
@@ -679,7 +681,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
   float* const s_coef = s_aux;                      // [kMaxOct][stride]
   float* const s_kahan = s_aux + kMaxOct * stride;  // od r,g,b then comp r,g,b
   float* const s_acc = s_kahan + 6 * stride;        // L r,g,b, sum(w t), sum(w)
-  if (u.kahan) {
+  if (FULL && u.kahan) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) s_kahan[c * stride + slot] = 0.0f;
   }
@@ -698,7 +700,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
     const float segment = t1 - t0;
     if (segment <= 0.0f) continue;
     const float step = __fdividef(segment, (float)u.cloud_steps);
-    const bool cb = CB && L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE;
+    const bool cb = FULL && L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE;
 
     // per ray and layer: a^n * phase_n * forward gain (shared memory)
     if (u.phase_mode == PSC_PHASE_DUAL_LOBE_HG) {
@@ -731,7 +733,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
       // the 1e-3 threshold the step adds nothing and its fetches are skipped.
       bool live = h >= 0.0f && h <= 1.0f;
       float nd = 0.0f;
-      if (live && !u.type_grid) {
+      if (live && !(FULL && u.type_grid)) {
         nd = L.ndf_mode ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}, h)
                         : ndf_fast(h, L.cloud_type, L.anvil_bias);
         live = fmaf(nd, 1.000001f, -L.skip_k) * L.density_scale > 1e-3f;
@@ -743,12 +745,12 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
         // weather, type and base fetches do not depend on each other
         const float wr = weather_fast(u, fmaf(wsx, u.inv_weather_scale, 0.5f),
                                       fmaf(wsz, u.inv_weather_scale, 0.5f));
-        const uint32_t type = effective_type(u, wsx, wsz, L.cloud_type);
+        const uint32_t type = FULL ? effective_type(u, wsx, wsz, L.cloud_type) : L.cloud_type;
         const float2 bs = base_tap<ST, FILT, false>(u, ax, py3, az);
         const CurlFetch cf = curl_fetch(u.curl_quad, fmaf(ax, u.curl_texel_scale, -0.5f),
                                         fmaf(az, u.curl_texel_scale, -0.5f));
         const float eff = clamp01(wr * L.coverage);
-        if (u.type_grid) nd = ndf_fast(h, type, L.anvil_bias);
+        if (FULL && u.type_grid) nd = ndf_fast(h, type, L.anvil_bias);
         float cloud = shape_from<ST>(bs, L.lf_c, nd, 1.0f - eff);
         if (eff >= 0.01f) {  // coverage gate (cloud_march.wgsl:450-451)
           if (cloud > 0.0f) {  // curl-perturbed detail erosion (:502-527)
@@ -770,7 +772,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             // a dense sample's texture fetches are in flight together
             float3 ts, sky;
             lut_lookups(u, alt, ux, uy, uz, ts, sky);
-            const float od = light_od<ST, FILT, CB>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
+            const float od = light_od<ST, FILT, FULL>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
             const float st_r = L.sigma_t[0], st_g = L.sigma_t[1], st_b = L.sigma_t[2];
             const float xr = st_r * od, xg = st_g * od, xb = st_b * od;
             // e[n] = exp(-x * b^n); with b = 1/2 one exponential at n = 3 and
@@ -826,7 +828,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             sb *= u.sun_illum[2] * ts.z;
             const float ag = mixf(0.3f, 1.0f, clamp01(h)) * u.ambient;
             float lr = 0.0f, lg = 0.0f, lb = 0.0f;
-            if (u.lightning_radius > 0.0f) {
+            if (FULL && u.lightning_radius > 0.0f) {
               const float ddx = px3 - u.lightning_origin_x, ddz = pz3 - u.lightning_origin_z;
               const float fo = clamp01(1.0f - sqrtf(ddx * ddx + ddz * ddz) / u.lightning_radius);
               const float wgt = fo * fo * (3.0f - 2.0f * fo);
@@ -850,7 +852,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             s_acc[2 * stride + slot] += slb;
             s_acc[3 * stride + slot] = fmaf(sw, t, s_acc[3 * stride + slot]);
             s_acc[4 * stride + slot] += sw;
-            if (u.kahan) {  // T = exp(-sum), the sum compensated (shared memory)
+            if (FULL && u.kahan) {  // T = exp(-sum), the sum compensated (shared memory)
               const float y3[3] = {yr, yg, yb};
               float T3[3];
 #pragma unroll

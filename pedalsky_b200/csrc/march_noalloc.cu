@@ -151,7 +151,7 @@ extern "C" int psc_render_batch_noalloc(psc_ctx* c, const PscBatchView* views, u
   const cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return psc::host::cuda_fail(e, "batch counter reset");
   rc = psc::launch_march_batch(c->opts, (int)c->batch_tuning.threads, c->batch_tuning.tile_w, d_u, d_v,
-                               d_tiles, n_tiles, d_counter, c->sms, psc::needs_cb_paths(g_host.u, n), s);
+                               d_tiles, n_tiles, d_counter, c->sms, psc::needs_full_paths(g_host.u, n), s);
   if (rc == PSC_ERR_UNSUPPORTED)
     return fail(rc, "batched march supports F16/U8/F32 exact, F16/U8 hybrid and U8 texture storage");
   if (rc) return fail(rc, "batched march launch failed: %s", cudaGetErrorString(cudaGetLastError()));

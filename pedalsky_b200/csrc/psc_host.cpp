@@ -629,7 +629,7 @@ int enqueue_batch(psc_ctx* c, uint32_t n, uint32_t n_tiles, cudaStream_t s, bool
   PSC_CUDA(cudaMemsetAsync(c->d_bcounter, 0, sizeof(uint32_t), s), "batch counter reset");
   const int rc = psc::launch_march_batch(c->opts, (int)c->batch_tuning.threads, c->batch_tuning.tile_w,
                                          c->d_bu, c->d_bv, c->d_btiles, n_tiles, c->d_bcounter, c->sms,
-                                         psc::needs_cb_paths(c->h_bu, n), s);
+                                         psc::needs_full_paths(c->h_bu, n), s);
   if (rc == PSC_ERR_UNSUPPORTED)
     return fail(rc, "batched march supports F16/U8/F32 exact, F16/U8 hybrid and U8 texture storage");
   if (rc) return fail(rc, "batched march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1782,14 +1782,14 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
     return PSC_OK;
   }
   // Graph path: the key is everything the captured nodes bake in (buffer
-  // pointers, sizes, options, launch shape, the kernel form with or without
-  // Cumulonimbus paths); uniforms are read from the pinned staging at launch
+  // pointers, sizes, options, launch shape, the full or lean kernel form);
+  // uniforms are read from the pinned staging at launch
   // time and may change freely within that form.
   std::vector<uint64_t> key = {n, n_tiles, c->batch_tuning.threads, c->batch_tuning.tile_w,
                                c->opts.storage, c->opts.filter, c->opts.composite,
                                (uint64_t)(uintptr_t)c->d_bu, (uint64_t)(uintptr_t)c->d_btiles,
                                (uint64_t)(uintptr_t)c->d_base_store, (uint64_t)c->tex_base,
-                               (uint64_t)psc::needs_cb_paths(c->h_bu, n)};
+                               (uint64_t)psc::needs_full_paths(c->h_bu, n)};
   if (!c->batch_exec || key != c->batch_key) {
     if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
     c->batch_exec = nullptr;

@@ -195,21 +195,22 @@ int launch_composite(const float4* l, const float4* t, float4* hdr, uint32_t n,
                      cudaStream_t stream);
 // Noise bakes (noise_bake.cu), synchronous on `stream`.
 int launch_noise_bakes(uint8_t* base, uint8_t* detail, uint8_t* curl, cudaStream_t stream);
-// True when a march over these n uniform blocks can meet a Cumulonimbus
-// profile: a layer of type 7, or a cloud-type grid (its cells may hold any
-// type).  The FAST kernels come with and without their Cumulonimbus paths.
-inline bool needs_cb_paths(const MarchUniforms* u, uint32_t n) {
+// True when a march over these n uniform blocks needs the FAST kernels' full
+// form: a layer of type 7 (Cumulonimbus), a cloud-type grid (its cells may
+// hold any type), Kahan sums, cone light sampling or lightning.  Otherwise
+// the lean form, built without those paths, computes the same values.
+inline bool needs_full_paths(const MarchUniforms* u, uint32_t n) {
   for (uint32_t v = 0; v < n; ++v) {
-    if (u[v].type_grid) return true;
+    if (u[v].type_grid || u[v].kahan || u[v].cone || u[v].lightning_radius > 0.0f) return true;
     for (uint32_t i = 0; i < u[v].layer_count && i < 8u; ++i)
       if (u[v].layers[i].cloud_type == 7u) return true;
   }
   return false;
 }
-// Persistent batched march (march_batch.cu); `cb` as needs_cb_paths.
+// Persistent batched march (march_batch.cu); `full` as needs_full_paths.
 int launch_march_batch(const PscMarchOptions& o, int threads, uint32_t tile_w,
                        const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles,
-                       uint32_t n_tiles, uint32_t* counter, int sms, bool cb, cudaStream_t stream);
+                       uint32_t n_tiles, uint32_t* counter, int sms, bool full, cudaStream_t stream);
 // Per-view sky-view + aerial-perspective LUTs for a batch (atmosphere.cu):
 // `d_frames` holds n frame records built by frame_lite_from; outputs are
 // float4 (RGBA16F-rounded), sky 192x108 and AP 32x32x64 per view.
