@@ -26,7 +26,11 @@ __device__ __forceinline__ void unpack_tile(uint32_t w, uint32_t& view, uint32_t
 // 768 threads per SM (6 CTAs of 128): the shared-memory uniform block turns
 // every uniform operand into a register, and 80 registers per thread remove
 // nearly all spills (measured: 8 CTAs/SM 5.80 ms, 7 5.50, 6 5.35 on a 1080p
-// view; 64 uneven views 224.9 -> 209.4 ms).
+// view; 64 uneven views 224.9 -> 209.4 ms).  FULL = false: every view of the
+// batch runs the lean form.  FULL = true: each view runs the form it needs
+// (needs_full_paths on its uniform block), so the views of a mixed batch that
+// need no full-form path still get the lean one (64 uneven views 209.5 ->
+// 194.2 ms).
 template <int ST, int FILT, int NT, bool FULL>
 __global__ void __launch_bounds__(NT, 768 / NT)
     k_march_batch(const MarchUniforms* __restrict__ views_u, const ViewDev* __restrict__ views_v,
@@ -39,6 +43,7 @@ __global__ void __launch_bounds__(NT, 768 / NT)
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t warps_x = tile_w >> 3;  // 8x4-pixel warp tiles per tile row
   uint32_t cur = 0xffffffffu;
+  bool vfull = FULL, changed = false;
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
     __syncthreads();
@@ -52,13 +57,20 @@ __global__ void __launch_bounds__(NT, 768 / NT)
       for (uint32_t i = threadIdx.x; i < sizeof(MarchUniforms) / 16; i += NT) dst[i] = __ldg(src + i);
       if (threadIdx.x == 0) sv = views_v[view];
       cur = view;
+      changed = true;
     }
     __syncthreads();
+    if (FULL && changed) vfull = needs_full_paths(&su, 1);  // this view's form
+    changed = false;
     const uint32_t tile_h = (NT / 32 / warps_x) * 4u;
     const uint32_t px = tx * tile_w + (warp % warps_x) * 8u + (lane & 7u);
     const uint32_t py = ty * tile_h + (warp / warps_x) * 4u + (lane >> 3);
-    if (px < sv.width && py < sv.height)
-      march_pixel_fast<ST, FILT, FULL>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
+    if (px < sv.width && py < sv.height) {
+      if (FULL && vfull)
+        march_pixel_fast<ST, FILT, true>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
+      else
+        march_pixel_fast<ST, FILT, false>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
+    }
     __syncthreads();  // su, sv and s_tile are rewritten by the next iteration
   }
 }

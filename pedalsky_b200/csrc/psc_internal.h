@@ -198,8 +198,9 @@ int launch_noise_bakes(uint8_t* base, uint8_t* detail, uint8_t* curl, cudaStream
 // True when a march over these n uniform blocks needs the FAST kernels' full
 // form: a layer of type 7 (Cumulonimbus), a cloud-type grid (its cells may
 // hold any type), Kahan sums, cone light sampling or lightning.  Otherwise
-// the lean form, built without those paths, computes the same values.
-inline bool needs_full_paths(const MarchUniforms* u, uint32_t n) {
+// the lean form, built without those paths, computes the same values.  The
+// batched kernel also evaluates it per view on the device.
+inline __host__ __device__ bool needs_full_paths(const MarchUniforms* u, uint32_t n) {
   for (uint32_t v = 0; v < n; ++v) {
     if (u[v].type_grid || u[v].kahan || u[v].cone || u[v].lightning_radius > 0.0f) return true;
     for (uint32_t i = 0; i < u[v].layer_count && i < 8u; ++i)

@@ -284,6 +284,30 @@ def test_edge_cases(case, oracle, oracle_noise):
     _variant(case, EDGE_CASES[case], oracle, oracle_noise, frac=5e-3)
 
 
+def test_kahan_optical_depth_matches_fp64_oracle(oracle, oracle_noise):
+    """options.kahan: compensated sums of the step and light-march optical
+    depths (the precision form), on both schedules, against the FP64 oracle."""
+    _variant("kahan", lambda s: setattr(s.options, "kahan", 1), oracle, oracle_noise, frac=5e-3)
+
+
+def test_lean_and_full_kernel_forms_agree(oracle, oracle_noise):
+    """The FAST kernels come in a lean form, built without the Cumulonimbus,
+    type-grid, Kahan, cone and lightning paths, and a full form; the library
+    runs the lean one when a scene needs none of those paths.  A lightning
+    source of zero illuminance selects the full form without changing any
+    value, so the two renders of the same scene must agree."""
+    for st, filt in ((capi.STORAGE_F16, capi.FILTER_HYBRID), (capi.STORAGE_U8, capi.FILTER_EXACT)):
+        s = scenes.precision_1080p(96, 54, storage=st, schedule=capi.SCHED_FAST, filt=filt)
+        luts = oracle.bake_luts(s.frame, s.world)
+        _, _, lean = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
+        s.frame.lightning_illuminance[0:4] = [0.0, 0.0, 0.0, 2000.0]
+        s.frame.lightning_origin_world[0:3] = [0.0, 0.0, 0.0]
+        _, _, full = _gpu.render(s, oracle_noise, luts, composite_bg=s.background)
+        st_ = rel_stats(lean, full)
+        _report(f"lean_vs_full/{st}/{filt}", st_)
+        assert st_["p999"] <= 1e-6 and st_["frac_gt_1e3"] == 0.0, st_
+
+
 def test_all_cloud_types_and_type_grid(oracle, oracle_noise):
     def mutate(s):
         ln = scenes.synth_layers([(t, 500.0 + 1300.0 * t, 1500.0 + 1300.0 * t, 0.6)
