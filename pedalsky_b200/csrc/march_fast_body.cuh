@@ -734,8 +734,10 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
       bool live = h >= 0.0f && h <= 1.0f;
       float nd = 0.0f;
       if (live && !(FULL && u.type_grid)) {
+        // the lean form has no Cumulonimbus layer, so ndf_mode 0 there means
+        // an unknown type, whose profile is 0
         nd = L.ndf_mode ? ndf_eval(NdfCoef{L.ndf_inv_a, L.ndf_b1, L.ndf_inv_w1}, h)
-                        : ndf_fast(h, L.cloud_type, L.anvil_bias);
+                        : (FULL ? ndf_fast(h, L.cloud_type, L.anvil_bias) : 0.0f);
         live = fmaf(nd, 1.000001f, -L.skip_k) * L.density_scale > 1e-3f;
       }
       if (live) {
