@@ -388,7 +388,8 @@ def run_ours(args):
 
     # the same frames through the persistent batched kernel (psc_render_batch,
     # one launch per step replayed from a CUDA graph, per-view LUT bakes
-    # included), the form the north-star ratio is stated for
+    # included): its rate against the plain FP32 drop-in and its fraction of
+    # the L2 read ceiling are reported beside the single-view kernel's
     batched = None
     if not args.no_plain_reference and schedule == capi.SCHED_FAST:
         from pedalsky_b200 import batch as B
