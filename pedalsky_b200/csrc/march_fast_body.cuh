@@ -410,6 +410,12 @@ struct NdfGeneral {
   NdfCoef k;
   __device__ __forceinline__ float operator()(float h) const { return ndf_eval(k, h); }
 };
+// ndf of a non-Cumulonimbus type on taps that are all past the bottom ramp
+// (h * inv_a >= 1, so its smoothstep is exactly 1): the top factor alone.
+struct NdfTop {
+  NdfCoef k;
+  __device__ __forceinline__ float operator()(float h) const { return ssr_b(k.inv_w1, k.b1, h); }
+};
 struct NdfCb {
   float anvil_bias;
   __device__ __forceinline__ float operator()(float h) const { return ndf_fast(h, 7u, anvil_bias); }
@@ -525,6 +531,12 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
       lr.c2 = s2 * lr.ih;
       lr.c3 = -cv * __fdividef(s2, r0) * lr.ih;
       if (FULL && type == 7u) return light_march_tex<ST, NdfCb, true, true, FULL>(u, L, lr, NdfCb{L.anvil_bias});
+      // heights rise along the light path when cos(up, sun) >= 0 (the cubic's
+      // slope stays positive over 20 km), so the first tap bounds them all
+      const float t_first = 0.5f * step;
+      const float h_first = fmaf(t_first, fmaf(t_first, fmaf(t_first, lr.c3, lr.c2), lr.c1), lr.c0);
+      if (cv >= 0.0f && h_first * gen.k.inv_a >= 1.0001f)
+        return light_march_tex<ST, NdfTop, false, true, FULL>(u, L, lr, NdfTop{gen.k});
       return light_march_tex<ST, NdfGeneral, false, true, FULL>(u, L, lr, gen);
     }
     if (FULL && type == 7u) return light_march_tex<ST, NdfCb, true, false, FULL>(u, L, lr, NdfCb{L.anvil_bias});
