@@ -535,7 +535,7 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
       // slope stays positive over 20 km), so the first tap bounds them all
       const float t_first = 0.5f * step;
       const float h_first = fmaf(t_first, fmaf(t_first, fmaf(t_first, lr.c3, lr.c2), lr.c1), lr.c0);
-      if (cv >= 0.0f && h_first * gen.k.inv_a >= 1.0001f)
+      if (!FULL && cv >= 0.0f && h_first * gen.k.inv_a >= 1.0001f)  // lean form only
         return light_march_tex<ST, NdfTop, false, true, FULL>(u, L, lr, NdfTop{gen.k});
       return light_march_tex<ST, NdfGeneral, false, true, FULL>(u, L, lr, gen);
     }
