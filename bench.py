@@ -176,7 +176,7 @@ def bytes_per_ray(storage: str, schedule: str = "fast", workload: str = WORKLOAD
 
 # DRAM bytes (read + write) per launch of the timed kernel, from one ncu
 # capture of the benchmark command (profiles/k_march_fast_f16_hybrid_1080p.md).
-DRAM_TRAFFIC_PER_LAUNCH = {("precision_1080p", "fast", "f16", "hybrid", 1920, 1080): 132808704}
+DRAM_TRAFFIC_PER_LAUNCH = {("precision_1080p", "fast", "f16", "hybrid", 1920, 1080): 132546048}
 
 
 def fetch_peaks(device: int) -> dict:
