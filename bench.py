@@ -440,6 +440,8 @@ def run_ours(args):
                                         d_hdr.data_ptr())})
 
     def e2e_pass(n_steps):
+        if n_steps <= 0:
+            return 0.0
         n = n_steps * n_frames
         freed = []  # read-back of frame i done: its slot is free for frame i + 2
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
