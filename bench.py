@@ -2,18 +2,31 @@
 primary + 6 light steps), one primary ray per pixel, march + composite.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload precision_1080p|plain_320x180|stress_2160p|batch_64|grid_512]
                   [--storage f16|u8|f32|bf16|fp8] [--schedule plain|fast]
-                  [--filter exact|hybrid|texture]
+                  [--filter exact|hybrid|texture] [--no-legs]
 
 Default: FP16 noise storage, FAST schedule, hybrid filtering (exact FP32
 weights for the primary density, texture-unit taps for the light march) —
-the form that meets the 1e-3 bar against the FP64 oracle.  The same run also
-times the plain FP32-storage drop-in kernel and reports the ratio.
+the form that meets the 1e-3 bar against the FP64 oracle.  The default run
+prints ONE JSON line: the headline (the 1080p frame), the plain FP32-storage
+drop-in on the same frame, the same frame through the batched kernel, the
+frame split into row bands over the ranks, and three legs with their own
+timing and clock record: the 64-view uneven batch, the eight 4K Cumulonimbus
+frames and the grid adjoint.
 
-One process per GPU (torchrun for N > 1).  The forward march has no exchange
-step, so each rank renders its own full frame of the sequence (weak scaling);
-time is the max over ranks of the device-timed step.  `--impl reference`
-times the CPU restatement of the reference's FP32 march on the host cores.
+One process per GPU.  `--gpus N` without a torchrun environment re-launches
+itself under torch.distributed.run with N ranks.  The forward march has no
+exchange step: for the headline each rank renders its own frame of the
+sequence (weak scaling); the 64 views and the eight 4K frames are partitioned
+over the ranks by estimated cost, and the row-band leg splits one frame (both
+strong scaling, the fixed total work divided); the grid adjoint shards rows
+and sums its gradient with one NCCL all-reduce.  Times are device-timed
+(CUDA events on the launching stream) and the max over ranks.
+
+`--impl reference` times the CPU restatement of the reference's FP32 march
+on the host cores (the reference's own WGSL cannot run on this box), each
+step a bounded row sample of the same frame; only rank 0 works.
 """
 from __future__ import annotations
 
@@ -21,6 +34,7 @@ import argparse
 import ctypes as C
 import json
 import os
+import socket
 import subprocess
 import sys
 import threading
@@ -35,6 +49,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Mrays/s at 1080p, FP16-stored vs FP32 march at <=1e-3 rel err; % L2/tex roofline"
 UNIT = "Mrays/s"
 WORKLOAD = "precision_1080p"
+L2_NOTE = ("GPU arm: L2 flushed between timed steps (256 MiB write); CPU arm: no flush, its "
+           "working set stays in the host caches")
 # Frame workloads: name -> (default size, frames per step, description).
 FRAME_WORKLOADS = {
     "precision_1080p": ((1920, 1080), 1, {"layers": "Cu 1500-2300 cov 0.5; As 4000-5000 cov 0.7; "
@@ -47,6 +63,28 @@ FRAME_WORKLOADS = {
                                        "primary_steps": 256, "light_steps": 8,
                                        "frames": "8, simulated_seconds 0..7, 15 m/s wind"}),
 }
+# Which GPU tests hold each workload's parity against the FP64 oracle.
+PARITY = {
+    "precision_1080p": "tests/test_gpu_fullsize.py::test_precision_1080p_benchmark_pipeline "
+                       "(full frame, GPU-baked noise and LUTs, this exact form)",
+    "plain_320x180": "tests/test_gpu_march.py (c1, every storage and filter form)",
+    "stress_2160p": "tests/test_gpu_fullsize.py::test_stress_2160p_frame_benchmark_pipeline "
+                    "(a full 3840x2160 frame) and tests/test_gpu_march.py (frames 0 and 7)",
+    "batch_64": "tests/test_gpu_batch.py (batched views against single-view renders and the "
+                "FP64 oracle)",
+    "grid_512": "tests/test_gpu_grid.py (gradients against the FP64 reverse sweep and central "
+                "differences)",
+}
+# ncu figures of the timed kernel on the benchmark command: DRAM bytes read +
+# written per launch and the fraction of issue slots busy (the binding limit).
+NCU_KERNEL = {("precision_1080p", "fast", "f16", "hybrid", 1920, 1080):
+              {"traffic": 132546048, "issue_active": 0.836}}
+
+
+def workload_config(wl, W, H):
+    """The workload as both arms state it (the reference arm uses the same dict)."""
+    _, _, desc = FRAME_WORKLOADS[wl]
+    return {"workload": f"{wl} {W}x{H}", **desc, "l2": L2_NOTE}
 
 
 def frame_scenes(workload, W, H, **kw):
@@ -59,7 +97,7 @@ def frame_scenes(workload, W, H, **kw):
     return [scenes.precision_1080p(W, H, **kw)]
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -69,7 +107,9 @@ def parse():
     ap.add_argument("--schedule", default="fast", choices=["plain", "fast"])
     ap.add_argument("--filter", default="hybrid", choices=["exact", "texture", "hybrid"])
     ap.add_argument("--no-plain-reference", action="store_true",
-                    help="skip timing the plain FP32-storage drop-in kernel for the speed-up ratio")
+                    help="skip the plain FP32-storage drop-in and the batched form of the frame")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the 64-view, 8x4K and grid-adjoint legs of the default run")
     ap.add_argument("--width", type=int, default=None, help="default: the workload's size")
     ap.add_argument("--height", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -79,14 +119,60 @@ def parse():
                     help="stress_2160p: eight 4K frames of a Cumulonimbus over a 2048^2 coverage "
                          "grid; batch_64: the 64-view uneven batch in one persistent kernel")
     ap.add_argument("--batch-views", type=int, default=64)
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
-def dist_env():
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
-    return rank, world, local
+# ---------------------------------------------------------------- ranks
+
+class Ranks:
+    """This process's place in the job (torchrun environment) and the
+    collectives the benchmark uses: a barrier and the max of a scalar."""
+
+    def __init__(self, backend="nccl"):
+        self.rank = int(os.environ.get("RANK", 0))
+        self.world = int(os.environ.get("WORLD_SIZE", 1))
+        self.local = int(os.environ.get("LOCAL_RANK", 0))
+        self.dist = None
+        self.backend = backend
+
+    def init(self, device):
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(self.backend, init_method="env://",
+                                    timeout=datetime.timedelta(seconds=180), device_id=device)
+            self.dist = dist
+            assert dist.get_world_size() == self.world
+        return self
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, value: float, device) -> float:
+        import torch
+        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+        if self.dist is not None:
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def relaunch(args) -> int:
+    """`--gpus N` outside torchrun: run this script under torch.distributed.run
+    with N ranks on this node and return its exit status."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
 
 
 class _NullCtx:
@@ -142,16 +228,31 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+# ------------------------------------------------------------- roofline
+
+# Bytes per fetch of the FAST schedule's forms, by kind: a bilinear or
+# trilinear tap is its texels times the bytes of the form read.  F16
+# storage reads the channel-folded volumes (base 4 B and detail 2 B per
+# texel, the curl tile as (R, G) half pairs); other storages read RGBA
+# texels (4 B for RGBA8 and FP8, 8 B for FP16/BF16, 16 B for FP32).  LUT
+# texels are RGBA32F.  Outputs: L and T written, the HDR target read and
+# written (64 B per ray).
+def fetch_sizes(storage: str, schedule: str = "fast") -> dict:
+    if schedule == "fast" and storage == "f16":
+        base_b, detail_b, curl_b = 4, 2, 4
+    else:
+        base_b = detail_b = {"u8": 4, "fp8": 4, "f16": 8, "bf16": 8, "f32": 16}[storage]
+        curl_b = 2
+    return {"weather": 4 * 4, "type": 1, "base": 8 * base_b, "curl": 4 * curl_b,
+            "detail": 8 * detail_b, "light": 8 * base_b, "trans": 4 * 16, "sky": 4 * 16,
+            "ap": 8 * 16, "blue": 4, "depth": 4, "output": 64}
+
+
 def bytes_per_ray(storage: str, schedule: str = "fast", workload: str = WORKLOAD) -> dict:
-    """Algorithmic texel bytes per primary ray of this workload: executed
-    fetches counted by the instrumented CPU restatement on the same scene
-    (tests/golden/fetch_counts.json) times texels per fetch (bilinear 4,
-    trilinear 8, load 1) times the bytes per texel of the form the kernel
-    reads.  The FAST schedule with FP16 storage reads channel-folded volumes:
-    base (R, fbm) 4 B and detail (fbm) 2 B per texel, the curl tile as (R, G)
-    half pairs 4 B per texel; other forms read RGBA texels (4 B for RGBA8
-    and FP8, 8 B for FP16/BF16, 16 B for FP32).  LUT texels are RGBA32F.
-    Outputs: L and T written, the HDR target read and written (64 B)."""
+    """Algorithmic texel bytes per primary ray of this workload: the fetches
+    the reference algorithm executes on the same scene, counted by the
+    instrumented CPU restatement (tests/golden/fetch_counts.json), times the
+    bytes per fetch of the form the kernel reads (fetch_sizes)."""
     p = ROOT / "tests" / "golden" / "fetch_counts.json"
     if not p.exists():
         return {}
@@ -159,24 +260,29 @@ def bytes_per_ray(storage: str, schedule: str = "fast", workload: str = WORKLOAD
     if not d:
         return {}
     c = d["counts"]
-    if schedule == "fast" and storage == "f16":
-        base_b, detail_b, curl_b = 4, 2, 4
-    else:
-        base_b = detail_b = {"u8": 4, "fp8": 4, "f16": 8, "bf16": 8, "f32": 16}[storage]
-        curl_b = 2
-    per_kind = {
-        "weather": 4 * 4, "base": 8 * base_b, "curl": 4 * curl_b, "detail": 8 * detail_b,
-        "light": 8 * base_b, "trans": 4 * 16, "sky": 4 * 16, "ap": 8 * 16, "blue": 4, "depth": 4,
-    }
-    total = sum(c[k] * v for k, v in per_kind.items()) + c["pixels"] * 64
+    sz = fetch_sizes(storage, schedule)
+    total = sum(c[k] * sz[k] for k in ("weather", "base", "curl", "detail", "light", "trans",
+                                       "sky", "ap", "blue", "depth")) + c["pixels"] * sz["output"]
     return {"bytes_per_ray": total / c["pixels"], "pixels": c["pixels"],
             "dense_per_ray": c["dense"] / c["pixels"], "steps_per_ray": c["steps"] / c["pixels"],
             "light_fetches_per_ray": c["light"] / c["pixels"]}
 
 
-# DRAM bytes (read + write) per launch of the timed kernel, from one ncu
-# capture of the benchmark command (profiles/k_march_fast_f16_hybrid_1080p.md).
-DRAM_TRAFFIC_PER_LAUNCH = {("precision_1080p", "fast", "f16", "hybrid", 1920, 1080): 132546048}
+def fetched_bytes_per_ray(counts: dict, storage: str, schedule: str = "fast") -> dict:
+    """Bytes per ray the FAST kernel actually requested, from the counts of
+    its instrumented build (psc_count_fetches) on the benchmark frame."""
+    sz = fetch_sizes(storage, schedule)
+    n = max(counts["rays"], 1)
+    total = (counts["weather_taps"] * sz["weather"] + counts["type_loads"] * sz["type"]
+             + counts["live_steps"] * (sz["base"] + sz["curl"])
+             + counts["detail_taps"] * sz["detail"] + counts["light_taps"] * sz["light"]
+             + counts["transmittance_taps"] * sz["trans"] + counts["skyview_taps"] * sz["sky"]
+             + counts["ap_taps"] * sz["ap"] + counts["depth_loads"] * sz["depth"]
+             + counts["rays"] * (sz["blue"] + sz["output"]))
+    return {"bytes_per_ray": total / n, "steps_per_ray": counts["primary_steps"] / n,
+            "live_steps_per_ray": counts["live_steps"] / n,
+            "dense_per_ray": counts["dense_samples"] / n,
+            "light_fetches_per_ray": counts["light_taps"] / n}
 
 
 def fetch_peaks(device: int) -> dict:
@@ -189,30 +295,121 @@ def fetch_peaks(device: int) -> dict:
             "tex_trilinear_gfetch_s": fp.tex_trilinear_gfetch_s}
 
 
-def cpu_baseline(scene, sample_rows: int, reps: int = 1):
-    """The FP32 CPU restatement on a bounded row sample; returns (rays/s, rays, threads)."""
+def measured_peaks() -> dict:
+    pk = ROOT / "MEASURED_PEAKS.json"
+    return json.loads(pk.read_text()) if pk.exists() else {}
+
+
+# ---------------------------------------------------------- CPU baseline
+
+def cpu_sample(scene, noise, luts, rows: int, bands: int = 8):
+    """One bounded sample of the FP32 CPU restatement: `bands` bands of
+    rows // bands consecutive rows spread over the frame, all host threads.
+    Returns (rays, seconds, threads)."""
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    band = max(1, rows // bands)
+    starts = np.linspace(0, scene.height - band, bands).astype(int)
+    t0 = time.perf_counter()
+    for r0 in starts:
+        pyoracle.render(scene, noise, luts, precision=pyoracle.FP32, threads=threads,
+                        rows=(int(r0), int(r0) + band))
+    return bands * band * scene.width, time.perf_counter() - t0, threads
+
+
+def cpu_baseline(scene, rows: int, reps: int = 5):
+    """Median over `reps` repeats (after one warm-up) of the FP32 CPU
+    restatement on a bounded row sample of `scene`."""
     from oracle import pyoracle
     noise = pyoracle.bake_noise()
     luts = pyoracle.bake_luts(scene.frame, scene.world)
-    h = scene.height
-    step = max(1, h // sample_rows)
-    rows = list(range(0, h, step))[:sample_rows]
+    cpu_sample(scene, noise, luts, rows)
+    runs = [cpu_sample(scene, noise, luts, rows) for _ in range(reps)]
+    rays, threads = runs[0][0], runs[0][2]
+    secs = float(np.median([r[1] for r in runs]))
+    return {"value": rays / secs / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{rays} rays (8 row bands of the {scene.width}x{scene.height} frame) per "
+                      f"repeat, median of {reps} repeats after one warm-up: {secs:.2f} s"}
+
+
+# ------------------------------------------------------- reference arm
+
+def run_reference(args):
+    """The CPU restatement of the reference's FP32 march, timed on the host
+    cores: each step is one bounded row sample of the frame, timed whole.
+    The scene is assembled by the oracle's own restatements of the
+    reference's input producers, so this process maps no product library."""
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return 0
+    from oracle import pyoracle
+    from pedalsky_b200 import scenes
+    if args.workload == "grid_512":
+        return run_reference_grid(args)
+    wl = args.workload if args.workload in FRAME_WORKLOADS else WORKLOAD
+    (dw, dh), n_frames, desc = FRAME_WORKLOADS[wl]
+    W, H = args.width or dw, args.height or dh
+    with scenes.host_helpers(pyoracle.OracleHost()):
+        if wl == "stress_2160p":
+            s = scenes.stress_2160p(W, H, frame_index=0)
+        else:
+            s = frame_scenes(wl, W, H)[0]
+    noise = pyoracle.bake_noise()
+    luts = pyoracle.bake_luts(s.frame, s.world)
+    rows = 64 if wl == WORKLOAD else 32
+    for _ in range(args.warmup):
+        cpu_sample(s, noise, luts, rows)
+    runs = [cpu_sample(s, noise, luts, rows) for _ in range(args.steps)]
+    rays, threads = runs[0][0], runs[0][2]
+    secs = [r[1] for r in runs]
+    value = float(np.median([rays / t for t in secs])) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(secs)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded reference noise hash, reference synthesis)",
+        "impl": "reference",
+        "config": workload_config(wl, W, H),
+        "arm": "CPU restatement of the reference's FP32 march (RGBA8 noise, RGBA16F LUTs and "
+               "weather, FP32 arithmetic), all host threads; the reference's own WGSL path "
+               "needs a graphics stack, which this box does not have",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"each step marches {rays} rays (8 row bands of the {W}x{H} "
+                                   f"frame) and is timed whole; ms_per_step is that sample's "
+                                   f"time, value the median rate over the steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "rays_per_step": rays,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def grid_cpu_sample(sc, noise, luts, rows: int):
+    """FP64 CPU restatement of the grid forward + reverse sweep on `rows`
+    rows (4 bands) spread over the view; returns (rays, seconds, threads)."""
+    from oracle import pyoracle
+    G = sc.extra["grid"]
+    spec = sc.extra["grid_spec"]
+    bg = sc.background
+    tgt = np.ascontiguousarray(bg, np.float32)  # the timing does not depend on the target values
     threads = os.cpu_count() or 1
-    # bands of consecutive rows spread over the image: `rows` start rows
-    band = max(1, sample_rows // 8)
-    starts = np.linspace(0, h - band, 8).astype(int)
-    times = []
-    rays = 0
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        rays = 0
-        for r0 in starts:
-            pyoracle.render(scene, noise, luts, precision=pyoracle.FP32, threads=threads,
-                            rows=(int(r0), int(r0) + band))
-            rays += band * scene.width
-        times.append(time.perf_counter() - t0)
-    del rows
-    return rays / float(np.median(times)), rays, threads, float(np.median(times))
+    band = max(1, rows // 4)
+    starts = np.linspace(0, sc.height - band, 4).astype(int)
+    t0 = time.perf_counter()
+    for r0 in starts:
+        pyoracle.grid_adjoint(sc, noise, luts, G, spec, bg, tgt, threads=threads,
+                              rows=(int(r0), int(r0) + band))
+    return 4 * band * sc.width, time.perf_counter() - t0, threads
+
+
+GRID_METRIC = ("Mrays/s of the adjoint (forward + checkpointed reverse + gradient all-reduce), "
+               "512^2 view of a 256x256x64 voxel grid, 96+6 steps")
+
+
+def grid_config(world=1):
+    return {"workload": "grid_512", "grid": [256, 256, 64], "view": [512, 512],
+            "primary_steps": 96, "light_steps": 6, "checkpoint_every": 16,
+            "exit_transmittance": 0.01, "l2": L2_NOTE}
 
 
 def run_reference_grid(args):
@@ -220,83 +417,326 @@ def run_reference_grid(args):
     reverse sweep on a bounded row sample per step, all host threads."""
     from oracle import pyoracle
     from pedalsky_b200 import scenes
-    sc = scenes.grid_512()
+    with scenes.host_helpers(pyoracle.OracleHost()):
+        sc = scenes.grid_512()
     noise = pyoracle.bake_noise()
     luts = pyoracle.bake_luts(sc.frame, sc.world)
     for _ in range(args.warmup):
-        grid_cpu_baseline(sc, noise, luts, 32)
-    vals = []
-    for _ in range(args.steps):
-        v, rays, threads, secs = grid_cpu_baseline(sc, noise, luts, 64)
-        vals.append(v)
-    value = float(np.median(vals)) / 1e6
+        grid_cpu_sample(sc, noise, luts, 32)
+    runs = [grid_cpu_sample(sc, noise, luts, 64) for _ in range(args.steps)]
+    rays, threads = runs[0][0], runs[0][2]
+    secs = [r[1] for r in runs]
+    value = float(np.median([rays / t for t in secs])) / 1e6
     line = {
         "metric": GRID_METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * sc.width * sc.height / (value * 1e6), "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(secs)),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Worley grid)", "impl": "reference",
-        "config": {"workload": "grid_512", "grid": [256, 256, 64], "view": [sc.width, sc.height],
-                   "primary_steps": 96, "light_steps": 6,
-                   "note": "the reference has no voxel-grid form or adjoint; this is the CPU "
-                           "restatement (FP64 reverse sweep) on a row sample"},
+        "config": grid_config(),
+        "arm": "the reference has no voxel-grid form or adjoint; this is the CPU restatement "
+               "(FP64 reverse sweep)",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{rays} rays per step (4 row bands)"},
+                         "sample": f"each step runs {rays} rays (4 row bands) and is timed whole"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "rays_per_step": rays,
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_reference(args):
-    rank, world, _ = dist_env()
-    if rank != 0:
-        return 0
-    if args.workload == "grid_512":
-        return run_reference_grid(args)
-    wl = args.workload if args.workload in FRAME_WORKLOADS else WORKLOAD
-    (dw, dh), n_frames, desc = FRAME_WORKLOADS[wl]
-    W, H = args.width or dw, args.height or dh
-    s = frame_scenes(wl, W, H)[0]
-    sample = 64 if wl == WORKLOAD else 32  # rows per step
-    for _ in range(args.warmup):
-        cpu_baseline(s, sample)
-    vals = []
-    for _ in range(args.steps):
-        v, rays, threads, secs = cpu_baseline(s, sample)
-        vals.append(v)
-    value = float(np.median(vals)) / 1e6
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * n_frames * W * H / (value * 1e6),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded reference noise hash, reference synthesis)",
-        "impl": "reference",
-        "config": {"workload": f"{wl} {W}x{H}", **desc,
-                   "note": "CPU restatement of the reference FP32 march (the reference's WGSL "
-                           "cannot run here: no graphics stack)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{rays} rays per step (8 row bands of the first frame)"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-    return 0
+# ------------------------------------------------------------ our arm
+
+class Bench:
+    """Per-process GPU state shared by the legs: device, stream, L2 flush
+    buffer, ranks."""
+
+    def __init__(self, args, ranks: Ranks):
+        import torch
+        self.torch = torch
+        self.args = args
+        self.ranks = ranks
+        torch.cuda.set_device(ranks.local)
+        self.dev = torch.device("cuda", ranks.local)
+        ranks.init(self.dev)
+        self.stream = torch.cuda.Stream(device=self.dev)
+        self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=self.dev)
+
+    def timed(self, step, pre=None, clk=None, kernel_events=None, steps=None, warmup=None):
+        """W untimed steps, then K device-timed steps with the L2 flushed (and
+        `pre` run) before each, outside the events.  Returns (per-step ms of
+        this rank, the max over ranks of their mean).  `kernel_events`, when
+        given, is a list that `step` appends (start, end) event pairs to."""
+        torch = self.torch
+        steps = self.args.steps if steps is None else steps
+        warmup = self.args.warmup if warmup is None else warmup
+        with torch.cuda.stream(self.stream):
+            for _ in range(warmup):
+                if pre:
+                    pre()
+                step()
+        torch.cuda.synchronize()
+        if kernel_events is not None:
+            kernel_events.clear()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        self.ranks.barrier()
+        torch.cuda.synchronize()
+        with (clk if clk is not None else _NullCtx()):
+            with torch.cuda.stream(self.stream):
+                for i in range(steps):
+                    self.flush.zero_()
+                    if pre:
+                        pre()
+                    evs[i][0].record(self.stream)
+                    step()
+                    evs[i][1].record(self.stream)
+            torch.cuda.synchronize()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        mean = float(np.mean(ms)) if ms else 0.0
+        return ms, self.ranks.max(mean, self.dev)
+
+    def sh(self):
+        return C.c_void_p(self.stream.cuda_stream)
 
 
-def run_ours(args):
-    import torch
-    import torch.distributed as dist
+def leg_row_bands(B: Bench, sub, s, depth, bg):
+    """One frame split into contiguous row bands, one per rank (weighted by
+    the rows' sky fraction: ground pixels stop at the depth buffer), each
+    band marched through psc_render with its viewport offset, then the
+    composited bands all-gathered so every rank holds the whole frame."""
+    from pedalsky_b200 import capi, sharding
+    from pedalsky_b200.capi import call
+    torch = B.torch
+    W, H = s.width, s.height
+    sky_rows = (s.depth == 0).mean(axis=1) + 0.25
+    bands = sharding.row_bands(H, B.ranks.world, sky_rows)
+    band = bands[B.ranks.rank]
+    rows = band.y1 - band.y0
+    L = torch.empty((max(rows, 1), W, 4), dtype=torch.float32, device=B.dev)
+    T = torch.empty_like(L)
+    hdr = torch.empty_like(L)
+    bg_band = bg[band.y0:band.y1].contiguous() if rows else None
+    dep_band = depth[band.y0:band.y1].contiguous() if rows else None
+    view = capi.View(W, rows, dep_band.data_ptr() if rows else None, L.data_ptr(), T.data_ptr(),
+                     hdr.data_ptr(), W, H, 0, band.y0)
+    full = {}
 
+    def pre():
+        if rows:
+            hdr[:rows].copy_(bg_band, non_blocking=True)
+
+    def step():
+        if rows:
+            call("psc_render", sub.handle, C.byref(view), 1, B.sh())
+        if B.ranks.world > 1:
+            full["img"] = sharding.gather_rows(hdr[:rows], band, bands)
+
+    ms, ms_max = B.timed(step, pre=pre)
+    return {"value": W * H / (ms_max * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_max,
+            "scaling": "strong", "ranks": B.ranks.world,
+            "bands": [[b.y0, b.y1] for b in bands],
+            "config": "the headline frame split into one row band per rank (psc_render with a "
+                      "viewport offset), then all-gathered (NCCL) into the whole frame on every "
+                      "rank; the gather is inside the timed step"}
+
+
+def leg_batch64(B: Bench, storage, filt, n_views=64):
+    """c3: 64 seeded views of uneven size and scene, partitioned over the
+    ranks by estimated cost (largest first onto the lightest rank); each
+    rank marches its views in one persistent kernel per step, replayed from
+    a captured CUDA graph, launch shape from the autotuner."""
+    from pedalsky_b200 import batch as Bt
+    from pedalsky_b200 import scenes, sharding
+    from pedalsky_b200.subsystem import subsystem_for_scene
+    views = scenes.batch_views(n_views, seed=0, host_inputs=False, storage=storage, filt=filt,
+                               composite=1)
+    costs = [sharding.view_cost(v.width, v.height, v.params.cloud_steps, v.n_layers) for v in views]
+    parts = sharding.partition_views(costs, B.ranks.world)
+    mine = [views[i] for i in parts[B.ranks.rank]]
+    total_rays = sum(v.width * v.height for v in views)
+    sub = b = None
+    tune = None
+    launches = 0
+    if mine:
+        sub = subsystem_for_scene(mine[0], device=B.ranks.local, luts=None)
+        b = Bt.Batch(mine, B.dev)
+        with B.torch.cuda.stream(B.stream):
+            tune = Bt.autotune(sub.handle, b, reps=1, stream=B.stream)
+        Bt.set_tuning(sub.handle, tune["threads"], tune["tile_w"], use_graph=1)
+        l0 = sub.launch_count()
+    clk = ClockSampler(B.ranks.local)
+    ms, ms_max = B.timed((lambda: b.render(sub.handle, B.stream)) if mine else (lambda: None),
+                         pre=(b.reset_hdr if mine else None), clk=clk)
+    if mine:
+        launches = sub.launch_count() - l0
+        sub.close()
+    return {"metric": f"Mrays/s, {n_views} uneven views (c3)", "value":
+            total_rays / (ms_max * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_max,
+            "scaling": "strong", "rays_per_step": total_rays, "views": n_views,
+            "views_this_rank": len(mine), "autotuned": tune, "gpu_launches": launches,
+            "config": "one persistent kernel per rank per step from a captured CUDA graph, "
+                      "per-view sky-view / aerial-perspective LUT bakes included; views split "
+                      "over ranks by estimated cost",
+            "parity": PARITY["batch_64"], "clocks": clk.summary(),
+            "step_ms": [round(x, 3) for x in ms]}
+
+
+def leg_stress(B: Bench, storage, schedule, filt, W=3840, H=2160):
+    """c5: eight 4K Cumulonimbus frames (simulated_seconds 0..7 at 15 m/s)
+    over a 2048^2 coverage grid, partitioned over the ranks; each frame is
+    one march + fused composite."""
+    from pedalsky_b200 import capi, scenes, sharding
+    from pedalsky_b200.capi import call
+    from pedalsky_b200.subsystem import subsystem_for_scene
+    torch = B.torch
+    frames = [scenes.stress_2160p(W, H, frame_index=k, host_inputs=False, storage=storage,
+                                  schedule=schedule, filt=filt) for k in range(8)]
+    parts = sharding.partition_views([1.0] * 8, B.ranks.world)
+    mine = [frames[i] for i in parts[B.ranks.rank]]
+    launches = 0
+    sub = None
+    if mine:
+        sub = subsystem_for_scene(mine[0], device=B.ranks.local, luts=None)
+        o = capi.MarchOptions.from_buffer_copy(sub.options)
+        o.composite = 1
+        sub.set_options(o)
+        depth, bg = scenes.device_inputs(mine[0].frame, mine[0].world, W, H, B.dev)
+        hdr = torch.empty_like(bg)
+        L = torch.empty_like(bg)
+        T = torch.empty_like(bg)
+        view = capi.View(W, H, depth.data_ptr(), L.data_ptr(), T.data_ptr(), hdr.data_ptr())
+
+    def step():
+        for f in mine:
+            call("psc_set_frame", sub.handle, C.byref(f.frame), C.byref(f.world))
+            hdr.copy_(bg, non_blocking=True)
+            call("psc_render", sub.handle, C.byref(view), 1, B.sh())
+
+    if mine:
+        l0 = sub.launch_count()
+    clk = ClockSampler(B.ranks.local)
+    ms, ms_max = B.timed(step, clk=clk)
+    if mine:
+        launches = sub.launch_count() - l0
+        sub.close()
+    rays = 8 * W * H
+    return {"metric": "Mrays/s, eight 3840x2160 Cumulonimbus frames (c5)",
+            "value": rays / (ms_max * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_max,
+            "scaling": "strong", "rays_per_step": rays, "frames_this_rank": len(mine),
+            "gpu_launches": launches,
+            "config": f"{storage} storage, {schedule} schedule, {filt} filtering, fused "
+                      "composite; 256 + 8 steps; frames split over ranks",
+            "parity": PARITY["stress_2160p"], "clocks": clk.summary(),
+            "step_ms": [round(x, 3) for x in ms]}
+
+
+def leg_grid(B: Bench, with_e2e=False):
+    """c4: one 512^2 view's loss gradient with respect to the 256x256x64
+    voxel grid per step.  Pixels are sharded in row bands over the ranks;
+    each rank runs its band's adjoint and one sum all-reduce (NCCL) of the
+    16 MiB gradient grid gives every rank the whole image's gradient."""
+    from pedalsky_b200 import grid as GR
+    from pedalsky_b200 import scenes, sharding
+    from pedalsky_b200.subsystem import subsystem_for_scene
+    torch = B.torch
+    sc = scenes.grid_512()
+    W, H = sc.width, sc.height
+    G = sc.extra["grid"]
+    sub = subsystem_for_scene(sc, device=B.ranks.local, luts=None)
+    P = GR.GridProblem(sc, G, device=B.dev)
+    Pt = GR.GridProblem(sc, scenes.grid_target_values(G), device=B.dev)
+    with torch.cuda.stream(B.stream):
+        Pt.render(sub.handle, stream=B.stream)
+        P.set_target(Pt.composite_image())
+    torch.cuda.synchronize()
+    del Pt
+    band = sharding.row_bands(H, B.ranks.world)[B.ranks.rank]
+    rows = (band.y0, band.y1) if B.ranks.world > 1 else None
+
+    def step():
+        P.zero_grad()
+        if band.y1 > band.y0:
+            P.adjoint(sub.handle, rows=rows, stream=B.stream)
+        sharding.allreduce_gradient(P.grad, P.acc)
+
+    l0 = sub.launch_count()
+    clk = ClockSampler(B.ranks.local)
+    ms, ms_max = B.timed(step, clk=clk)
+    launches = sub.launch_count() - l0
+    _, fwd_ms = B.timed(lambda: P.render(sub.handle, rows=rows, stream=B.stream))
+    _, adj_ms = B.timed(lambda: (P.zero_grad(), P.adjoint(sub.handle, rows=rows, stream=B.stream)))
+    out = {"metric": GRID_METRIC, "value": W * H / (ms_max * 1e-3) / 1e6, "unit": UNIT,
+           "ms_per_step": ms_max, "scaling": "strong", "gpu_launches": launches,
+           "forward_only": {"value": W * H / (fwd_ms * 1e-3) / 1e6, "ms_per_step": fwd_ms},
+           "adjoint_kernel_ms": adj_ms, "rows_this_rank": [band.y0, band.y1],
+           "config": grid_config(), "parity": PARITY["grid_512"], "clocks": clk.summary(),
+           "step_ms": [round(x, 4) for x in ms]}
+    bpr = grid_bytes_per_ray()
+    if bpr:
+        rays_rank = W * (band.y1 - band.y0)
+        peak, src = _hbm_peak()
+        ach = bpr["adjoint"] * rays_rank / (adj_ms * 1e-3) / 1e9
+        out["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                           "frac": ach / peak, "traffic": None, "peak_source": src,
+                           "bytes_per_ray": bpr["adjoint"], "kernel": "k_grid_march<adjoint>",
+                           "note": "algorithmic bytes (texels, LUT taps, atomic adds); the grid "
+                                   "and gradient (16 MiB each) are L2-resident"}
+    if with_e2e:
+        h_vals = torch.from_numpy(np.ascontiguousarray(G)).pin_memory()
+        h_grad = torch.empty_like(h_vals).pin_memory()
+        h_acc = torch.empty(2, dtype=torch.float64).pin_memory()
+
+        def e2e():
+            P.values.copy_(h_vals, non_blocking=True)
+            step()
+            h_grad.copy_(P.grad, non_blocking=True)
+            h_acc.copy_(P.acc, non_blocking=True)
+
+        _, e2e_ms = B.timed(e2e)
+        out["e2e"] = {"value": W * H / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
+                      "h2d_bytes_per_step": h_vals.numel() * 4,
+                      "d2h_bytes_per_step": h_grad.numel() * 4 + 16}
+        out["_scene"] = sc
+    sub.close()
+    return out
+
+
+def _hbm_peak():
+    hbm = measured_peaks().get("hbm_gbs")
+    return (hbm, "measured (MEASURED_PEAKS.json)") if hbm else (6650.0, "fallback")
+
+
+def grid_bytes_per_ray() -> dict:
+    """Algorithmic bytes per ray of the grid forward and adjoint kernels from
+    the executed work counted by the CPU restatement (fetch_counts.json):
+    FP32 texels read by primary and light taps, two bilinear RGBA32F LUT taps
+    (sun transmittance, sky view) per step, the blue-noise load and the L/T
+    writes; the adjoint adds the segment recompute (texels again), the
+    reverse sweep's LUT taps, one 4-byte atomic add per texel and the
+    background/target reads."""
+    p = ROOT / "tests" / "golden" / "fetch_counts.json"
+    if not p.exists():
+        return {}
+    d = json.loads(p.read_text()).get("grid_512")
+    if not d:
+        return {}
+    c = d["counts"]
+    px = c["pixels"]
+    tex = 4 * (c["primary_texels"] + c["light_texels"])
+    lut = c["steps"] * 2 * 4 * 16
+    fwd = (tex + lut) / px + 4 + 32
+    adj = (3 * tex + 2 * lut) / px + 4 + 32 + 32
+    return {"forward": fwd, "adjoint": adj, "steps_per_ray": c["steps"] / px}
+
+
+def run_frames(args, ranks: Ranks):
+    """Frame workloads (the default): the headline frame and the extras."""
     from pedalsky_b200 import capi, scenes
     from pedalsky_b200.capi import call
     from pedalsky_b200.subsystem import subsystem_for_scene
 
-    rank, world, local = dist_env()
-    if world > 1:
-        dist.init_process_group("nccl", init_method="env://",
-                                timeout=__import__("datetime").timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
+    B = Bench(args, ranks)
+    torch, dev = B.torch, B.dev
     storage = capi.STORAGE_NAMES[args.storage]
     schedule = capi.SCHED_FAST if args.schedule == "fast" else capi.SCHED_PLAIN
     filt = capi.FILTER_NAMES[args.filter]
@@ -306,73 +746,58 @@ def run_ours(args):
     # each rank renders its own frame(s) of the sequence (weak scaling)
     frames = frame_scenes(wl, W, H, storage=storage, schedule=schedule, filt=filt)
     for f in frames:
-        f.frame.frame_index += rank * n_frames
+        f.frame.frame_index += ranks.rank * n_frames
     s = frames[0]
-    sub = subsystem_for_scene(s, device=local, luts=None)  # noise + LUTs baked on the device
-    stream = torch.cuda.Stream(device=dev)
-    sh = C.c_void_p(stream.cuda_stream)
+    sub = subsystem_for_scene(s, device=ranks.local, luts=None)  # noise + LUTs baked on the device
+    sh = B.sh()
+    stream = B.stream
 
     L = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
     T = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
     bg = torch.from_numpy(s.background).to(dev)
     hdr = torch.empty_like(bg)
     depth = torch.from_numpy(s.depth).to(dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     o = capi.MarchOptions.from_buffer_copy(sub.options)
     o.composite = 1
     sub.set_options(o)
     view = capi.View(W, H, depth.data_ptr(), L.data_ptr(), T.data_ptr(), hdr.data_ptr())
+    kev = []
 
     def render_step():
         """One step: every frame of the workload (the frames differ only in
-        simulated time, so the sky-view and AP LUTs stay valid)."""
+        simulated time, so the sky-view and AP LUTs stay valid); the march
+        launch itself is bracketed by its own events for the roofline."""
         for f in frames:
             if n_frames > 1:
                 call("psc_set_frame", sub.handle, C.byref(f.frame), C.byref(f.world))
             hdr.copy_(bg, non_blocking=True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
             call("psc_render", sub.handle, C.byref(view), 1, sh)
-
-    timed_launches = {}
-
-    def timed_steps(clk=None):
-        """W untimed steps, then K device-timed steps (L2 flushed before each);
-        the library's kernel launches inside the timed loop go to
-        timed_launches["n"]."""
-        with torch.cuda.stream(stream):
-            for _ in range(args.warmup):
-                render_step()
-        torch.cuda.synchronize()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(args.steps)]
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        l0 = sub.launch_count()
-        with (clk if clk is not None else _NullCtx()):
-            with torch.cuda.stream(stream):
-                for i in range(args.steps):
-                    flush.zero_()                      # evict L2 between timed steps
-                    evs[i][0].record(stream)
-                    render_step()
-                    evs[i][1].record(stream)
-            torch.cuda.synchronize()
-        timed_launches["n"] = sub.launch_count() - l0
-        ms_list = [a.elapsed_time(b) for a, b in evs]
-        t = torch.tensor([float(np.mean(ms_list))], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return ms_list, float(t.item())
+            e1.record(stream)
+            kev.append((e0, e1))
 
     peaks_fetch = None
     try:
-        peaks_fetch = fetch_peaks(local)
-    except Exception as e:  # the calibration is reported, never required
+        peaks_fetch = fetch_peaks(ranks.local)
+    except Exception as e:  # reported with the roofline, never required
         print(f"fetch-peak calibration failed: {e}", file=sys.stderr)
-    clk = ClockSampler(local)
-    step_ms, ms_max = timed_steps(clk)
-    kernel_launches = timed_launches["n"]
+    clk = ClockSampler(ranks.local)
+    l0 = sub.launch_count()
+    step_ms, ms_max = B.timed(render_step, clk=clk, kernel_events=kev)
+    kernel_launches = sub.launch_count() - l0
+    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kev])) if kev else None
     rays_step = n_frames * W * H
-    value = world * rays_step / (ms_max * 1e-3) / 1e6
+    value = ranks.world * rays_step / (ms_max * 1e-3) / 1e6
+
+    # the fetches the timed kernel issues on this frame (instrumented build)
+    counts = None
+    if schedule == capi.SCHED_FAST and args.storage in ("f16", "u8") and args.filter != "texture":
+        fc = capi.FetchCounts()
+        with torch.cuda.stream(stream):
+            hdr.copy_(bg)
+            call("psc_count_fetches", sub.handle, C.byref(view), C.byref(fc), sh)
+        counts = fc.as_dict()
 
     # the plain FP32-storage drop-in kernel on the same frame, for the ratio
     plain = None
@@ -381,46 +806,30 @@ def run_ours(args):
         o_plain.schedule, o_plain.storage, o_plain.filter = (capi.SCHED_PLAIN, capi.STORAGE_F32,
                                                              capi.FILTER_EXACT)
         sub.set_options(o_plain)
-        _, ms_plain = timed_steps()
+        _, ms_plain = B.timed(render_step)
         sub.set_options(o)
-        plain = {"value": world * rays_step / (ms_plain * 1e-3) / 1e6, "ms_per_step": ms_plain,
-                 "config": "plain schedule, f32 storage, exact filtering"}
+        plain = {"value": ranks.world * rays_step / (ms_plain * 1e-3) / 1e6,
+                 "ms_per_step": ms_plain, "config": "plain schedule, f32 storage, exact filtering"}
 
     # the same frames through the persistent batched kernel (psc_render_batch,
     # one launch per step replayed from a CUDA graph, per-view LUT bakes
-    # included): its rate against the plain FP32 drop-in and its fraction of
-    # the L2 read ceiling are reported beside the single-view kernel's
+    # included)
     batched = None
     if not args.no_plain_reference and schedule == capi.SCHED_FAST:
-        from pedalsky_b200 import batch as B
-        bt = B.Batch(frames, dev)
+        from pedalsky_b200 import batch as Bt
+        bt = Bt.Batch(frames, dev)
         with torch.cuda.stream(stream):
-            btune = B.autotune(sub.handle, bt, reps=1, stream=stream)
-        B.set_tuning(sub.handle, btune["threads"], btune["tile_w"], use_graph=1)
-        with torch.cuda.stream(stream):
-            for _ in range(args.warmup):
-                bt.reset_hdr()
-                bt.render(sub.handle, stream)
-        torch.cuda.synchronize()
-        bevs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                for _ in range(args.steps)]
-        with torch.cuda.stream(stream):
-            for i in range(args.steps):
-                flush.zero_()
-                bt.reset_hdr()
-                bevs[i][0].record(stream)
-                bt.render(sub.handle, stream)
-                bevs[i][1].record(stream)
-        torch.cuda.synchronize()
-        ms_b = float(np.mean([a.elapsed_time(b) for a, b in bevs]))
-        if world > 1:
-            tb = torch.tensor([ms_b], dtype=torch.float64, device=dev)
-            dist.all_reduce(tb, op=dist.ReduceOp.MAX)
-            ms_b = float(tb.item())
-        batched = {"value": world * rays_step / (ms_b * 1e-3) / 1e6, "ms_per_step": ms_b,
+            btune = Bt.autotune(sub.handle, bt, reps=1, stream=stream)
+        Bt.set_tuning(sub.handle, btune["threads"], btune["tile_w"], use_graph=1)
+        _, ms_b = B.timed(lambda: bt.render(sub.handle, stream), pre=bt.reset_hdr)
+        batched = {"value": ranks.world * rays_step / (ms_b * 1e-3) / 1e6, "ms_per_step": ms_b,
                    "config": "psc_render_batch: persistent kernel from a captured CUDA graph, "
                              "per-view LUT bakes included", "autotuned": btune}
         del bt
+
+    row_bands = None
+    if n_frames == 1 and not args.no_legs:
+        row_bands = leg_row_bands(B, sub, s, depth, bg)
 
     # End to end through the C ABI with host buffers, as a frame stream would
     # run it: every frame copies its own depth and background from pinned host
@@ -458,7 +867,7 @@ def run_ours(args):
             stream.wait_event(got)
             with torch.cuda.stream(stream):
                 if i % n_frames == 0:
-                    flush.zero_()  # L2 evicted once per step, as in the device-timed run
+                    B.flush.zero_()  # L2 evicted once per step, as in the device-timed run
                 if n_frames > 1:
                     call("psc_set_frame", sub.handle, C.byref(f.frame), C.byref(f.world))
                 call("psc_render", sub.handle, C.byref(sl["view"]), 1, sh)
@@ -474,333 +883,197 @@ def run_ours(args):
         return start.elapsed_time(end) / n_steps
 
     e2e_pass(args.warmup)
-    te = torch.tensor([e2e_pass(args.steps)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * rays_step / (float(te.item()) * 1e-3) / 1e6
-    h_out = slots[0]["out"]
+    ranks.barrier()
+    e2e_ms = ranks.max(e2e_pass(args.steps), dev)
+    e2e_value = ranks.world * rays_step / (e2e_ms * 1e-3) / 1e6
     h2d = n_frames * (h_bg.numel() * 4 + h_depth.numel() * 4)
-    d2h = n_frames * h_out.numel() * 4
+    d2h = n_frames * slots[0]["out"].numel() * 4
+    sub.close()
 
-    if rank == 0:
-        peaks = {}
-        pk = ROOT / "MEASURED_PEAKS.json"
-        if pk.exists():
-            peaks = json.loads(pk.read_text())
-        hbm = peaks.get("hbm_gbs")
-        bpr = bytes_per_ray(args.storage, args.schedule, wl)
-        roof = None
-        if bpr:
-            achieved = bpr["bytes_per_ray"] * rays_step / (ms_max * 1e-3) / 1e9
-            peak = hbm if hbm else 6650.0
-            traffic = DRAM_TRAFFIC_PER_LAUNCH.get((wl, args.schedule, args.storage, args.filter, W, H))
-            roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "traffic": traffic,
-                    "peak_source": "measured" if hbm else "fallback",
-                    "bytes_per_ray": bpr["bytes_per_ray"], "kernel": "k_march_fast",
-                    "note": "achieved = algorithmic texel bytes of the executed fetches per launch / "
-                            "kernel time.  The noise/LUT working set is L2-resident, so these bytes "
-                            "are served by L1/TEX and L2, not HBM (DRAM traffic per launch is "
-                            "`traffic`); `fetch` relates them to the on-chip ceilings measured on "
-                            "this GPU"}
-            if peaks_fetch and batched:
-                b_ach = bpr["bytes_per_ray"] * rays_step / (batched["ms_per_step"] * 1e-3) / 1e9
-                batched["fetch_gbs"] = b_ach
-                batched["frac_of_l2_read"] = b_ach / peaks_fetch["l2_read_gbs"]
-            if peaks_fetch:
-                light_rate = bpr["light_fetches_per_ray"] * rays_step / (ms_max * 1e-3) / 1e9
-                roof["fetch"] = {
-                    "l2_read_peak_gbs": peaks_fetch["l2_read_gbs"],
-                    "frac_of_l2_read": achieved / peaks_fetch["l2_read_gbs"],
-                    "l1_read_peak_gbs": peaks_fetch["l1_read_gbs"],
-                    "frac_of_l1_read": achieved / peaks_fetch["l1_read_gbs"],
-                    "tex_trilinear_peak_gfetch_s": peaks_fetch["tex_trilinear_gfetch_s"],
-                    "light_march_gfetch_s": light_rate,
-                    "frac_of_tex_trilinear": light_rate / peaks_fetch["tex_trilinear_gfetch_s"],
-                    "source": "psc_measure_fetch_peaks, this run"}
+    legs = {}
+    if wl == WORKLOAD and not args.no_legs and schedule == capi.SCHED_FAST:
+        legs["batch_64"] = leg_batch64(B, storage, filt)
+        legs["stress_2160p"] = leg_stress(B, storage, schedule, filt)
+        legs["grid_512"] = leg_grid(B)
+
+    if ranks.rank == 0:
+        roof = roofline(args, wl, W, H, rays_step, kernel_ms, peaks_fetch, counts, batched)
         cpu = None
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_cpu_baseline and ranks.world == 1:
             try:
-                v, rays, threads, secs = cpu_baseline(s, 64 if wl == WORKLOAD else 32)
-                cpu = {"value": v / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-                       "sample": f"{rays} rays (8 row bands of the first {W}x{H} frame), {secs:.1f} s"}
+                cpu = cpu_baseline(s, 64 if wl == WORKLOAD else 32)
             except Exception as e:  # the baseline is reported, never the product
                 cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                        "sample": f"failed: {e}"}
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded reference noise hash, reference synthesis)",
-            "config": {"workload": f"{wl} {W}x{H}", **desc, "storage": args.storage,
-                       "schedule": args.schedule,
-                       "filter": args.filter, "composite": "fused",
-                       "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"views{world}"},
+            "config": workload_config(wl, W, H),
+            "form": {"storage": args.storage, "schedule": args.schedule, "filter": args.filter,
+                     "composite": "fused", "parallelism": f"frames{ranks.world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "pipeline": "per frame: pinned H2D, march + composite, D2H on three "
                                 "streams, two device slots"},
             "gpu_launches": kernel_launches,
+            "kernel_ms": kernel_ms,
             "roofline": roof,
+            "fetch_counts": counts,
+            "parity": PARITY.get(wl),
             "plain_fp32_dropin": plain,
             "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
             "batched_fp16": batched,
             "batched_speedup_vs_plain_fp32": (batched["value"] / plain["value"])
             if (batched and plain) else None,
+            "row_bands": row_bands,
+            "legs": legs or None,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "step_ms": [round(x, 4) for x in step_ms],
         }
         print(json.dumps(line), flush=True)
-    sub.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
-def run_batch(args):
-    """64 uneven views with their own scenes, one persistent kernel per step,
-    relaunched from a captured CUDA graph; launch shape chosen by the autotuner."""
-    import torch
+def roofline(args, wl, W, H, rays, kernel_ms, peaks_fetch, counts, batched):
+    """The timed kernel against the ceiling that bounds it.  The march's
+    working set (folded volumes, LUTs, weather) is L2-resident, so its
+    fetches are served on chip: the ceiling is the L2 read bandwidth
+    measured on this GPU in this run.  `achieved` counts the algorithmic
+    bytes (the reference algorithm's executed fetches); `fetched_*` counts
+    what the kernel requests (its instrumented build's tally); `hbm` is the
+    DRAM traffic from the ncu capture of the same command against the
+    measured copy bandwidth."""
+    if not kernel_ms:
+        return None
+    alg = bytes_per_ray(args.storage, args.schedule, wl)
+    ncu = NCU_KERNEL.get((wl, args.schedule, args.storage, args.filter, W, H), {})
+    out = {"kernel": "k_march_fast" if args.schedule == "fast" else "k_march_plain",
+           "kernel_ms": kernel_ms, "unit": "GB/s"}
+    if peaks_fetch:
+        l2 = peaks_fetch["l2_read_gbs"]
+        out.update({"bound": "l2_fetch", "peak": l2,
+                    "peak_source": "psc_measure_fetch_peaks: L2 read bandwidth of this GPU, "
+                                   "this run"})
+    else:
+        hbm, src = _hbm_peak()
+        out.update({"bound": "hbm", "peak": hbm, "peak_source": src,
+                    "note": "the on-chip calibration failed; HBM copy peak as the ceiling"})
+    if alg:
+        out["bytes_per_ray"] = alg["bytes_per_ray"]
+        out["achieved"] = alg["bytes_per_ray"] * rays / (kernel_ms * 1e-3) / 1e9
+        out["frac"] = out["achieved"] / out["peak"]
+    if counts:
+        fb = fetched_bytes_per_ray(counts, args.storage, args.schedule)
+        out["fetched_bytes_per_ray"] = fb["bytes_per_ray"]
+        out["fetched_achieved"] = fb["bytes_per_ray"] * rays / (kernel_ms * 1e-3) / 1e9
+        out["fetched_frac"] = out["fetched_achieved"] / out["peak"]
+        out["fetched"] = fb
+    out["traffic"] = ncu.get("traffic")
+    out["issue_active"] = ncu.get("issue_active")
+    if ncu:
+        out["binding_limit"] = "SM issue slots (ncu smsp__issue_active of this kernel)"
+    hbm, src = _hbm_peak()
+    if ncu.get("traffic"):
+        dram = ncu["traffic"] / (kernel_ms * 1e-3) / 1e9
+        out["hbm"] = {"dram_gbs": dram, "peak": hbm, "peak_source": src, "frac": dram / hbm}
+    if peaks_fetch:
+        out["fetch"] = {
+            "l1_read_peak_gbs": peaks_fetch["l1_read_gbs"],
+            "tex_trilinear_peak_gfetch_s": peaks_fetch["tex_trilinear_gfetch_s"]}
+        if alg:
+            out["fetch"]["frac_of_l1_read"] = out["achieved"] / peaks_fetch["l1_read_gbs"]
+            light = alg["light_fetches_per_ray"] * rays / (kernel_ms * 1e-3) / 1e9
+            out["fetch"]["light_march_gfetch_s"] = light
+            out["fetch"]["frac_of_tex_trilinear"] = light / peaks_fetch["tex_trilinear_gfetch_s"]
+        if alg and batched:
+            b_ach = alg["bytes_per_ray"] * rays / (batched["ms_per_step"] * 1e-3) / 1e9
+            batched["fetch_gbs"] = b_ach
+            batched["frac_of_l2_read"] = b_ach / peaks_fetch["l2_read_gbs"]
+    return out
 
-    from pedalsky_b200 import batch as B
-    from pedalsky_b200 import capi, scenes
-    from pedalsky_b200.subsystem import subsystem_for_scene
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    storage = capi.STORAGE_NAMES[args.storage]
-    filt = capi.FILTER_NAMES[args.filter]
-    views = scenes.batch_views(args.batch_views, seed=rank, host_inputs=False, storage=storage,
-                               filt=filt, composite=1)
-    sub = subsystem_for_scene(views[0], device=local, luts=None)
-    b = B.Batch(views, dev)
-    stream = torch.cuda.Stream(device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    with torch.cuda.stream(stream):
-        tune = B.autotune(sub.handle, b, reps=1, stream=stream)
-    B.set_tuning(sub.handle, tune["threads"], tune["tile_w"], use_graph=1)
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            b.reset_hdr()
-            b.render(sub.handle, stream)
-    torch.cuda.synchronize()
-    launches0 = sub.launch_count()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    with ClockSampler(local) as clk:
-        with torch.cuda.stream(stream):
-            for i in range(args.steps):
-                flush.zero_()
-                b.reset_hdr()
-                evs[i][0].record(stream)
-                b.render(sub.handle, stream)
-                evs[i][1].record(stream)
-        torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(c) for a, c in evs]
-    ms = float(np.mean(step_ms))
-    value = world * b.rays / (ms * 1e-3) / 1e6
-    if rank == 0:
+def run_batch(args, ranks: Ranks):
+    """64 uneven views with their own scenes: the c3 leg as the headline."""
+    from pedalsky_b200 import capi
+    B = Bench(args, ranks)
+    leg = leg_batch64(B, capi.STORAGE_NAMES[args.storage], capi.FILTER_NAMES[args.filter],
+                      args.batch_views)
+    if ranks.rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32",
+            "metric": METRIC, "value": leg["value"], "unit": UNIT, "n_gpus": ranks.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg["ms_per_step"],
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded random scenes per view, reference synthesis)",
-            "config": {"workload": f"batch_{args.batch_views} uneven views", "rays_per_step": b.rays,
-                       "storage": args.storage, "filter": args.filter, "schedule": "fast",
-                       "launch": "one persistent kernel per step from a captured CUDA graph",
-                       "autotuned": tune, "l2": "flushed between timed steps (256 MiB write)"},
-            "e2e": None, "gpu_launches": sub.launch_count() - launches0,
-            "clocks": clk.summary(), "step_ms": [round(x, 3) for x in step_ms],
+            "config": {"workload": f"batch_{args.batch_views} uneven views",
+                       "rays_per_step": leg["rays_per_step"], "l2": L2_NOTE},
+            "form": {"storage": args.storage, "filter": args.filter, "schedule": "fast",
+                     "launch": leg["config"], "autotuned": leg["autotuned"]},
+            "e2e": None, "gpu_launches": leg["gpu_launches"], "parity": leg["parity"],
+            "clocks": leg["clocks"], "step_ms": leg["step_ms"],
         }
         print(json.dumps(line), flush=True)
-    sub.close()
+    ranks.close()
     return 0
 
 
-GRID_METRIC = ("Mrays/s of the adjoint (forward + checkpointed reverse + gradient all-reduce), "
-               "512^2 view of a 256x256x64 voxel grid, 96+6 steps")
-
-
-def grid_bytes_per_ray() -> dict:
-    """Algorithmic bytes per ray of the grid forward and adjoint kernels from
-    the executed work counted by the CPU restatement (fetch_counts.json):
-    FP32 texels read by primary and light taps, two bilinear RGBA32F LUT taps
-    (sun transmittance, sky view) per step, the blue-noise load and the L/T
-    writes; the adjoint adds the segment recompute (texels again), the
-    reverse sweep's LUT taps, one 4-byte atomic add per texel and the
-    background/target reads."""
-    p = ROOT / "tests" / "golden" / "fetch_counts.json"
-    if not p.exists():
-        return {}
-    d = json.loads(p.read_text()).get("grid_512")
-    if not d:
-        return {}
-    c = d["counts"]
-    px = c["pixels"]
-    tex = 4 * (c["primary_texels"] + c["light_texels"])
-    lut = c["steps"] * 2 * 4 * 16
-    fwd = (tex + lut) / px + 4 + 32
-    adj = (3 * tex + 2 * lut) / px + 4 + 32 + 32
-    return {"forward": fwd, "adjoint": adj, "steps_per_ray": c["steps"] / px}
-
-
-def grid_cpu_baseline(sc, noise, luts, rows: int):
-    """FP64 CPU restatement of forward + reverse sweep on `rows` rows spread
-    over the view; returns (rays/s, rays, threads, seconds)."""
-    from oracle import pyoracle
-    G = sc.extra["grid"]
-    spec = sc.extra["grid_spec"]
-    bg = sc.background
-    tgt = np.ascontiguousarray(bg, np.float32)  # the timing does not depend on the target values
-    threads = os.cpu_count() or 1
-    band = max(1, rows // 4)
-    starts = np.linspace(0, sc.height - band, 4).astype(int)
-    t0 = time.perf_counter()
-    for r0 in starts:
-        pyoracle.grid_adjoint(sc, noise, luts, G, spec, bg, tgt, threads=threads,
-                              rows=(int(r0), int(r0) + band))
-    secs = time.perf_counter() - t0
-    rays = 4 * band * sc.width
-    return rays / secs, rays, threads, secs
-
-
-def run_grid(args):
-    """The differentiable form: one 512^2 view's loss gradient per step.  Pixels
-    are sharded in row bands over the ranks (strong scaling); each rank runs
-    its band's adjoint and one sum all-reduce (NCCL) of the 16 MiB gradient
-    grid gives every rank the whole image's gradient."""
-    import datetime
-
-    import torch
-    import torch.distributed as dist
-
-    from pedalsky_b200 import grid as GR
-    from pedalsky_b200 import scenes, sharding
-    from pedalsky_b200.subsystem import subsystem_for_scene
-
-    rank, world, local = dist_env()
-    if world > 1:
-        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    sc = scenes.grid_512()
-    W, H = sc.width, sc.height
-    G = sc.extra["grid"]
-    sub = subsystem_for_scene(sc, device=local, luts=None)
-    stream = torch.cuda.Stream(device=dev)
-    sh = stream
-    P = GR.GridProblem(sc, G, device=dev)
-    Pt = GR.GridProblem(sc, scenes.grid_target_values(G), device=dev)
-    with torch.cuda.stream(stream):
-        Pt.render(sub.handle, stream=sh)
-        P.set_target(Pt.composite_image())
-    torch.cuda.synchronize()
-    del Pt
-    band = sharding.row_bands(H, world)[rank]
-    rows = (band.y0, band.y1) if world > 1 else None
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-
-    def step():
-        P.zero_grad()
-        P.adjoint(sub.handle, rows=rows, stream=sh)
-        sharding.allreduce_gradient(P.grad, P.acc)
-
-    def timed(fn, n):
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(n)]
-        with torch.cuda.stream(stream):
-            for i in range(n):
-                flush.zero_()
-                evs[i][0].record(stream)
-                fn()
-                evs[i][1].record(stream)
-        torch.cuda.synchronize()
-        ms = [a.elapsed_time(b) for a, b in evs]
-        return ms, sharding.max_over_ranks(float(np.mean(ms)), device=dev)
-
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    launches0 = sub.launch_count()
-    with ClockSampler(local) as clk:
-        step_ms, ms = timed(step, args.steps)
-    launches = sub.launch_count() - launches0
-    value = W * H / (ms * 1e-3) / 1e6
-    fwd_ms_list, fwd_ms = timed(lambda: P.render(sub.handle, rows=rows, stream=sh), args.steps)
-    adj_only_ms_list, adj_ms = timed(lambda: (P.zero_grad(), P.adjoint(sub.handle, rows=rows, stream=sh)),
-                                     args.steps)
-
-    # end to end: the grid values go up from pinned host memory, the loss
-    # and the gradient come back
-    h_vals = torch.from_numpy(np.ascontiguousarray(G)).pin_memory()
-    h_grad = torch.empty_like(h_vals).pin_memory()
-    h_acc = torch.empty(2, dtype=torch.float64).pin_memory()
-
-    def e2e():
-        P.values.copy_(h_vals, non_blocking=True)
-        step()
-        h_grad.copy_(P.grad, non_blocking=True)
-        h_acc.copy_(P.acc, non_blocking=True)
-
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            e2e()
-    _, e2e_ms = timed(e2e, args.steps)
-    if rank == 0:
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-        hbm = peaks.get("hbm_gbs")
-        peak = hbm if hbm else 6650.0
-        bpr = grid_bytes_per_ray()
-        roof = None
-        if bpr:
-            rays_rank = W * (band.y1 - band.y0)
-            ach = bpr["adjoint"] * rays_rank / (adj_ms * 1e-3) / 1e9
-            roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                    "traffic": None, "peak_source": "measured" if hbm else "fallback",
-                    "bytes_per_ray": bpr["adjoint"], "kernel": "k_grid_march<adjoint>",
-                    "note": "algorithmic bytes (texels, LUT taps, atomic adds); the grid and "
-                            "gradient (16 MiB each) are L2-resident"}
+def run_grid(args, ranks: Ranks):
+    """The differentiable form as the headline (c4)."""
+    B = Bench(args, ranks)
+    leg = leg_grid(B, with_e2e=True)
+    sc = leg.pop("_scene")
+    if ranks.rank == 0:
         cpu = None
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_cpu_baseline and ranks.world == 1:
             from oracle import pyoracle
             noise = pyoracle.bake_noise()
             luts = pyoracle.bake_luts(sc.frame, sc.world)
-            v, rays, threads, secs = grid_cpu_baseline(sc, noise, luts, 128)
-            cpu = {"value": v / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"{rays} rays (4 row bands), FP64 forward + reverse sweep, {secs:.1f} s"}
+            runs = [grid_cpu_sample(sc, noise, luts, 128) for _ in range(5)]
+            secs = float(np.median([r[1] for r in runs]))
+            cpu = {"value": runs[0][0] / secs / 1e6, "unit": UNIT, "cores": runs[0][2],
+                   "kind": "port", "sample": f"{runs[0][0]} rays (4 row bands), FP64 forward + "
+                                             f"reverse sweep, median of 5: {secs:.2f} s"}
         line = {
-            "metric": GRID_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "metric": GRID_METRIC, "value": leg["value"], "unit": UNIT, "n_gpus": ranks.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg["ms_per_step"],
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Worley grid; target = render of the grid with 5% noise)",
-            "config": {"workload": "grid_512", "grid": [256, 256, 64], "view": [W, H],
-                       "primary_steps": 96, "light_steps": 6, "checkpoint_every": 16,
-                       "exit_transmittance": 0.01,
-                       "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"rowbands{world} + all-reduce"},
-            "forward_only": {"value": W * H / (fwd_ms * 1e-3) / 1e6, "ms_per_step": fwd_ms},
-            "adjoint_kernel_ms": adj_ms,
-            "e2e": {"value": W * H / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
-                    "h2d_bytes_per_step": h_vals.numel() * 4,
-                    "d2h_bytes_per_step": h_grad.numel() * 4 + 16},
-            "gpu_launches": launches,
-            "roofline": roof,
-            "cpu_baseline": cpu,
-            "clocks": clk.summary(),
-            "step_ms": [round(x, 4) for x in step_ms],
+            "config": grid_config(),
+            "form": {"parallelism": f"rowbands{ranks.world} + all-reduce"},
+            "forward_only": leg["forward_only"], "adjoint_kernel_ms": leg["adjoint_kernel_ms"],
+            "e2e": leg["e2e"], "gpu_launches": leg["gpu_launches"],
+            "roofline": leg.get("roofline"), "cpu_baseline": cpu, "parity": leg["parity"],
+            "clocks": leg["clocks"], "step_ms": leg["step_ms"],
         }
         print(json.dumps(line), flush=True)
-    sub.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
+    return 0
+
+
+def run_stress(args, ranks: Ranks):
+    """Eight 4K frames as the headline (c5), frames split over the ranks."""
+    from pedalsky_b200 import capi
+    B = Bench(args, ranks)
+    leg = leg_stress(B, capi.STORAGE_NAMES[args.storage],
+                     capi.SCHED_FAST if args.schedule == "fast" else capi.SCHED_PLAIN,
+                     capi.FILTER_NAMES[args.filter])
+    if ranks.rank == 0:
+        line = {
+            "metric": METRIC, "value": leg["value"], "unit": UNIT, "n_gpus": ranks.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg["ms_per_step"],
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded coverage grid, reference synthesis)",
+            "config": workload_config("stress_2160p", 3840, 2160),
+            "form": {"storage": args.storage, "schedule": args.schedule, "filter": args.filter,
+                     "composite": "fused", "parallelism": f"frames split over {ranks.world}"},
+            "e2e": None, "gpu_launches": leg["gpu_launches"], "parity": leg["parity"],
+            "clocks": leg["clocks"], "step_ms": leg["step_ms"],
+        }
+        print(json.dumps(line), flush=True)
+    ranks.close()
     return 0
 
 
@@ -808,11 +1081,18 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args)
+    ranks = Ranks()
+    if ranks.world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but the launch has WORLD_SIZE={ranks.world} ranks")
     if args.workload == "batch_64":
-        return run_batch(args)
+        return run_batch(args, ranks)
     if args.workload == "grid_512":
-        return run_grid(args)
-    return run_ours(args)
+        return run_grid(args, ranks)
+    if args.workload == "stress_2160p" and args.width is None:
+        return run_stress(args, ranks)
+    return run_frames(args, ranks)
 
 
 if __name__ == "__main__":

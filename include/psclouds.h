@@ -190,8 +190,11 @@ enum {
 /* Kernel schedule. */
 enum {
   PSC_SCHED_PLAIN = 0,     /* straight restatement, one thread per ray      */
-  PSC_SCHED_FAST = 1       /* hoisted per-ray constants, lane-compacted
-                              dense shading, fast transcendentals          */
+  PSC_SCHED_FAST = 1       /* hoisted per-ray and per-layer constants,
+                              folded FP16 volumes, batched light-march
+                              fetches, a profile bound that skips the
+                              fetches of steps that cannot be dense, fast
+                              transcendentals                              */
 };
 
 /* Settings the reference does not expose in `CloudParamsGpu`.  Zero-filled
@@ -446,6 +449,34 @@ int psc_composite_halfres(const float* luminance, const float* transmittance, ui
 int psc_composite(const float* luminance, const float* transmittance,
                   float* hdr, uint32_t width, uint32_t height, void* stream);
 
+/* No counterpart in the reference.  Counts of the fetches the FAST march
+ * issues for one view, by kind: the measured side of the fetch roofline
+ * (the algorithmic side counts the reference algorithm's fetches, which
+ * include taps the FAST kernel proves unnecessary and skips: a uniform
+ * weather map is not sampled, and steps whose profile bound keeps them
+ * below the density threshold fetch nothing).  Produced by an instrumented
+ * build of the FAST kernel that computes the same image (outputs as
+ * psc_render for this view) and counts as it goes; the timed kernels carry
+ * no counters.  Options: FAST schedule, F16 or U8 storage, exact or hybrid
+ * filtering, no debug checks, half-res or TAA; else PSC_ERR_UNSUPPORTED.
+ * Synchronous; allocates and frees a 96-byte counter buffer. */
+typedef struct PscFetchCounts {
+  uint64_t rays;                /* pixels marched                          */
+  uint64_t primary_steps;       /* primary steps executed                  */
+  uint64_t live_steps;          /* steps past the profile bound: one base-
+                                   shape tap and one curl tap each          */
+  uint64_t weather_taps;        /* bilinear weather taps (0: uniform map)  */
+  uint64_t type_loads;          /* cloud-type grid loads                   */
+  uint64_t detail_taps;         /* trilinear detail taps                   */
+  uint64_t dense_samples;       /* samples with density > 1e-3             */
+  uint64_t light_taps;          /* light-march base taps                   */
+  uint64_t transmittance_taps;  /* transmittance-LUT taps (sunlit samples) */
+  uint64_t skyview_taps;        /* sky-view LUT taps                       */
+  uint64_t ap_taps;             /* aerial-perspective taps                 */
+  uint64_t depth_loads;         /* depth-buffer loads                      */
+} PscFetchCounts;
+int psc_count_fetches(psc_ctx* ctx, const PscView* view, PscFetchCounts* out, void* stream);
+
 /* Number of march-kernel launches issued by this context so far. */
 int psc_launch_count(psc_ctx* ctx, uint64_t* out);
 
@@ -593,7 +624,17 @@ int psc_measure_fetch_peaks(int cuda_device, PscFetchPeaks* out, void* stream);
  * (those calls allocate); otherwise PSC_ERR_MISSING_INPUT.  The first call
  * on each device looks up the array's device address (and may load the
  * library's GPU code on that device); make that first call before any stream
- * capture.
+ * capture.  The address is kept for the life of the device's primary
+ * context: do not cudaDeviceReset a device while rendering on it with this
+ * entry point.
+ *
+ * The work list is staged through host arrays shared by all calls and
+ * copied with cudaMemcpyAsync from that pageable memory, which the driver
+ * stages itself: the calling thread may block until the driver has taken the
+ * bytes (about 2 KB per view plus 4 bytes per tile).  Because the staging
+ * is shared, a stream that is being captured into a CUDA graph is refused
+ * with PSC_ERR_UNSUPPORTED; psc_render_batch with use_graph = 1 is the
+ * graph-replayed form.
  *
  * Every call shares the one array, whose contents persist from the previous
  * call (the counter is cleared on each call).  Calls whose work overlaps on

@@ -32,6 +32,11 @@ int oracle_bake_noise_detail(uint8_t* out_rgba8);  /* 32^3 * 4  */
 int oracle_bake_noise_curl(uint8_t* out_rg8);      /* 128^2 * 2 */
 int oracle_blue_noise(uint8_t* out_r8);            /* 64^2      */
 
+/* ---- defaults: CloudParamsGpu::default() (crates/ps-clouds/src/params.rs:142-212),
+ *      AtmosphereParams::default() (crates/ps-core/src/weather.rs:60-84) ---- */
+int oracle_params_default(PscCloudParamsGpu* out);
+int oracle_world_default(PscWorldUniformsGpu* out);
+
 /* ---- synthesis (crates/ps-synthesis) ---- */
 float oracle_remap_coverage(float scene_coverage);
 int oracle_synthesise_layers(const PscCloudLayerDesc* in, uint32_t n,
@@ -122,6 +127,15 @@ int oracle_render_pixel(const OracleScene* scene, uint32_t width,
                         uint32_t height, uint32_t x, uint32_t y,
                         int precision, int filter, double* lum4,
                         double* trans4);
+
+/* The FP64 march of rows [row0, row1) (row1 = 0: all rows) recording per
+ * pixel how close it came to its two data-dependent branches
+ * (cloud_march.wgsl:833,885,996): out_t the smallest |max3(T) - 0.01| / 0.01
+ * of its early-exit tests, out_d the smallest |density - 1e-3| / 1e-3 of its
+ * primary samples (width*height doubles each; 1e30 where never tested). */
+int oracle_branch_margins(const OracleScene* scene, uint32_t width, uint32_t height,
+                          int threads, uint32_t row0, uint32_t row1, double* out_t,
+                          double* out_d);
 
 /* One FP64 primary density sample at world point p3 / altitude alt in layer
  * li with weather R value weather_r, and the layer profile ndf(h) there

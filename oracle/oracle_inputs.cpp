@@ -558,4 +558,60 @@ int oracle_frame_from_camera(const PscFlyCamera* cam, uint32_t width,
   return 0;
 }
 
+/* CloudParamsGpu::default() (crates/ps-clouds/src/params.rs:142-212), field
+ * by field in declaration order. */
+int oracle_params_default(PscCloudParamsGpu* o) {
+  if (!o) return -1;
+  std::memset(o, 0, sizeof(*o));
+  const float sig_s[3] = {0.030f, 0.040f, 0.060f};
+  for (int k = 0; k < 3; ++k) o->sigma_s[k] = sig_s[k];
+  o->droplet_diameter_bias = 1.0f;
+  o->cone_light_sampling = 0u;
+  o->forward_bias = 0.0f;
+  o->detail_strength = 0.05f;
+  o->curl_strength = 0.1f;
+  o->powder_strength = 1.0f;
+  o->multi_scatter_a = 0.5f;
+  o->multi_scatter_b = 0.5f;
+  o->multi_scatter_c = 0.5f;
+  o->ambient_strength = 1.0f;
+  o->base_scale_m = 4500.0f;
+  o->detail_scale_m = 800.0f;
+  o->weather_scale_m = 32000.0f;
+  o->light_steps = 6u;
+  o->cloud_steps = 192u;
+  o->multi_scatter_octaves = 4u;
+  o->cloud_layer_count = 0u;
+  o->temporal_jitter = 0u;
+  o->wind_drift_strength = 1.0f;
+  o->wind_skew_strength = 0.5f;
+  o->diurnal_strength = 1.0f;
+  return 0;
+}
+
+/* AtmosphereParams::default() (crates/ps-core/src/weather.rs:60-84). */
+int oracle_world_default(PscWorldUniformsGpu* o) {
+  if (!o) return -1;
+  std::memset(o, 0, sizeof(*o));
+  o->planet_radius_m = 6360000.0f;
+  o->atmosphere_top_m = 6460000.0f;
+  o->rayleigh_scale_height_m = 8000.0f;
+  o->mie_scale_height_m = 1200.0f;
+  const float rayleigh[4] = {5.802e-6f, 13.558e-6f, 33.100e-6f, 0.0f};
+  const float ozone[4] = {0.650e-6f, 1.881e-6f, 0.085e-6f, 0.0f};
+  for (int k = 0; k < 4; ++k) {
+    const float rgb = k < 3 ? 1.0f : 0.0f;  // w components are 0
+    o->rayleigh_scattering[k] = rayleigh[k];
+    o->mie_scattering[k] = 3.996e-6f * rgb;
+    o->mie_absorption[k] = 4.4e-6f * rgb;
+    o->ozone_absorption[k] = ozone[k];
+    o->ground_albedo[k] = 0.18f * rgb;
+    o->haze_extinction_per_m[k] = 0.0f;
+  }
+  o->mie_g = 0.8f;
+  o->ozone_center_m = 25000.0f;
+  o->ozone_thickness_m = 30000.0f;
+  return 0;
+}
+
 }  // extern "C"

@@ -108,6 +108,41 @@ int oracle_render_pixel(const OracleScene* s, uint32_t w, uint32_t h, uint32_t x
   return 0;
 }
 
+// Test support: the FP64 march of rows [row0, row1) (all rows when row1 is
+// 0) recording, per pixel, how close it came to its two data-dependent
+// branches (March::margin): out_t the smallest |max3(T) - 0.01| / 0.01 over
+// its early-exit tests, out_d the smallest |density - 1e-3| / 1e-3 over its
+// primary samples; 1e30 where a test never ran.  A pixel whose margin is
+// within the rounding of the operands can take the other branch under a
+// last-bit change of its inputs.
+int oracle_branch_margins(const OracleScene* s, uint32_t w, uint32_t h, int threads, uint32_t row0,
+                          uint32_t row1, double* out_t, double* out_d) {
+  if (!scene_ok(s) || !w || !h || !out_t || !out_d) return -1;
+  March<double> base;
+  base.init(s, false);
+  if (row1 == 0 || row1 > h) row1 = h;
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel
+  {
+    March<double> m = base;
+#pragma omp for schedule(dynamic, 1)
+    for (int y = (int)row0; y < (int)row1; ++y) {
+      for (uint32_t x = 0; x < w; ++x) {
+        double mg[2] = {1e30, 1e30};
+        m.margin = mg;
+        double l4[4], t4[4];
+        m.pixel(x, (uint32_t)y, s->depth, w, l4, t4);
+        const size_t o = (size_t)y * w + x;
+        out_t[o] = mg[0];
+        out_d[o] = mg[1];
+      }
+    }
+  }
+  return 0;
+}
+
 // Test support: one primary density sample (sample_density,
 // cloud_march.wgsl:432-530) in FP64 at world point p3 and altitude `alt`, in
 // layer `li`, with weather R channel `weather_r`; also the layer's profile

@@ -657,6 +657,19 @@ struct March {
     return r;
   }
 
+  // Branch-margin diagnostic (oracle_branch_margins): when not null, the
+  // march lowers margin[0] to the smallest |max3(T) - 0.01| / 0.01 of its
+  // early-exit tests and margin[1] to the smallest |density - 1e-3| / 1e-3
+  // of its primary samples, the two tests whose outcome a last-bit change of
+  // the operands can flip (cloud_march.wgsl:833,885,996).
+  double* margin = nullptr;
+  void note_exit(R tmax) const {
+    if (margin) margin[0] = std::fmin(margin[0], std::fabs((double)tmax - 0.01) / 0.01);
+  }
+  void note_density(R d) const {
+    if (margin) margin[1] = std::fmin(margin[1], std::fabs((double)d - 1e-3) / 1e-3);
+  }
+
   void pixel(uint32_t px, uint32_t py, const float* depth, uint32_t width, R lum_out[4],
              R tr_out[4]) const {
     count(ORACLE_CNT_PIXELS);
@@ -695,6 +708,7 @@ struct March {
     const V3<R> lw = mk<R>(R(0.2126), R(0.7152), R(0.0722));
 
     for (uint32_t i = 0; i < layer_count; ++i) {
+      note_exit(max3(trans));
       if (max3(trans) < R(0.01)) break;
       const Hit lh = hits[i];
       if (!lh.hit) continue;
@@ -718,6 +732,7 @@ struct March {
         count(ORACLE_CNT_WEATHER);
         const uint32_t type = effective_type(wsx, wsz, L);
         const R density = sample_density(p, alt, L, wr, w, type);
+        note_density(density);
         if (density > R(1e-3)) {
           count(ORACLE_CNT_DENSE);
           const R od = march_to_light(p, alt, L, wr, w, type);
@@ -763,6 +778,7 @@ struct March {
           twn = twn + sw;
           trans = trans * samp;
         }
+        note_exit(max3(trans));
         if (max3(trans) < R(0.01)) break;
         t = t + step;
       }

@@ -60,6 +60,8 @@ def lib() -> C.CDLL:
             ("oracle_bake_noise_detail", [vp], C.c_int),
             ("oracle_bake_noise_curl", [vp], C.c_int),
             ("oracle_blue_noise", [vp], C.c_int),
+            ("oracle_params_default", [vp], C.c_int),
+            ("oracle_world_default", [vp], C.c_int),
             ("oracle_remap_coverage", [f32], f32),
             ("oracle_synthesise_layers", [vp, u32, vp], C.c_int),
             ("oracle_weather_map", [u32, f32, f32, vp, u32, u32, f32, vp], C.c_int),
@@ -74,6 +76,7 @@ def lib() -> C.CDLL:
             ("oracle_bake_aerial", [vp, vp, vp, vp, vp], C.c_int),
             ("oracle_render", [vp, u32, u32, C.c_int, C.c_int, C.c_int, u32, u32, vp, vp, vp], C.c_int),
             ("oracle_render_pixel", [vp, u32, u32, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
+            ("oracle_branch_margins", [vp, u32, u32, C.c_int, u32, u32, vp, vp], C.c_int),
             ("oracle_composite", [vp, vp, vp, u32], C.c_int),
             ("oracle_density_sample", [vp, u32, vp, C.c_double, C.c_double, vp, vp], C.c_int),
             ("oracle_grid_render", [vp, vp, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
@@ -88,6 +91,46 @@ def lib() -> C.CDLL:
             fn.argtypes, fn.restype = args, res
         _LIB = L
     return _LIB
+
+
+class OracleHost:
+    """The scene-assembly helpers of `pedalsky_b200.scenes` (its CapiHost)
+    answered by this restatement instead of the product library, so a
+    process that only runs the CPU restatement (the reference arm of the
+    benchmark) assembles the same scenes without mapping libpsclouds.so:
+
+        with scenes.host_helpers(pyoracle.OracleHost()):
+            s = scenes.precision_1080p()
+    """
+
+    def params_default(self, out):
+        _ok(lib().oracle_params_default(C.byref(out)), "oracle_params_default")
+
+    def world_default(self, out):
+        _ok(lib().oracle_world_default(C.byref(out)), "oracle_world_default")
+
+    def options_default(self, out):
+        # PscMarchOptions' reference behaviour: approx-Mie, U8 storage, exact
+        # filtering, plain schedule; the dual-lobe HG lobes at 0.8 / -0.2 / 0.5
+        C.memset(C.byref(out), 0, C.sizeof(out))
+        out.phase_mode = capi.PHASE_APPROX_MIE
+        out.hg_g_forward, out.hg_g_backward, out.hg_blend = 0.8, -0.2, 0.5
+        out.storage, out.filter, out.schedule = capi.STORAGE_U8, capi.FILTER_EXACT, capi.SCHED_PLAIN
+
+    def synthesise_layers(self, descs, n, out):
+        _ok(lib().oracle_synthesise_layers(C.cast(descs, C.c_void_p), n, C.cast(out, C.c_void_p)),
+            "oracle_synthesise_layers")
+
+    def frame_from_camera(self, cam, width, height, alt, az, ang, lux, out):
+        _ok(lib().oracle_frame_from_camera(C.byref(cam), width, height, alt, az, ang, lux,
+                                           C.byref(out)), "oracle_frame_from_camera")
+
+    def weather_map(self, n_layers, grid, gw, gh, extent, out):
+        _ok(lib().oracle_weather_map(n_layers, 0.0, 0.0, grid, gw, gh, extent, out),
+            "oracle_weather_map")
+
+    def wind_field(self, speed, dir_deg, out):
+        _ok(lib().oracle_wind_field(speed, dir_deg, out), "oracle_wind_field")
 
 
 def _p(a):
@@ -174,6 +217,21 @@ def render(scene, noise, luts, precision=FP64, filt=FILTER_EXACT, threads=0, row
     if counters:
         return L, T, dict(zip(COUNTERS, (int(c) for c in cnt)))
     return L, T
+
+
+def branch_margins(scene, noise, luts, threads=0, rows=None):
+    """Per-pixel relative distance of the FP64 march from its early-exit
+    test (max3(T) vs 0.01) and its dense-sample test (density vs 1e-3):
+    two (h, w) float64 arrays (1e30 where the test never ran)."""
+    s, keep = make_scene(scene, noise, luts)
+    w, h = scene.width, scene.height
+    mt = np.full((h, w), 1e30)
+    md = np.full((h, w), 1e30)
+    r0, r1 = rows if rows else (0, 0)
+    _ok(lib().oracle_branch_margins(C.byref(s), w, h, threads, r0, r1, _p(mt), _p(md)),
+        "oracle_branch_margins")
+    del keep
+    return mt, md
 
 
 def density_sample(scene, noise, luts, layer, p3, alt, weather_r):

@@ -155,6 +155,17 @@ class FetchPeaks(C.Structure):
                 ("_reserved", f32)]
 
 
+class FetchCounts(C.Structure):
+    """`PscFetchCounts`: fetches issued by the FAST march, by kind."""
+    _fields_ = [(n, C.c_uint64) for n in (
+        "rays", "primary_steps", "live_steps", "weather_taps", "type_loads", "detail_taps",
+        "dense_samples", "light_taps", "transmittance_taps", "skyview_taps", "ap_taps",
+        "depth_loads")]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
 class PscError(RuntimeError):
     def __init__(self, code: int, func: str, msg: str):
         super().__init__(f"{func}: {PSC_ERR.get(code, code)} ({code}): {msg}")
@@ -195,6 +206,7 @@ _PROTOS = {
     "psc_download_lut": [_vp, i32, _vp, C.c_size_t],
     "psc_render": [_vp, P(View), u32, _vp],
     "psc_composite": [_vp, _vp, _vp, u32, u32, _vp],
+    "psc_count_fetches": [_vp, P(View), P(FetchCounts), _vp],
     "psc_launch_count": [_vp, P(C.c_uint64)],
     "psc_set_batch_tuning": [_vp, P(BatchTuning)],
     "psc_get_batch_tuning": [_vp, P(BatchTuning)],

@@ -31,6 +31,45 @@ __global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constan
   march_pixel_fast<ST, FILT, FULL>(u, v, px, py, s_t0, s_t1, s_aux, kThreads, threadIdx.x);
 }
 
+// The instrumented build of the same kernel (psc_count_fetches): every
+// thread counts the fetches its ray issues, and each warp adds its sums to
+// `out` (kTallyKinds 64-bit counters).  Not a timed kernel.
+template <int ST, int FILT, bool FULL>
+__global__ void __launch_bounds__(kThreads) k_march_fast_tally(const __grid_constant__ MarchUniforms u,
+                                                               const __grid_constant__ ViewDev v,
+                                                               unsigned long long* out) {
+  extern __shared__ float s_dyn[];
+  const uint32_t nl = u.layer_count;
+  float* const s_t0 = s_dyn;
+  float* const s_t1 = s_dyn + nl * kThreads;
+  float* const s_aux = s_dyn + 2u * nl * kThreads;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t px = blockIdx.x * kTileW + (warp & 1u) * 8u + (lane & 7u);
+  const uint32_t py = blockIdx.y * kTileH + (warp >> 1) * 4u + (lane >> 3);
+  uint32_t tc[kTallyKinds];
+#pragma unroll
+  for (uint32_t k = 0; k < kTallyKinds; ++k) tc[k] = 0u;
+  if (px < v.width && py < v.height)
+    march_pixel_fast<ST, FILT, FULL, true>(u, v, px, py, s_t0, s_t1, s_aux, kThreads, threadIdx.x, tc);
+#pragma unroll
+  for (uint32_t k = 0; k < kTallyKinds; ++k) {
+    const uint32_t sum = __reduce_add_sync(0xffffffffu, tc[k]);
+    if (lane == 0 && sum) atomicAdd(out + k, (unsigned long long)sum);
+  }
+}
+
+template <int ST, int FILT>
+cudaError_t launch_fast_tally(const MarchUniforms& u, const ViewDev& v, unsigned long long* out,
+                              cudaStream_t s) {
+  const dim3 grid((v.width + kTileW - 1) / kTileW, (v.height + kTileH - 1) / kTileH);
+  const size_t smem = (2u * u.layer_count + kAuxWords) * kThreads * sizeof(float);
+  if (needs_full_paths(&u, 1))
+    k_march_fast_tally<ST, FILT, true><<<grid, kThreads, smem, s>>>(u, v, out);
+  else
+    k_march_fast_tally<ST, FILT, false><<<grid, kThreads, smem, s>>>(u, v, out);
+  return cudaGetLastError();
+}
+
 template <int ST, int FILT>
 cudaError_t launch_fast(const MarchUniforms& u, const ViewDev& v, cudaStream_t s) {
   const dim3 grid((v.width + kTileW - 1) / kTileW, (v.height + kTileH - 1) / kTileH);
@@ -43,6 +82,23 @@ cudaError_t launch_fast(const MarchUniforms& u, const ViewDev& v, cudaStream_t s
 }
 
 }  // namespace
+
+int launch_march_fast_tally(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
+                            unsigned long long* counts, cudaStream_t s) {
+  if (u.octaves > (uint32_t)kMaxOct || u.octaves == 0) return PSC_ERR_UNSUPPORTED;
+  cudaError_t e;
+  if (o.storage == PSC_STORAGE_F16 && o.filter == PSC_FILTER_HYBRID)
+    e = launch_fast_tally<PSC_STORAGE_F16, PSC_FILTER_HYBRID>(u, v, counts, s);
+  else if (o.storage == PSC_STORAGE_F16 && o.filter == PSC_FILTER_EXACT)
+    e = launch_fast_tally<PSC_STORAGE_F16, PSC_FILTER_EXACT>(u, v, counts, s);
+  else if (o.storage == PSC_STORAGE_U8 && o.filter == PSC_FILTER_HYBRID)
+    e = launch_fast_tally<PSC_STORAGE_U8, PSC_FILTER_HYBRID>(u, v, counts, s);
+  else if (o.storage == PSC_STORAGE_U8 && o.filter == PSC_FILTER_EXACT)
+    e = launch_fast_tally<PSC_STORAGE_U8, PSC_FILTER_EXACT>(u, v, counts, s);
+  else
+    return PSC_ERR_UNSUPPORTED;
+  return e == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
 
 int launch_march_fast(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
                       cudaStream_t s) {

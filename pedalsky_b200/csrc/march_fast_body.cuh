@@ -578,7 +578,9 @@ __device__ __forceinline__ float atan2_upper(float y, float x) {
 //  * sky-view ambient at the local up (cloud_march.wgsl:672-700): zenith
 //    angle, horizon angle pi/2 + atan2(rho, R) (rho < R below 2600 km) and
 //    azimuth; scaled by the sun illuminance.
-__device__ __forceinline__ void lut_lookups(const MarchUniforms& u, float alt, float ux, float uy,
+// Returns whether the transmittance LUT was fetched (not in the earth's
+// shadow), which only the fetch tally reads.
+__device__ __forceinline__ bool lut_lookups(const MarchUniforms& u, float alt, float ux, float uy,
                                             float uz, float3& trans, float3& sky) {
   const float R = u.planet_r;
   const float a0 = fmaxf(alt, 0.0f);
@@ -588,7 +590,8 @@ __device__ __forceinline__ void lut_lookups(const MarchUniforms& u, float alt, f
   const float r = R + a;
   const float rho = alt >= 1.0f ? rho0 : u.rho_1m;
   const float mu = clampf(fmaf(ux, u.sun[0], fmaf(uy, u.sun[1], uz * u.sun[2])), -1.0f, 1.0f);
-  if (mu <= -__fdividef(rho, r)) {
+  const bool lit = !(mu <= -__fdividef(rho, r));
+  if (!lit) {
     trans = make_float3(0.0f, 0.0f, 0.0f);
   } else {
     const float top = u.atmo_top;
@@ -612,6 +615,7 @@ __device__ __forceinline__ void lut_lookups(const MarchUniforms& u, float alt, f
   du = du - floorf(du);
   const float4 sk = u.tex_sky ? tex2D<float4>(u.tex_sky, du, vv) : lut2d(u.lut_sky, 192, 108, du, vv);
   sky = make_float3(sk.x * u.sun_illum[0], sk.y * u.sun_illum[1], sk.z * u.sun_illum[2]);
+  return lit;
 }
 
 // Weather R channel, repeat + bilinear; a uniform map is its value, power-of-
@@ -651,14 +655,30 @@ __device__ __forceinline__ float one_minus_exp_neg(float y, float e) {
 // aerial-perspective distance weights.
 constexpr uint32_t kAuxWords = kMaxOct + 6 + 5;
 
+// Fetch tally of the instrumented build (TALLY = true): per ray, the
+// fetches march_pixel_fast issues, by kind, in the order of PscFetchCounts.
+enum TallyKind : uint32_t {
+  kTallyRays, kTallySteps, kTallyLive, kTallyWeather, kTallyType, kTallyDetail, kTallyDense,
+  kTallyLight, kTallyTrans, kTallySky, kTallyAp, kTallyDepth, kTallyKinds
+};
+static_assert(kTallyKinds == kFetchTallyKinds, "one tally counter per PscFetchCounts field");
+
 // One primary ray of the FAST schedule.  `s_t0/s_t1` are this CTA's shared
 // arrays of per-layer entry/exit distances, laid out [layer][slot] with
 // `stride` slots; `slot` is this thread's column.  `s_aux` holds kAuxWords
 // words per thread, laid out the same way.
-template <int ST, int FILT, bool FULL = true>
+// TALLY = true is the instrumented build behind psc_count_fetches: the same
+// arithmetic, and `tc` (kTallyKinds counters of this thread) counts every
+// fetch issued; the timed kernels are built with TALLY = false, where `tc`
+// is unused and the counting compiles away.
+template <int ST, int FILT, bool FULL = true, bool TALLY = false>
 __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const ViewDev& v, uint32_t px,
                                                  uint32_t py, float* s_t0, float* s_t1, float* s_aux,
-                                                 uint32_t stride, uint32_t slot) {
+                                                 uint32_t stride, uint32_t slot, uint32_t* tc = nullptr) {
+  if constexpr (TALLY) {
+    ++tc[kTallyRays];
+    if (v.depth) ++tc[kTallyDepth];
+  }
 
   // Per-lane layer intervals live in shared memory for the march, so the 16
   // entry/exit distances do not occupy registers across the loop.
@@ -733,6 +753,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
     }
 
     for (uint32_t s = 0; s < u.cloud_steps; ++s) {
+      if constexpr (TALLY) ++tc[kTallySteps];
       const float t = fmaf((float)s + jitter, step, t0);
       const float px3 = fmaf(dx, t, cx), py3 = fmaf(dy, t, cy), pz3 = fmaf(dz, t, cz);
       const float bt = ray_B + t;
@@ -753,6 +774,11 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
         live = fmaf(nd, 1.000001f, -L.skip_k) * L.density_scale > 1e-3f;
       }
       if (live) {
+        if constexpr (TALLY) {
+          ++tc[kTallyLive];  // base-shape and curl fetches
+          if (!u.weather_uniform) ++tc[kTallyWeather];
+          if (FULL && u.type_grid) ++tc[kTallyType];
+        }
         const float wsx = px3 - L.wind_off_x, wsz = pz3 - L.wind_off_z;
         const float ax = fmaf(-L.skew_kx, h, wsx);
         const float az = fmaf(-L.skew_kz, h, wsz);
@@ -768,6 +794,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
         float cloud = shape_from<ST>(bs, L.lf_c, nd, 1.0f - eff);
         if (eff >= 0.01f) {  // coverage gate (cloud_march.wgsl:450-451)
           if (cloud > 0.0f) {  // curl-perturbed detail erosion (:502-527)
+            if constexpr (TALLY) ++tc[kTallyDetail];
             const float2 c2 = curl_blend(cf);
             const float ddx = fmaf(fmaf(c2.x, 2.0f, -1.0f), u.curl_offset_scale, ax);
             const float ddz = fmaf(fmaf(c2.y, 2.0f, -1.0f), u.curl_offset_scale, az);
@@ -785,7 +812,13 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             // the two LUT fetches go out before the light march's, so all of
             // a dense sample's texture fetches are in flight together
             float3 ts, sky;
-            lut_lookups(u, alt, ux, uy, uz, ts, sky);
+            [[maybe_unused]] const bool trans_fetched = lut_lookups(u, alt, ux, uy, uz, ts, sky);
+            if constexpr (TALLY) {
+              ++tc[kTallyDense];
+              ++tc[kTallySky];
+              tc[kTallyTrans] += trans_fetched ? 1u : 0u;
+              tc[kTallyLight] += (FULL && u.cone) ? 6u : u.light_steps;
+            }
             const float od = light_od<ST, FILT, FULL>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
             const float st_r = L.sigma_t[0], st_g = L.sigma_t[1], st_b = L.sigma_t[2];
             const float xr = st_r * od, xg = st_g * od, xb = st_b * od;
@@ -899,6 +932,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
   const float tw = s_acc[3 * stride + slot], twn = s_acc[4 * stride + slot];
   float Or = Lr, Og = Lg, Ob = Lb;
   if (opacity > 1e-4f) {
+    if constexpr (TALLY) ++tc[kTallyAp];
     const float t_cloud = __fdividef(tw, fmaxf(twn, 1e-6f));
     const float ds = fmaxf(t_cloud, 50.0f);
     const float az = clamp01(__logf(ds * (1.0f / 50.0f)) * (1.0f / 7.6009024595f));  // ln 2000

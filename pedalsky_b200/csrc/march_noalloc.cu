@@ -63,7 +63,10 @@ std::mutex g_mutex;                         // serialises host staging across th
 
 // Device address of the scratch array on `device`, which must be current.
 // Resolved once per device; the first lookup also loads this library's
-// module on that device if it is not loaded yet.
+// module on that device if it is not loaded yet.  The address stays valid
+// for the life of the device's primary context: a cudaDeviceReset while the
+// library is in use would leave it stale, so callers must not reset a
+// device they render on with this entry point.
 int scratch_on(int device, unsigned char** out) {
   if (device < 0 || device >= kMaxDevices)
     return fail(PSC_ERR_INVALID_ARGUMENT, "device %d beyond the allocation-free path's %d devices", device,
@@ -104,6 +107,19 @@ extern "C" int psc_render_batch_noalloc(psc_ctx* c, const PscBatchView* views, u
   if (fl > kFrameSlot) return fail(PSC_ERR_UNSUPPORTED, "frame record of %zu bytes exceeds its slot", fl);
   rc = psc::host::ensure_device(c);
   if (rc) return rc;
+  // The work list is staged through host arrays that every call reuses, so
+  // a graph recorded from this call would replay whatever the latest call
+  // staged, not the views it was recorded with: a capturing stream is
+  // refused before anything is enqueued on it.
+  {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    const cudaError_t e = cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap);
+    if (e != cudaSuccess) return psc::host::cuda_fail(e, "cudaStreamIsCapturing");
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(PSC_ERR_UNSUPPORTED,
+                  "the allocation-free batch cannot be recorded into a CUDA graph (its staging is "
+                  "shared by all calls); use psc_render_batch with use_graph = 1");
+  }
   if (!psc::host::storage_ready(c))
     return fail(PSC_ERR_MISSING_INPUT,
                 "noise storage for the current options is not built; render once with psc_render or "

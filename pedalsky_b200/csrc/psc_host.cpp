@@ -1598,12 +1598,12 @@ int psc_download_lut(psc_ctx* c, int kind, uint16_t* out, size_t count) {
   return PSC_OK;
 }
 
-int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
-  if (!c || (n && !views)) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
-  const bool rt_form = c->opts.half_res || c->opts.taa;
-  if (rt_form && n != 1)
-    return fail(PSC_ERR_INVALID_ARGUMENT,
-                "the half-res / TAA forms render one view per call (its march, TAA and composite)");
+namespace {
+
+// Input, option and view checks of a march call (psc_render,
+// psc_count_fetches); builds the noise storage form and the texture objects
+// the march reads.
+int prepare_render(psc_ctx* c, const PscView* views, uint32_t n, bool rt_form) {
   if (!c->have_frame) return fail(PSC_ERR_MISSING_INPUT, "psc_set_frame was not called");
   if (!c->have_base || !c->have_detail || !c->have_curl || !c->have_blue)
     return fail(PSC_ERR_MISSING_INPUT, "noise volumes missing (psc_bake_noise or psc_upload_noise)");
@@ -1635,6 +1635,19 @@ int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
     if (rt_form && (v.x_offset || v.y_offset || vw != v.width || vh != v.height))
       return fail(PSC_ERR_INVALID_ARGUMENT, "the half-res / TAA forms render whole viewports");
   }
+  return PSC_OK;
+}
+
+}  // namespace
+
+int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
+  if (!c || (n && !views)) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  const bool rt_form = c->opts.half_res || c->opts.taa;
+  if (rt_form && n != 1)
+    return fail(PSC_ERR_INVALID_ARGUMENT,
+                "the half-res / TAA forms render one view per call (its march, TAA and composite)");
+  int rc = prepare_render(c, views, n, rt_form);
+  if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   ++c->taa[c->active_view].marches;  // a resolve of this march keeps the view's history going
   if (rt_form) return render_rt_view(c, views[0], s);
@@ -1649,6 +1662,44 @@ int psc_render(psc_ctx* c, const PscView* views, uint32_t n, void* stream) {
     rc = launch_view_march(c, u, vd, s);
     if (rc) return rc;
   }
+  return PSC_OK;
+}
+
+int psc_count_fetches(psc_ctx* c, const PscView* view, PscFetchCounts* out, void* stream) {
+  if (!c || !view || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (c->opts.schedule != PSC_SCHED_FAST || c->opts.debug_checks || c->opts.half_res || c->opts.taa)
+    return fail(PSC_ERR_UNSUPPORTED,
+                "fetch counts come from the FAST schedule's full-resolution march (no debug checks, "
+                "half-res or TAA)");
+  int rc = prepare_render(c, view, 1, false);
+  if (rc) return rc;
+  const PscView& v = *view;
+  const uint32_t vw = v.viewport_w ? v.viewport_w : v.width, vh = v.viewport_h ? v.viewport_h : v.height;
+  psc::MarchUniforms u;
+  build_uniforms(c, vw, vh, u);
+  const psc::ViewDev vd{v.width, v.height, v.x_offset, v.y_offset, v.depth,
+                        reinterpret_cast<float4*>(v.out_luminance),
+                        reinterpret_cast<float4*>(v.out_transmittance), reinterpret_cast<float4*>(v.hdr)};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  unsigned long long* d = nullptr;
+  unsigned long long h[psc::kFetchTallyKinds] = {};
+  PSC_CUDA(cudaMalloc(&d, sizeof(h)), "cudaMalloc fetch counters");
+  cudaError_t e = cudaMemsetAsync(d, 0, sizeof(h), s);
+  if (e == cudaSuccess) {
+    rc = psc::launch_march_fast_tally(u, vd, c->opts, d, s);
+    if (rc == PSC_OK) {
+      ++c->launches;
+      e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+  }
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "fetch-count march");
+  if (rc == PSC_ERR_UNSUPPORTED)
+    return fail(rc, "fetch counts cover F16 and U8 storage with exact or hybrid filtering, up to 4 octaves");
+  if (rc) return fail(rc, "fetch-count march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  static_assert(sizeof(PscFetchCounts) == sizeof(h), "PscFetchCounts holds one counter per kind");
+  std::memcpy(out, h, sizeof(h));
   return PSC_OK;
 }
 

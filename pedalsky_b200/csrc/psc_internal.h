@@ -19,6 +19,7 @@
 
 namespace psc {
 
+constexpr uint32_t kFetchTallyKinds = 12;  // counters of PscFetchCounts
 constexpr float kPi = 3.14159265358979f;  // HG_PI, cloud_march.wgsl:71
 
 // Per-layer constants.  Everything here is a pure function of the layer,
@@ -191,6 +192,12 @@ int launch_march(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions
 // does not cover (more than 4 octaves), which the caller serves with PLAIN.
 int launch_march_fast(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
                       cudaStream_t stream);
+// Instrumented FAST march (psc_count_fetches): the kernel of
+// launch_march_fast built to count the fetches it issues into `counts`
+// (kFetchTallyKinds 64-bit counters in PscFetchCounts order, added to).  F16 and U8 storage, exact or
+// hybrid filtering; PSC_ERR_UNSUPPORTED otherwise.
+int launch_march_fast_tally(const MarchUniforms& u, const ViewDev& v, const PscMarchOptions& o,
+                            unsigned long long* counts, cudaStream_t stream);
 int launch_composite(const float4* l, const float4* t, float4* hdr, uint32_t n,
                      cudaStream_t stream);
 // Noise bakes (noise_bake.cu), synchronous on `stream`.

@@ -9,7 +9,11 @@ field, frame uniforms from a `FlyCamera`, and determinism switches as the
 golden harness sets them (wind drift 0, diurnal 0, simulated_seconds 0;
 crates/ps-app/tests/golden.rs:112,119).
 
-All host arithmetic goes through the C ABI helpers of libpsclouds.so.
+All host arithmetic goes through the C ABI helpers of libpsclouds.so by
+default; `host_helpers(h)` swaps in another implementation of the same seven
+helpers (defaults, layer synthesis, camera, weather map, wind field) for the
+duration of a `with` block, which is how a CPU-only caller assembles the same
+scenes without mapping the library.
 Workloads:
   plain_320x180   one Cumulus layer 1500-2300 m, coverage 0.5, 320x180,
                   64/6 steps, 3 octaves, dual-lobe HG 0.8/-0.2 w=0.5
@@ -25,6 +29,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+from contextlib import contextmanager
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -60,10 +65,49 @@ class Scene:
     extra: dict = field(default_factory=dict)
 
 
+class CapiHost:
+    """Scene-assembly host arithmetic through the library's C ABI helpers."""
+
+    def params_default(self, out: capi.CloudParamsGpu) -> None:
+        call("psc_params_default", C.byref(out))
+
+    def world_default(self, out: capi.WorldUniformsGpu) -> None:
+        call("psc_world_default", C.byref(out))
+
+    def options_default(self, out: capi.MarchOptions) -> None:
+        call("psc_options_default", C.byref(out))
+
+    def synthesise_layers(self, descs, n: int, out) -> None:
+        call("psc_synthesise_layers", descs, n, out)
+
+    def frame_from_camera(self, cam, width, height, alt, az, ang, lux, out) -> None:
+        call("psc_frame_from_camera", C.byref(cam), width, height, alt, az, ang, lux, C.byref(out))
+
+    def weather_map(self, n_layers: int, grid, gw: int, gh: int, extent: float, out) -> None:
+        call("psc_synthesise_weather_map", n_layers, 0.0, 0.0, grid, gw, gh, extent, out)
+
+    def wind_field(self, speed: float, dir_deg: float, out) -> None:
+        call("psc_synthesise_wind_field", speed, dir_deg, out)
+
+
+_HOST = CapiHost()
+
+
+@contextmanager
+def host_helpers(helpers):
+    """Assemble scenes with `helpers` (an object with CapiHost's methods)."""
+    global _HOST
+    prev, _HOST = _HOST, helpers
+    try:
+        yield helpers
+    finally:
+        _HOST = prev
+
+
 def default_params() -> capi.CloudParamsGpu:
     """CloudParamsGpu::default() + CloudsTuning::default() as CloudsSubsystem::new applies it."""
     p = capi.CloudParamsGpu()
-    call("psc_params_default", C.byref(p))
+    _HOST.params_default(p)
     p.cloud_steps, p.light_steps, p.multi_scatter_octaves = 192, 6, 4
     p.detail_strength = 0.35       # CloudsTuning::default (config.rs:484)
     p.powder_strength = 1.0
@@ -75,14 +119,14 @@ def default_params() -> capi.CloudParamsGpu:
 
 def world_default() -> capi.WorldUniformsGpu:
     w = capi.WorldUniformsGpu()
-    call("psc_world_default", C.byref(w))
+    _HOST.world_default(w)
     return w
 
 
 def options(phase=capi.PHASE_APPROX_MIE, storage=capi.STORAGE_U8, filt=capi.FILTER_EXACT,
             schedule=capi.SCHED_PLAIN, kahan=0, composite=0) -> capi.MarchOptions:
     o = capi.MarchOptions()
-    call("psc_options_default", C.byref(o))
+    _HOST.options_default(o)
     o.phase_mode, o.storage, o.filter, o.schedule = phase, storage, filt, schedule
     o.kahan, o.composite = kahan, composite
     return o
@@ -97,7 +141,7 @@ def synth_layers(descs: list[tuple]) -> tuple[object, int]:
         dens = d[4] if len(d) > 4 else -1.0
         arr[i] = capi.CloudLayerDesc(t, base, top, cov, dens, 0.0, 0.0, -1.0, -1.0)
     out = (capi.CloudLayerGpu * 8)()
-    call("psc_synthesise_layers", arr, n, out)
+    _HOST.synthesise_layers(arr, n, out)
     return out, n
 
 
@@ -106,8 +150,8 @@ def frame_for(width, height, cam_pos=(0.0, 100.0, 0.0), pitch_deg=10.0, yaw_deg=
     cam = capi.FlyCamera((C.c_float * 3)(*cam_pos), math.radians(pitch_deg), math.radians(yaw_deg),
                          0.0, math.radians(fov_deg), 0.1)
     f = capi.FrameUniformsGpu()
-    call("psc_frame_from_camera", C.byref(cam), width, height, math.radians(sun_alt_deg),
-         math.radians(sun_az_deg), SUN_ANGULAR_RADIUS, TOA_LUX, C.byref(f))
+    _HOST.frame_from_camera(cam, width, height, math.radians(sun_alt_deg), math.radians(sun_az_deg),
+                            SUN_ANGULAR_RADIUS, TOA_LUX, f)
     f.simulated_seconds = sim_seconds
     return f
 
@@ -115,18 +159,17 @@ def frame_for(width, height, cam_pos=(0.0, 100.0, 0.0), pitch_deg=10.0, yaw_deg=
 def reference_weather(n_layers: int, grid: np.ndarray | None = None, grid_extent=32000.0):
     out = np.zeros(128 * 128 * 4, np.uint16)
     if grid is None:
-        call("psc_synthesise_weather_map", n_layers, 0.0, 0.0, None, 0, 0, 0.0, capi.ptr(out))
+        _HOST.weather_map(n_layers, None, 0, 0, 0.0, capi.ptr(out))
     else:
         g = np.ascontiguousarray(grid, np.float32)
-        call("psc_synthesise_weather_map", n_layers, 0.0, 0.0, capi.ptr(g), g.shape[1],
-             g.shape[0], grid_extent, capi.ptr(out))
+        _HOST.weather_map(n_layers, capi.ptr(g), g.shape[1], g.shape[0], grid_extent, capi.ptr(out))
     return out
 
 
 def wind_field(speed=5.0, dir_deg=240.0):
     """Surface::default() wind (scene.rs:217-218) unless given."""
     out = np.zeros(32 * 16 * 32 * 4, np.uint16)
-    call("psc_synthesise_wind_field", speed, dir_deg, capi.ptr(out))
+    _HOST.wind_field(speed, dir_deg, capi.ptr(out))
     return out
 
 
@@ -298,7 +341,7 @@ def mountain_wave_grid(size=2048, seed=0, wavelength_m=8000.0, amplitude=0.3, ex
     return np.clip(0.55 + wave + 0.35 * (vn - 0.5), 0, 1).astype(np.float32)
 
 
-def stress_2160p(width=3840, height=2160, frame_index=0, **kw) -> Scene:
+def stress_2160p(width=3840, height=2160, frame_index=0, host_inputs=True, **kw) -> Scene:
     p = default_params()
     p.cloud_steps, p.light_steps = 256, 8
     p.wind_drift_strength = 1.0
@@ -306,7 +349,8 @@ def stress_2160p(width=3840, height=2160, frame_index=0, **kw) -> Scene:
     frame = frame_for(width, height, sim_seconds=float(frame_index))
     grid = mountain_wave_grid()
     s = _finish("stress_2160p", width, height, p, ln, frame, options(**kw), grid.reshape(-1),
-                2048, 2048, capi.WEATHER_R32F, wind=wind_field(15.0 / 1.0, 240.0))
+                2048, 2048, capi.WEATHER_R32F, wind=wind_field(15.0 / 1.0, 240.0),
+                host_inputs=host_inputs)
     s.extra["frame_index"] = frame_index
     return s
 

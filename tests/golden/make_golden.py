@@ -8,8 +8,10 @@ fetch_counts.json  executed-fetch counts per kind (instrumented FP64 CPU
                    its eight); bench.py turns them into algorithmic bytes
                    per ray.
 plain_96x54.npz    FP64-oracle L/T of the plain workload at 96x54 (float32),
-precision_96x54.npz  and of the three-layer workload; the GPU parity tests
-                   compare against these (they pin the oracle as well).
+precision_96x54.npz  and of the three-layer workload.  The oracle must
+                   reproduce them (tests/test_oracle_goldens.py) and the GPU
+                   benchmark form is compared with them
+                   (tests/test_gpu_fullsize.py::test_committed_goldens).
 """
 from __future__ import annotations
 

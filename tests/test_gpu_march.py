@@ -99,10 +99,15 @@ def test_u8_matches_fp64_oracle(c1, oracle_noise, sched):
 
 
 def test_gpu_baked_inputs_match_oracle_inputs(c1, oracle_noise):
-    """Product path end to end: noise baked on the GPU, same LUT data."""
+    """Product path end to end: noise and the four atmosphere LUTs baked on
+    the GPU, against the FP64 oracle fed with its own CPU bakes."""
     s, luts, ref = c1
-    L, T, hdr = _gpu.render(s, None, luts, composite_bg=s.background)
-    _check("plain_320x180/gpu-noise", hdr, ref)
+    L, T, hdr = _gpu.render(s, None, None, composite_bg=s.background)
+    _check("plain_320x180/gpu-noise-and-luts", hdr, ref)
+    f = scenes.plain_320x180(storage=capi.STORAGE_F16, schedule=capi.SCHED_FAST,
+                             filt=capi.FILTER_HYBRID)
+    L, T, hdr = _gpu.render(f, None, None, composite_bg=s.background, fused=True)
+    _check("plain_320x180/fast/f16/hybrid/gpu-noise-and-luts", hdr, ref)
 
 
 @pytest.mark.parametrize("sched", sorted(SCHEDULES))

@@ -88,3 +88,70 @@ def test_gloo_world_size_two_gather_and_timing():
         assert t == 2.5                       # max over ranks
         assert parts == res[0][3]             # every rank computes the same plan
         assert sorted(i for p in parts for i in p) == list(range(5))
+
+
+def _march_worker(rank, world, port, q):
+    """One gloo rank of the two forward partitions, with the FP64 CPU
+    restatement standing in for the march kernel: a row band of one frame
+    (psc_render's viewport offset does the same on a GPU), all-gathered into
+    the frame, and this rank's share of a cost-partitioned set of views."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import pyoracle
+        from pedalsky_b200 import scenes
+        noise = pyoracle.bake_noise()
+        s = scenes.precision_1080p(64, 37)
+        luts = pyoracle.bake_luts(s.frame, s.world)
+        bands = sharding.row_bands(s.height, world, (s.depth == 0).mean(axis=1) + 0.25)
+        band = bands[rank]
+        L, T = pyoracle.render(s, noise, luts, precision=pyoracle.FP64, threads=2,
+                               rows=(band.y0, band.y1))
+        local = torch.from_numpy(np.concatenate([L, T], axis=-1)[band.y0:band.y1].copy())
+        full = sharding.gather_rows(local, band, bands).numpy()
+        views = scenes.batch_views(5, seed=4, size_scale=0.03)
+        costs = [sharding.view_cost(v.width, v.height, v.params.cloud_steps, v.n_layers)
+                 for v in views]
+        parts = sharding.partition_views(costs, world)
+        mine = {}
+        for i in parts[rank]:
+            v = views[i]
+            lv = pyoracle.bake_luts(v.frame, v.world)
+            Lv, Tv = pyoracle.render(v, noise, lv, precision=pyoracle.FP64, threads=2)
+            mine[i] = np.concatenate([Lv, Tv], axis=-1)
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        q.put((rank, full, {k: v for d in gathered for k, v in d.items()}, parts))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_world_size_two_renders_bands_and_views_like_one_process(oracle, oracle_noise):
+    """Row bands and view partitions over two gloo ranks reassemble the
+    single-process FP64 renders bit for bit (the forward march has no
+    exchange step: every pixel is a function of its own coordinates)."""
+    from pedalsky_b200 import scenes
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_march_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=600) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    s = scenes.precision_1080p(64, 37)
+    luts = oracle.bake_luts(s.frame, s.world)
+    L, T = oracle.render(s, oracle_noise, luts, precision=oracle.FP64)
+    want = np.concatenate([L, T], axis=-1)
+    views = scenes.batch_views(5, seed=4, size_scale=0.03)
+    for rank, full, rendered, parts in res:
+        assert np.array_equal(full, want)
+        assert sorted(rendered) == list(range(5))
+        assert all(len(p) > 0 for p in parts)
+        for i, img in rendered.items():
+            v = views[i]
+            lv = oracle.bake_luts(v.frame, v.world)
+            Lv, Tv = oracle.render(v, oracle_noise, lv, precision=oracle.FP64)
+            assert np.array_equal(img, np.concatenate([Lv, Tv], axis=-1)), i
