@@ -11,18 +11,23 @@
 // aerial perspective is applied.
 //
 // Adjoint: one thread per ray runs the forward march keeping the
-// transmittance at every k-th step (registers/local memory), evaluates its
-// pixel's loss term (I - target)^2 / N with I = L + background * T, then
-// walks the checkpoint segments backwards: each segment is recomputed from
-// its checkpoint (storing per-step transmittance and the primary and light
-// grid sums), then traversed in reverse, carrying the adjoint of the
-// transmittance.  d loss / d density at the primary sample and d loss /
+// transmittance at every k-th step, evaluates its pixel's loss term
+// (I - target)^2 / N with I = L + background * T, then walks the checkpoint
+// segments backwards: each segment is recomputed from its checkpoint,
+// storing per step the light-march grid sum and the prefix sum of the
+// primary grid values within the segment, then traversed in reverse,
+// carrying the adjoint of the transmittance.  The transmittance before a
+// step is the checkpoint's times exp(-sigma_t * step * k * prefix) and the
+// primary grid value is fetched again.  Checkpoints and segment buffers live
+// in dynamic shared memory laid out [slot][thread], so every access is
+// conflict-free and nothing is kept in local memory.  d loss / d density at the primary sample and d loss /
 // d optical depth toward the sun are scattered into the gradient grid with
 // atomic adds over the trilinear weights of the primary sample and of the
 // six light taps.  Loss and d loss / d density_scale are reduced per CTA and
 // added in double.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include "march_fast_body.cuh"
 
@@ -32,8 +37,15 @@ namespace {
 constexpr int kTileW = 16;
 constexpr int kTileH = 8;
 constexpr int kThreads = 128;
+constexpr int kAdjointCtasDefault = 6;  // see adjoint_ctas_per_sm
 constexpr int kMaxCp = 32;   // checkpoints per ray
 constexpr int kMaxSeg = 32;  // steps per checkpoint segment
+
+// Shared-memory words per thread of the adjoint: three transmittances per
+// checkpoint, then a prefix sum and a light sum per step of one segment.
+__host__ __device__ constexpr uint32_t adjoint_words(uint32_t n_cp, uint32_t k_cp) {
+  return 3u * n_cp + 2u * k_cp;
+}
 
 struct Tri {
   int x0, y0, z0;
@@ -195,9 +207,12 @@ __device__ __forceinline__ float source(const MarchUniforms& u, const Light& l, 
   return fmaf(S, E, l.amb[c]);
 }
 
+// `sm` is this thread's column of the adjoint's shared memory (stride
+// kThreads words); unused by the forward form.
 template <bool ADJ>
 __device__ __forceinline__ void grid_pixel(const MarchUniforms& u, const ViewDev& v, const GridDev& g,
-                                           uint32_t px, uint32_t py, float& loss_out, float& dk_out) {
+                                           uint32_t px, uint32_t py, float* sm, float& loss_out,
+                                           float& dk_out) {
   RaySetup rs;
   setup_ray(u, v, px, py, rs);
   const LayerConst& L = u.layers[0];
@@ -239,7 +254,11 @@ __device__ __forceinline__ void grid_pixel(const MarchUniforms& u, const ViewDev
   const float step = hit ? __fdividef(t1 - t0, (float)u.cloud_steps) : 0.0f;
   const uint32_t kcp = g.k_cp;
   uint32_t n_exec = 0;
-  float cp[ADJ ? kMaxCp : 1][3];
+  // shared-memory slots: checkpoint transmittances, then the segment's
+  // prefix sums and light sums
+  float* const s_cp = sm;
+  float* const s_pre = sm + 3u * ((u.cloud_steps + kcp - 1u) / kcp) * kThreads;
+  float* const s_gl = s_pre + kcp * kThreads;
 
   auto position = [&](uint32_t s, float& px3, float& py3, float& pz3, float& alt, float& ux, float& uy,
                       float& uz) {
@@ -258,9 +277,10 @@ __device__ __forceinline__ void grid_pixel(const MarchUniforms& u, const ViewDev
     for (uint32_t s = 0; s < u.cloud_steps; ++s) {
       if constexpr (ADJ) {
         if (s % kcp == 0) {
-          cp[s / kcp][0] = T[0];
-          cp[s / kcp][1] = T[1];
-          cp[s / kcp][2] = T[2];
+          const uint32_t c0 = 3u * (s / kcp) * kThreads;
+          s_cp[c0] = T[0];
+          s_cp[c0 + kThreads] = T[1];
+          s_cp[c0 + 2u * kThreads] = T[2];
         }
       }
       float px3, py3, pz3, alt, ux, uy, uz;
@@ -311,31 +331,31 @@ __device__ __forceinline__ void grid_pixel(const MarchUniforms& u, const ViewDev
   loss_out = loss;
   float dk = 0.0f;
   if (n_exec > 0) {
-    float bT[kMaxSeg][3], bg_[kMaxSeg], bl[kMaxSeg];
+    const float kstep = g.k * step;
     for (int seg = (int)((n_exec - 1) / kcp); seg >= 0; --seg) {
       const uint32_t s0 = (uint32_t)seg * kcp;
       const uint32_t s1 = min(s0 + kcp, n_exec);
-      float Ts[3] = {cp[seg][0], cp[seg][1], cp[seg][2]};
+      float pre = 0.0f;
       for (uint32_t s = s0; s < s1; ++s) {  // recompute the segment
         float px3, py3, pz3, alt, ux, uy, uz;
         position(s, px3, py3, pz3, alt, ux, uy, uz);
         const float gv = grid_fetch(g, grid_coords(g, px3, alt, pz3));
         const float gl = light_sum(u, g, light_geo(u, L, alt, ux, uy, uz), px3, py3, pz3, alt);
-        const uint32_t b = s - s0;
-        bT[b][0] = Ts[0];
-        bT[b][1] = Ts[1];
-        bT[b][2] = Ts[2];
-        bg_[b] = gv;
-        bl[b] = gl;
-        const float rho = g.k * gv;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) Ts[c] *= __expf(-(rho * st[c] * step));
+        const uint32_t b = (s - s0) * kThreads;
+        s_pre[b] = pre;
+        s_gl[b] = gl;
+        pre += gv;
       }
+      const uint32_t c0 = 3u * (uint32_t)seg * kThreads;
+      const float cp3[3] = {s_cp[c0], s_cp[c0 + kThreads], s_cp[c0 + 2u * kThreads]};
       for (uint32_t s = s1; s-- > s0;) {  // reverse
-        const uint32_t b = s - s0;
+        const uint32_t b = (s - s0) * kThreads;
         float px3, py3, pz3, alt, ux, uy, uz;
         position(s, px3, py3, pz3, alt, ux, uy, uz);
-        const float gv = bg_[b], gl = bl[b];
+        const float gv = grid_fetch(g, grid_coords(g, px3, alt, pz3)), gl = s_gl[b];
+        const float p_od = kstep * s_pre[b];  // optical depth per unit sigma_t since the checkpoint
+        const float bT[3] = {cp3[0] * __expf(-st[0] * p_od), cp3[1] * __expf(-st[1] * p_od),
+                             cp3[2] * __expf(-st[2] * p_od)};
         const float rho = g.k * gv, od = g.k * gl;
         Light l;
         lighting(u, L, coef, cb, cos_theta, fwd_gain, px3, pz3, alt, ux, uy, uz, l);
@@ -347,9 +367,9 @@ __device__ __forceinline__ void grid_pixel(const MarchUniforms& u, const ViewDev
           const float x = rho * st[c] * step;
           const float e = __expf(-x), ph = phi_of(x, e);
           const float s_int = rho * ss[c] * X * step * ph;
-          const float gT = gI[c] * bT[b][c];
+          const float gT = gI[c] * bT[c];
           drho = fmaf(gT, ss[c] * X * step * e, drho);
-          drho = fmaf(lam[c] * bT[b][c], -st[c] * step * e, drho);
+          drho = fmaf(lam[c] * bT[c], -st[c] * step * e, drho);
           dod = fmaf(gT * rho * ss[c] * step * ph, dX, dod);
           lam[c] = fmaf(lam[c], e, gI[c] * s_int);
         }
@@ -373,15 +393,18 @@ __device__ __forceinline__ double warp_sum(double x) {
   return x;
 }
 
-template <bool ADJ>
-__global__ void __launch_bounds__(kThreads) k_grid_march(const __grid_constant__ MarchUniforms u,
-                                                         const __grid_constant__ ViewDev v,
-                                                         const __grid_constant__ GridDev g) {
+// MINB: CTAs per SM the register allocation is bounded for (0: unbounded,
+// 96 registers, 5 CTAs per SM).
+template <bool ADJ, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_grid_march(const __grid_constant__ MarchUniforms u,
+                                                               const __grid_constant__ ViewDev v,
+                                                               const __grid_constant__ GridDev g) {
+  extern __shared__ float s_adj[];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t px = blockIdx.x * kTileW + (warp & 1u) * 8u + (lane & 7u);
   const uint32_t py = blockIdx.y * kTileH + (warp >> 1) * 4u + (lane >> 3);
   float loss = 0.0f, dk = 0.0f;
-  if (px < v.width && py < v.height) grid_pixel<ADJ>(u, v, g, px, py, loss, dk);
+  if (px < v.width && py < v.height) grid_pixel<ADJ>(u, v, g, px, py, s_adj + threadIdx.x, loss, dk);
   if (!ADJ) return;
   __shared__ double s_red[2][kThreads / 32];
   const double ls = warp_sum((double)loss), ks = warp_sum((double)dk);
@@ -402,6 +425,29 @@ __global__ void __launch_bounds__(kThreads) k_grid_march(const __grid_constant__
   }
 }
 
+// The adjoint's CTAs per SM: PSC_ADJOINT_CTAS_PER_SM (5, 6 or 8) overrides
+// the measured default, read once per process.
+int adjoint_ctas_per_sm() {
+  static const int n = [] {
+    const char* e = getenv("PSC_ADJOINT_CTAS_PER_SM");
+    const int v = e ? atoi(e) : 0;
+    return (v == 5 || v == 6 || v == 8) ? v : kAdjointCtasDefault;
+  }();
+  return n;
+}
+
+template <int MINB>
+cudaError_t launch_adjoint(const MarchUniforms& u, const ViewDev& v, const GridDev& g, dim3 grid,
+                           size_t smem, cudaStream_t s) {
+  if (smem > 48u * 1024u) {
+    const cudaError_t e = cudaFuncSetAttribute(k_grid_march<true, MINB>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_grid_march<true, MINB><<<grid, kThreads, smem, s>>>(u, v, g);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g, bool adjoint,
@@ -411,10 +457,17 @@ int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g
                   (u.cloud_steps + g.k_cp - 1) / g.k_cp > (uint32_t)kMaxCp))
     return PSC_ERR_INVALID_ARGUMENT;
   const dim3 grid((v.width + kTileW - 1) / kTileW, (v.height + kTileH - 1) / kTileH);
-  if (adjoint)
-    k_grid_march<true><<<grid, kThreads, 0, s>>>(u, v, g);
-  else
-    k_grid_march<false><<<grid, kThreads, 0, s>>>(u, v, g);
+  if (adjoint) {
+    // at most 3 x 32 + 2 x 32 words per thread (80 KiB per CTA)
+    const uint32_t n_cp = (u.cloud_steps + g.k_cp - 1) / g.k_cp;
+    const size_t smem = (size_t)adjoint_words(n_cp, g.k_cp) * kThreads * sizeof(float);
+    const int ctas = adjoint_ctas_per_sm();
+    const cudaError_t e = ctas == 8   ? launch_adjoint<8>(u, v, g, grid, smem, s)
+                          : ctas == 6 ? launch_adjoint<6>(u, v, g, grid, smem, s)
+                                      : launch_adjoint<0>(u, v, g, grid, smem, s);
+    return e == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+  }
+  k_grid_march<false, 0><<<grid, kThreads, 0, s>>>(u, v, g);
   return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
 }
 
