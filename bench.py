@@ -279,10 +279,12 @@ def fetched_bytes_per_ray(counts: dict, storage: str, schedule: str = "fast") ->
              + counts["transmittance_taps"] * sz["trans"] + counts["skyview_taps"] * sz["sky"]
              + counts["ap_taps"] * sz["ap"] + counts["depth_loads"] * sz["depth"]
              + counts["rays"] * (sz["blue"] + sz["output"]))
+    passes = max(counts.get("dense_warp_passes", 0), 1)
     return {"bytes_per_ray": total / n, "steps_per_ray": counts["primary_steps"] / n,
             "live_steps_per_ray": counts["live_steps"] / n,
             "dense_per_ray": counts["dense_samples"] / n,
-            "light_fetches_per_ray": counts["light_taps"] / n}
+            "light_fetches_per_ray": counts["light_taps"] / n,
+            "dense_body_simt_efficiency": counts.get("dense_warp_lanes", 0) / (32.0 * passes)}
 
 
 def fetch_peaks(device: int) -> dict:
@@ -562,7 +564,8 @@ def leg_batch64(B: Bench, storage, filt, n_views=64):
         b = Bt.Batch(mine, B.dev)
         with B.torch.cuda.stream(B.stream):
             tune = Bt.autotune(sub.handle, b, reps=1, stream=B.stream)
-        Bt.set_tuning(sub.handle, tune["threads"], tune["tile_w"], use_graph=1)
+        Bt.set_tuning(sub.handle, tune["threads"], tune["tile_w"], use_graph=1,
+                      form=tune["form_id"])
         l0 = sub.launch_count()
     clk = ClockSampler(B.ranks.local)
     ms, ms_max = B.timed((lambda: b.render(sub.handle, B.stream)) if mine else (lambda: None),
@@ -820,7 +823,8 @@ def run_frames(args, ranks: Ranks):
         bt = Bt.Batch(frames, dev)
         with torch.cuda.stream(stream):
             btune = Bt.autotune(sub.handle, bt, reps=1, stream=stream)
-        Bt.set_tuning(sub.handle, btune["threads"], btune["tile_w"], use_graph=1)
+        Bt.set_tuning(sub.handle, btune["threads"], btune["tile_w"], use_graph=1,
+                      form=btune["form_id"])
         _, ms_b = B.timed(lambda: bt.render(sub.handle, stream), pre=bt.reset_hdr)
         batched = {"value": ranks.world * rays_step / (ms_b * 1e-3) / 1e6, "ms_per_step": ms_b,
                    "config": "psc_render_batch: persistent kernel from a captured CUDA graph, "

@@ -459,7 +459,7 @@ int psc_composite(const float* luminance, const float* transmittance,
  * psc_render for this view) and counts as it goes; the timed kernels carry
  * no counters.  Options: FAST schedule, F16 or U8 storage, exact or hybrid
  * filtering, no debug checks, half-res or TAA; else PSC_ERR_UNSUPPORTED.
- * Synchronous; allocates and frees a 96-byte counter buffer. */
+ * Synchronous; allocates and frees a 112-byte counter buffer. */
 typedef struct PscFetchCounts {
   uint64_t rays;                /* pixels marched                          */
   uint64_t primary_steps;       /* primary steps executed                  */
@@ -474,6 +474,10 @@ typedef struct PscFetchCounts {
   uint64_t skyview_taps;        /* sky-view LUT taps                       */
   uint64_t ap_taps;             /* aerial-perspective taps                 */
   uint64_t depth_loads;         /* depth-buffer loads                      */
+  uint64_t dense_warp_passes;   /* warp passes through the dense-sample
+                                   body (LUTs, light march, octaves)        */
+  uint64_t dense_warp_lanes;    /* lanes active in those passes: / (32 x
+                                   passes) is the body's SIMT efficiency    */
 } PscFetchCounts;
 int psc_count_fetches(psc_ctx* ctx, const PscView* view, PscFetchCounts* out, void* stream);
 
@@ -504,15 +508,29 @@ typedef struct PscBatchView {
   float* hdr;                   /* device; composited when options.composite */
 } PscBatchView;
 
-/* Launch shape of the persistent batched kernel. */
+/* Launch shape of the batched march. */
 typedef struct PscBatchTuning {
-  uint32_t threads;    /* CTA size: 64, 128 or 256                          */
+  uint32_t threads;    /* CTA size: 64, 128 or 256 (form 0)                 */
   uint32_t tile_w;     /* tile width in pixels, a multiple of 8 dividing
-                          threads/4; tile height = threads/32/(tile_w/8)*4 */
+                          threads/4; tile height = threads/32/(tile_w/8)*4
+                          (form 0)                                          */
   uint32_t use_graph;  /* 1: capture the batch once as a CUDA graph and
-                          relaunch it while the batch shape is unchanged    */
-  uint32_t _reserved;
+                          relaunch it while the batch is unchanged          */
+  uint32_t form;       /* PSC_BATCH_PERSISTENT or PSC_BATCH_PER_VIEW        */
 } PscBatchTuning;
+
+enum {
+  /* One persistent kernel for the whole batch: CTAs sized to the SMs'
+   * resident capacity pull pixel tiles of all views, in descending cost,
+   * from one atomic counter; each view's uniform block is copied to shared
+   * memory when a CTA moves to that view. */
+  PSC_BATCH_PERSISTENT = 0,
+  /* One single-view FAST kernel per view with its uniforms as constant-bank
+   * kernel parameters, enqueued in descending cost on parallel branch
+   * streams, so the views run concurrently and the block scheduler balances
+   * them; with use_graph the branches are one captured CUDA graph. */
+  PSC_BATCH_PER_VIEW = 1
+};
 
 int psc_set_batch_tuning(psc_ctx* ctx, const PscBatchTuning* tuning);
 int psc_get_batch_tuning(psc_ctx* ctx, PscBatchTuning* out);
@@ -524,8 +542,9 @@ int psc_get_batch_tuning(psc_ctx* ctx, PscBatchTuning* out);
 int psc_render_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, void* stream);
 
 /* Time every candidate launch shape on this batch (`reps` timed runs each,
- * after one warm-up), keep the fastest in the context and return it with
- * its median time in milliseconds.  Synchronous. */
+ * after one warm-up): the persistent form at each CTA size and tile width,
+ * and the per-view form.  Keeps the fastest in the context and returns it
+ * with its median time in milliseconds.  Synchronous. */
 int psc_autotune_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, uint32_t reps,
                        PscBatchTuning* best, float* best_ms, void* stream);
 

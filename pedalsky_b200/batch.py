@@ -61,8 +61,8 @@ class Batch:
              C.c_void_p(stream.cuda_stream if stream is not None else None))
 
 
-def set_tuning(handle, threads=128, tile_w=16, use_graph=0):
-    t = capi.BatchTuning(threads, tile_w, use_graph, 0)
+def set_tuning(handle, threads=128, tile_w=16, use_graph=0, form=capi.BATCH_PERSISTENT):
+    t = capi.BatchTuning(threads, tile_w, use_graph, form)
     call("psc_set_batch_tuning", handle, C.byref(t))
 
 
@@ -71,5 +71,6 @@ def autotune(handle, batch: Batch, reps=3, stream=None):
     ms = C.c_float()
     call("psc_autotune_batch", handle, batch.arr, len(batch.views), reps, C.byref(best),
          C.byref(ms), C.c_void_p(stream.cuda_stream if stream is not None else None))
-    return {"threads": best.threads, "tile_w": best.tile_w,
+    return {"form": "per_view" if best.form == capi.BATCH_PER_VIEW else "persistent",
+            "form_id": best.form, "threads": best.threads, "tile_w": best.tile_w,
             "tile_h": best.threads // 32 // (best.tile_w // 8) * 4, "ms": ms.value}

@@ -136,8 +136,11 @@ class BatchView(C.Structure):
     ]
 
 
+BATCH_PERSISTENT, BATCH_PER_VIEW = 0, 1
+
+
 class BatchTuning(C.Structure):
-    _fields_ = [("threads", u32), ("tile_w", u32), ("use_graph", u32), ("_reserved", u32)]
+    _fields_ = [("threads", u32), ("tile_w", u32), ("use_graph", u32), ("form", u32)]
 
 
 class DensityGrid(C.Structure):
@@ -160,7 +163,7 @@ class FetchCounts(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "rays", "primary_steps", "live_steps", "weather_taps", "type_loads", "detail_taps",
         "dense_samples", "light_taps", "transmittance_taps", "skyview_taps", "ap_taps",
-        "depth_loads")]
+        "depth_loads", "dense_warp_passes", "dense_warp_lanes")]
 
     def as_dict(self) -> dict:
         return {n: int(getattr(self, n)) for n, _ in self._fields_}

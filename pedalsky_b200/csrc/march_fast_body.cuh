@@ -657,9 +657,13 @@ constexpr uint32_t kAuxWords = kMaxOct + 6 + 5;
 
 // Fetch tally of the instrumented build (TALLY = true): per ray, the
 // fetches march_pixel_fast issues, by kind, in the order of PscFetchCounts.
+// The last two count, for the dense-sample body (LUT lookups, light march,
+// octaves, radiance), the warp passes through it and the lanes active in
+// them: their ratio over 32 is the body's SIMT efficiency.
 enum TallyKind : uint32_t {
   kTallyRays, kTallySteps, kTallyLive, kTallyWeather, kTallyType, kTallyDetail, kTallyDense,
-  kTallyLight, kTallyTrans, kTallySky, kTallyAp, kTallyDepth, kTallyKinds
+  kTallyLight, kTallyTrans, kTallySky, kTallyAp, kTallyDepth, kTallyDensePasses, kTallyDenseLanes,
+  kTallyKinds
 };
 static_assert(kTallyKinds == kFetchTallyKinds, "one tally counter per PscFetchCounts field");
 
@@ -814,6 +818,11 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             float3 ts, sky;
             [[maybe_unused]] const bool trans_fetched = lut_lookups(u, alt, ux, uy, uz, ts, sky);
             if constexpr (TALLY) {
+              const uint32_t act = __activemask();
+              if ((threadIdx.x & 31u) == (uint32_t)__ffs(act) - 1u) {
+                ++tc[kTallyDensePasses];
+                tc[kTallyDenseLanes] += (uint32_t)__popc(act);
+              }
               ++tc[kTallyDense];
               ++tc[kTallySky];
               tc[kTallyTrans] += trans_fetched ? 1u : 0u;

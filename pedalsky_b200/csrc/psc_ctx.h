@@ -106,6 +106,14 @@ struct psc_ctx {
   cudaStream_t batch_stream = nullptr;  // capture stream
   cudaGraphExec_t batch_exec = nullptr;
   std::vector<uint64_t> batch_key;
+  // per-view form (PscBatchTuning.form = 1): the views in descending
+  // estimated cost, and the branch streams and fork/join events the views'
+  // kernels are enqueued on (parallel branches of the captured graph)
+  std::vector<uint32_t> batch_order;
+  static constexpr int kBranches = 8;
+  cudaStream_t batch_branch[kBranches] = {};
+  cudaEvent_t batch_fork = nullptr;
+  cudaEvent_t batch_join[kBranches] = {};
   int sms = 0;
 };
 

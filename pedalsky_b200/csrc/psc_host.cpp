@@ -472,6 +472,14 @@ void release_batch(psc_ctx* c) {
   if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
   c->batch_exec = nullptr;
   c->batch_key.clear();
+  for (int j = 0; j < psc_ctx::kBranches; ++j) {
+    if (c->batch_branch[j]) cudaStreamDestroy(c->batch_branch[j]);
+    if (c->batch_join[j]) cudaEventDestroy(c->batch_join[j]);
+    c->batch_branch[j] = nullptr;
+    c->batch_join[j] = nullptr;
+  }
+  if (c->batch_fork) cudaEventDestroy(c->batch_fork);
+  c->batch_fork = nullptr;
   if (c->batch_stream) cudaStreamDestroy(c->batch_stream);
   if (c->batch_staged) cudaEventDestroy(c->batch_staged);
   c->batch_stream = nullptr;
@@ -542,6 +550,8 @@ int reserve_batch(psc_ctx* c, uint32_t views, uint32_t tiles) {
 }
 
 int validate_tuning(const PscBatchTuning& t) {
+  if (t.form != PSC_BATCH_PERSISTENT && t.form != PSC_BATCH_PER_VIEW)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "batch form must be PSC_BATCH_PERSISTENT or PSC_BATCH_PER_VIEW");
   if (t.threads != 64 && t.threads != 128 && t.threads != 256)
     return fail(PSC_ERR_INVALID_ARGUMENT, "batch threads must be 64, 128 or 256 (got %u)", t.threads);
   const uint32_t warps = t.threads / 32;
@@ -570,9 +580,10 @@ void build_batch_view_uniforms(const psc_ctx* c, const PscBatchView& bv, float4*
 
 int stage_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32_t* n_tiles_out) {
   const PscBatchTuning& tu = c->batch_tuning;
+  const bool per_view = tu.form == PSC_BATCH_PER_VIEW;
   const uint32_t tile_w = tu.tile_w, tile_h = (tu.threads / 32 / (tu.tile_w / 8)) * 4;
   uint64_t total = 0;
-  for (uint32_t i = 0; i < n; ++i) {
+  for (uint32_t i = 0; i < n && !per_view; ++i) {
     const uint64_t tx = (views[i].width + tile_w - 1) / tile_w, ty = (views[i].height + tile_h - 1) / tile_h;
     if (tx > 4096 || ty > 4096) return fail(PSC_ERR_INVALID_ARGUMENT, "view %u has too many tiles", i);
     total += tx * ty;
@@ -602,14 +613,57 @@ int stage_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32_t* n_t
     if (ca != cb) return ca > cb;
     return (uint64_t)views[a].width * views[a].height > (uint64_t)views[b].width * views[b].height;
   });
+  c->batch_order = order;
   uint32_t k = 0;
   for (uint32_t i : order) {
+    if (per_view) break;
     const uint32_t tx = (views[i].width + tile_w - 1) / tile_w, ty = (views[i].height + tile_h - 1) / tile_h;
     for (uint32_t y = 0; y < ty; ++y)
       for (uint32_t x = 0; x < tx; ++x) c->h_btiles[k++] = (i << 24) | (x << 12) | y;
   }
   *n_tiles_out = k;
   return PSC_OK;
+}
+
+// The per-view form on `s`: frame records H2D, the per-view LUT bakes, then
+// one FAST kernel per view (uniforms by value) in descending cost on the
+// branch streams, forked from and joined back into `s`.
+int enqueue_batch_per_view(psc_ctx* c, uint32_t n, cudaStream_t s, bool capturing) {
+  if (!c->batch_fork) {
+    PSC_CUDA(cudaEventCreateWithFlags(&c->batch_fork, cudaEventDisableTiming), "batch fork event");
+    for (int j = 0; j < psc_ctx::kBranches; ++j) {
+      PSC_CUDA(cudaStreamCreateWithFlags(&c->batch_branch[j], cudaStreamNonBlocking), "batch branch stream");
+      PSC_CUDA(cudaEventCreateWithFlags(&c->batch_join[j], cudaEventDisableTiming), "batch join event");
+    }
+  }
+  const size_t fl = psc::frame_lite_size();
+  PSC_CUDA(cudaMemcpyAsync(c->d_bframes, c->h_bframes, n * fl, cudaMemcpyHostToDevice, s), "batch frames H2D");
+  PSC_CUDA(cudaEventRecordWithFlags(c->batch_staged, s, capturing ? cudaEventRecordExternal : 0),
+           "batch event");
+  if (psc::launch_view_lut_bakes(c->world, c->d_bframes, n, c->d_lut_h[PSC_LUT_TRANSMITTANCE],
+                                 c->d_lut_h[PSC_LUT_MULTISCATTER], c->d_bsky, c->d_bap, s))
+    return fail(PSC_ERR_CUDA, "per-view LUT bake launch failed");
+  const uint32_t nb = std::min<uint32_t>(n, (uint32_t)psc_ctx::kBranches);
+  PSC_CUDA(cudaEventRecord(c->batch_fork, s), "batch fork");
+  for (uint32_t j = 0; j < nb; ++j)
+    PSC_CUDA(cudaStreamWaitEvent(c->batch_branch[j], c->batch_fork, 0), "batch fork wait");
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t i = c->batch_order[k];
+    int rc = psc::launch_march_fast(c->h_bu[i], c->h_bv[i], c->opts, c->batch_branch[k % nb]);
+    if (rc == PSC_ERR_UNSUPPORTED) rc = psc::launch_march(c->h_bu[i], c->h_bv[i], c->opts, c->batch_branch[k % nb]);
+    if (rc) return fail(rc, "per-view march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  for (uint32_t j = 0; j < nb; ++j) {
+    PSC_CUDA(cudaEventRecord(c->batch_join[j], c->batch_branch[j]), "batch join");
+    PSC_CUDA(cudaStreamWaitEvent(s, c->batch_join[j], 0), "batch join wait");
+  }
+  return PSC_OK;
+}
+
+uint64_t fnv1a(const void* p, size_t n, uint64_t h = 1469598103934665603ull) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  return h;
 }
 
 // Copies, per-view LUT bakes, counter reset and the persistent march on `s`.
@@ -1826,40 +1880,66 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
   rc = stage_batch(c, views, n, &n_tiles);
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool per_view = c->batch_tuning.form == PSC_BATCH_PER_VIEW;
+  const uint64_t marches = per_view ? n : 1;  // march-kernel launches per call
+  auto enqueue = [&](cudaStream_t st, bool capturing) {
+    return per_view ? enqueue_batch_per_view(c, n, st, capturing) : enqueue_batch(c, n, n_tiles, st, capturing);
+  };
   if (!c->batch_tuning.use_graph) {
-    rc = enqueue_batch(c, n, n_tiles, s, false);
+    rc = enqueue(s, false);
     if (rc) return rc;
-    ++c->launches;
+    c->launches += marches;
     return PSC_OK;
   }
   // Graph path: the key is everything the captured nodes bake in (buffer
-  // pointers, sizes, options, launch shape, the full or lean kernel form);
-  // uniforms are read from the pinned staging at launch
-  // time and may change freely within that form.
-  std::vector<uint64_t> key = {n, n_tiles, c->batch_tuning.threads, c->batch_tuning.tile_w,
-                               c->opts.storage, c->opts.filter, c->opts.composite,
+  // pointers, sizes, options, launch shape, the full or lean kernel form).
+  // The persistent form reads its uniforms from the pinned staging at launch
+  // time, so they may change freely within that form; the per-view form
+  // bakes each view's uniforms into its kernel node, so their bytes are part
+  // of its key, and a change of them alone updates the instantiated graph in
+  // place (cudaGraphExecUpdate) instead of instantiating a new one.
+  std::vector<uint64_t> key = {c->batch_tuning.form, n, n_tiles, c->batch_tuning.threads,
+                               c->batch_tuning.tile_w, c->opts.storage, c->opts.filter, c->opts.composite,
                                (uint64_t)(uintptr_t)c->d_bu, (uint64_t)(uintptr_t)c->d_btiles,
+                               (uint64_t)(uintptr_t)c->d_bframes,
                                (uint64_t)(uintptr_t)c->d_base_store, (uint64_t)c->tex_base,
                                (uint64_t)psc::needs_full_paths(c->h_bu, n)};
+  if (per_view) {
+    key.push_back(fnv1a(c->h_bu, n * sizeof(psc::MarchUniforms)));
+    key.push_back(fnv1a(c->h_bv, n * sizeof(psc::ViewDev)));
+  }
   if (!c->batch_exec || key != c->batch_key) {
-    if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
-    c->batch_exec = nullptr;
     cudaGraph_t g = nullptr;
     PSC_CUDA(cudaStreamBeginCapture(c->batch_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    rc = enqueue_batch(c, n, n_tiles, c->batch_stream, true);
+    rc = enqueue(c->batch_stream, true);
     const cudaError_t ce = cudaStreamEndCapture(c->batch_stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
       return rc;
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "end capture");
-    const cudaError_t ie = cudaGraphInstantiate(&c->batch_exec, g, 0);
+    const bool same_shape = c->batch_exec && c->batch_key.size() == key.size() &&
+                            std::equal(key.begin(), key.end() - (per_view ? 2 : 0), c->batch_key.begin());
+    bool updated = false;
+    if (same_shape) {
+      cudaGraphExecUpdateResultInfo info;
+      updated = cudaGraphExecUpdate(c->batch_exec, g, &info) == cudaSuccess;
+      if (!updated) cudaGetLastError();  // clear the failed update's error
+    }
+    if (!updated) {
+      if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+      c->batch_exec = nullptr;
+      const cudaError_t ie = cudaGraphInstantiate(&c->batch_exec, g, 0);
+      if (ie != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(ie, "graph instantiate");
+      }
+    }
     cudaGraphDestroy(g);
-    if (ie != cudaSuccess) return cuda_fail(ie, "graph instantiate");
     c->batch_key = key;
   }
   PSC_CUDA(cudaGraphLaunch(c->batch_exec, s), "graph launch");
-  ++c->launches;
+  c->launches += marches;
   return PSC_OK;
 }
 
@@ -1868,8 +1948,13 @@ int psc_autotune_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32
   if (!c || !views || !n) return fail(PSC_ERR_INVALID_ARGUMENT, "null or empty batch");
   if (reps == 0 || reps > 100) return fail(PSC_ERR_INVALID_ARGUMENT, "reps must be 1..100");
   const PscBatchTuning saved = c->batch_tuning;
-  static const uint32_t cand[][2] = {{128, 16}, {128, 32}, {128, 8}, {256, 16}, {256, 32},
-                                     {256, 64}, {64, 8}, {64, 16}};
+  // {form, threads, tile_w}: the persistent form at each launch shape, and
+  // the per-view form (whose kernels have their own fixed shape)
+  static const uint32_t cand[][3] = {{PSC_BATCH_PERSISTENT, 128, 16}, {PSC_BATCH_PERSISTENT, 128, 32},
+                                     {PSC_BATCH_PERSISTENT, 128, 8},  {PSC_BATCH_PERSISTENT, 256, 16},
+                                     {PSC_BATCH_PERSISTENT, 256, 32}, {PSC_BATCH_PERSISTENT, 256, 64},
+                                     {PSC_BATCH_PERSISTENT, 64, 8},   {PSC_BATCH_PERSISTENT, 64, 16},
+                                     {PSC_BATCH_PER_VIEW, 128, 16}};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaEvent_t a = nullptr, b = nullptr;
   PSC_CUDA(cudaEventCreate(&a), "event");
@@ -1878,7 +1963,7 @@ int psc_autotune_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32
   PscBatchTuning best_tu = saved;
   int rc = PSC_OK;
   for (const auto& cd : cand) {
-    c->batch_tuning = PscBatchTuning{cd[0], cd[1], 0, 0};
+    c->batch_tuning = PscBatchTuning{cd[1], cd[2], 0, cd[0]};
     rc = psc_render_batch(c, views, n, stream);  // warm-up
     if (rc) break;
     std::vector<float> ts;

@@ -19,7 +19,7 @@
 
 namespace psc {
 
-constexpr uint32_t kFetchTallyKinds = 12;  // counters of PscFetchCounts
+constexpr uint32_t kFetchTallyKinds = 14;  // counters of PscFetchCounts
 constexpr float kPi = 3.14159265358979f;  // HG_PI, cloud_march.wgsl:71
 
 // Per-layer constants.  Everything here is a pure function of the layer,

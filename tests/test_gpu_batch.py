@@ -38,7 +38,7 @@ def small_batch():
                               filt=capi.FILTER_HYBRID)
 
 
-def _run_batch(views, noise, tuning=(128, 16, 0), reps=1):
+def _run_batch(views, noise, tuning=(128, 16, 0, 0), reps=1):
     torch = _gpu.torch_cuda()
     sub = subsystem_for_scene(views[0], luts=None, noise=noise)
     b = B.Batch(views, "cuda:0", outputs=("luminance", "transmittance"))
@@ -102,15 +102,53 @@ def test_graph_replay_equals_eager_and_follows_camera_changes(small_batch, oracl
     sub.close()
 
 
+@pytest.mark.parametrize("use_graph", [0, 1])
+def test_per_view_form_matches_single_view_renders(small_batch, oracle_noise, use_graph):
+    """PSC_BATCH_PER_VIEW: one single-view kernel per view on parallel
+    branches (a captured graph with use_graph)."""
+    got = _run_batch(small_batch, oracle_noise, (128, 16, use_graph, capi.BATCH_PER_VIEW), reps=2)
+    _compare(small_batch, got, oracle_noise)
+    persistent = _run_batch(small_batch, oracle_noise)
+    for (a, b), (c, d) in zip(got, persistent):
+        assert np.array_equal(b, d)  # transmittance: the same density path
+
+
+def test_per_view_graph_follows_uniform_changes(small_batch, oracle_noise):
+    """The per-view form bakes each view's uniforms into its graph node: a
+    changed view updates the instantiated graph before the launch."""
+    torch = _gpu.torch_cuda()
+    sub = subsystem_for_scene(small_batch[0], luts=None, noise=oracle_noise)
+    b = B.Batch(small_batch, "cuda:0", outputs=("luminance", "transmittance"))
+    B.set_tuning(sub.handle, 128, 16, 1, capi.BATCH_PER_VIEW)
+    b.render(sub.handle)
+    torch.cuda.synchronize()
+    first = b.lum[1].cpu().numpy().copy()
+    f = scenes.frame_for(small_batch[1].width, small_batch[1].height, sun_alt_deg=8.0)
+    b.arr[1].frame = f
+    b.render(sub.handle)
+    torch.cuda.synchronize()
+    moved = b.lum[1].cpu().numpy().copy()
+    assert not np.array_equal(first, moved)
+    B.set_tuning(sub.handle, 128, 16, 0, capi.BATCH_PER_VIEW)  # eager, same batch
+    b.render(sub.handle)
+    torch.cuda.synchronize()
+    assert np.array_equal(moved, b.lum[1].cpu().numpy())
+    n0 = sub.launch_count()
+    b.render(sub.handle)
+    assert sub.launch_count() - n0 == len(small_batch)  # one march kernel per view
+    sub.close()
+
+
 def test_autotuner_picks_a_valid_shape(small_batch, oracle_noise):
     _gpu.torch_cuda()
     sub = subsystem_for_scene(small_batch[0], luts=None, noise=oracle_noise)
     b = B.Batch(small_batch, "cuda:0", outputs=("luminance",))
     res = B.autotune(sub.handle, b, reps=1)
     assert res["threads"] in (64, 128, 256) and res["ms"] > 0
+    assert res["form"] in ("persistent", "per_view")
     t = capi.BatchTuning()
     call("psc_get_batch_tuning", sub.handle, C.byref(t))
-    assert (t.threads, t.tile_w) == (res["threads"], res["tile_w"])
+    assert (t.threads, t.tile_w, t.form) == (res["threads"], res["tile_w"], res["form_id"])
     sub.close()
 
 
@@ -122,6 +160,8 @@ def test_batch_argument_errors(small_batch, oracle_noise):
         call("psc_set_batch_tuning", sub.handle, C.byref(capi.BatchTuning(96, 16, 0, 0)))
     with pytest.raises(PscError):
         call("psc_set_batch_tuning", sub.handle, C.byref(capi.BatchTuning(128, 24, 0, 0)))
+    with pytest.raises(PscError):  # unknown form
+        call("psc_set_batch_tuning", sub.handle, C.byref(capi.BatchTuning(128, 16, 0, 7)))
     b.arr[0].n_layers = 9
     with pytest.raises(PscError):
         b.render(sub.handle)

@@ -65,6 +65,10 @@ def test_fetch_counts_match_the_timed_kernel_and_the_oracle(oracle, oracle_noise
     assert c["skyview_taps"] == c["dense_samples"]
     assert c["transmittance_taps"] <= c["dense_samples"]
     assert abs(c["ap_taps"] - oc["ap"]) <= 1e-3 * max(oc["ap"], 1) + 2
+    # every dense lane is counted in exactly one warp pass through the body
+    assert c["dense_warp_lanes"] == c["dense_samples"]
+    assert 0 < c["dense_warp_passes"] <= c["dense_samples"]
+    print(f"  dense-body SIMT efficiency {c['dense_warp_lanes'] / (32 * c['dense_warp_passes']):.3f}")
 
 
 def test_fetch_counts_reject_unsupported_forms(oracle_noise):
