@@ -597,6 +597,25 @@ int psc_adjoint(psc_ctx* ctx, const PscDensityGrid* grid, const PscView* view,
                 const float* background, const float* target, float* grad_values,
                 double* grad_density_scale, double* loss, void* stream);
 
+/* Gradient of the same loss as psc_adjoint with respect to the layer's
+ * altitude range: grad_base_top[0] += d loss / d base_m and
+ * grad_base_top[1] += d loss / d top_m of layer 0 (device doubles).  No
+ * counterpart in the reference.  In the grid form the layer's base and top
+ * place the ray's entry and exit (the spheres at planet radius + base and +
+ * top), spread the primary samples over that interval, stretch the grid's
+ * altitude axis over base..top, end the light path at the top and set the
+ * ambient height gradient; the derivative follows all of them (forward
+ * mode, FP32, per ray, summed in double).  The layer's other parameters do
+ * not enter the grid form, whose grid replaces the procedural density they
+ * shape; d loss / d density_scale comes from psc_adjoint.  LUTs are read
+ * with FP32 bilinear weights here whatever the filtering option.  Not for a
+ * Cumulonimbus layer under the approx-Mie phase (its droplet size varies
+ * with height): PSC_ERR_UNSUPPORTED.  Rows of one viewport add up as in
+ * psc_adjoint. */
+int psc_layer_gradient(psc_ctx* ctx, const PscDensityGrid* grid, const PscView* view,
+                       const float* background, const float* target, double* grad_base_top,
+                       void* stream);
+
 /* ------------------------------------------------ allocation-free batch */
 
 #define PSC_NOALLOC_MAX_VIEWS 64u

@@ -29,6 +29,7 @@ CUDA_UNITS = {
     "march_batch.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "march_noalloc.cu": [],
     "grid_march.cu": ["-prec-div=false", "-prec-sqrt=false"],
+    "grid_layer_grad.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
     "fetch_peak.cu": [],

@@ -2108,6 +2108,32 @@ int psc_adjoint(psc_ctx* c, const PscDensityGrid* g, const PscView* v, const flo
   return PSC_OK;
 }
 
+int psc_layer_gradient(psc_ctx* c, const PscDensityGrid* g, const PscView* v, const float* background,
+                       const float* target, double* grad_base_top, void* stream) {
+  if (!background || !target || !grad_base_top) return fail(PSC_ERR_INVALID_ARGUMENT, "null gradient buffer");
+  psc::MarchUniforms u;
+  psc::ViewDev vd;
+  psc::GridDev gd;
+  int rc = prepare_grid(c, g, v, true, u, vd, gd);
+  if (rc) return rc;
+  const psc::LayerConst& L = u.layers[0];
+  if (L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE)
+    return fail(PSC_ERR_UNSUPPORTED,
+                "the layer gradient covers height-independent phase (not the Cumulonimbus droplet blend)");
+  if (!(L.top_m - L.base_m > 1.0f))
+    return fail(PSC_ERR_INVALID_ARGUMENT, "the layer must be more than 1 m thick for its range gradient");
+  // the tangent march reads both LUTs with FP32 bilinear weights, the form
+  // whose derivatives it carries
+  u.tex_trans = 0;
+  u.tex_sky = 0;
+  gd.bg = reinterpret_cast<const float4*>(background);
+  gd.target = reinterpret_cast<const float4*>(target);
+  rc = psc::launch_grid_layer_grad(u, vd, gd, grad_base_top, static_cast<cudaStream_t>(stream));
+  if (rc) return fail(rc, "layer-gradient launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  ++c->launches;
+  return PSC_OK;
+}
+
 int psc_launch_count(psc_ctx* c, uint64_t* out) {
   if (!c || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
   *out = c->launches;

@@ -163,6 +163,10 @@ struct GridDev {
 };
 int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g, bool adjoint,
                       cudaStream_t stream);
+// d loss / d (base_m, top_m) of layer 0 in the grid form, added to out[0..1]
+// (grid_layer_grad.cu); g.bg / g.target / g.inv_n as for the adjoint.
+int launch_grid_layer_grad(const MarchUniforms& u, const ViewDev& v, const GridDev& g, double* out,
+                           cudaStream_t stream);
 
 // TAA resolve of one cloud RT (post.cu, shaders/clouds/cloud_taa.wgsl).
 struct TaaParams {

@@ -81,6 +81,17 @@ class GridProblem:
              C.c_void_p(self.grad.data_ptr()), C.c_void_p(acc + 8), C.c_void_p(acc),
              C.c_void_p(stream.cuda_stream if stream is not None else None))
 
+    def layer_gradient(self, handle, out, rows=None, stream=None):
+        """Adds d loss / d (base_m, top_m) of the layer for this view (or
+        band) into `out`, a device float64 tensor of two values."""
+        assert self.target is not None, "set_target first"
+        v, off = self._view(rows, outputs=False)
+        call("psc_layer_gradient", handle, C.byref(self.grid()), C.byref(v),
+             C.c_void_p(self.bg.data_ptr() + off), C.c_void_p(self.target.data_ptr() + off),
+             C.c_void_p(out.data_ptr()),
+             C.c_void_p(stream.cuda_stream if stream is not None else None))
+        return out
+
     def composite_image(self):
         """I = L + background * T (what the loss compares with the target)."""
         return self.L + self.bg * self.T

@@ -158,3 +158,51 @@ def test_grid_argument_errors(prob):
         call("psc_adjoint", h, C.byref(P.grid()), C.byref(v), C.c_void_p(P.bg.data_ptr()), None,
              C.c_void_p(P.grad.data_ptr()), C.c_void_p(P.acc.data_ptr() + 8),
              C.c_void_p(P.acc.data_ptr()), None)
+
+
+def test_layer_range_gradient_matches_central_differences(oracle, oracle_noise):
+    """d loss / d base_m and d loss / d top_m of the layer (psc_layer_gradient)
+    on a 128x128 view of the same grid scene, no early exit, against
+    Richardson-extrapolated central differences (1 m and 0.5 m) of the FP64
+    oracle's loss; and row bands add up to the whole view."""
+    import dataclasses
+    torch = _gpu.torch_cuda()
+    sc = scenes.grid_512(128, 128)
+    luts = oracle.bake_luts(sc.frame, sc.world)
+    G = sc.extra["grid"]
+    spec = dict(sc.extra["grid_spec"], exit_transmittance=0.0)
+    Lt, Tt = oracle.grid_render(sc, oracle_noise, luts, scenes.grid_target_values(G), spec)
+    tgt = (Lt + sc.background * Tt).astype(np.float32)
+    sub = subsystem_for_scene(sc, luts=luts, noise=oracle_noise)
+    try:
+        P = GR.GridProblem(sc, G, spec=spec)
+        P.set_target(tgt)
+        out = torch.zeros(2, dtype=torch.float64, device="cuda:0")
+        P.layer_gradient(sub.handle, out)
+        bands = torch.zeros(2, dtype=torch.float64, device="cuda:0")
+        P.layer_gradient(sub.handle, bands, rows=(0, 50))
+        P.layer_gradient(sub.handle, bands, rows=(50, 128))
+        torch.cuda.synchronize()
+        g = out.cpu().numpy()
+        gb = bands.cpu().numpy()
+    finally:
+        sub.close()
+
+    def loss(d_base, d_top):
+        layers = (capi.CloudLayerGpu * 8).from_buffer_copy(sc.layers)
+        layers[0].base_m = float(np.float32(sc.layers[0].base_m + d_base))
+        layers[0].top_m = float(np.float32(sc.layers[0].top_m + d_top))
+        s2 = dataclasses.replace(sc, layers=layers)
+        return oracle.grid_loss(s2, oracle_noise, luts, G, spec, sc.background, tgt)
+
+    fd = []
+    for e_base, e_top in ((1.0, 0.0), (0.0, 1.0)):
+        d1 = (loss(e_base, e_top) - loss(-e_base, -e_top)) / 2.0
+        d2 = (loss(e_base / 2, e_top / 2) - loss(-e_base / 2, -e_top / 2)) / 1.0
+        fd.append((4.0 * d2 - d1) / 3.0)
+    fd = np.array(fd)
+    rel = np.abs(g - fd) / np.abs(fd)
+    print(f"\nlayer gradient d/dbase, d/dtop: GPU {g}, FD {fd}, rel {rel}")
+    assert np.all(np.abs(fd) > 0)
+    assert np.all(rel <= 2e-2), (g, fd)
+    assert np.allclose(gb, g, rtol=1e-5, atol=0)
