@@ -463,11 +463,14 @@ class Bench:
         self.stream = torch.cuda.Stream(device=self.dev)
         self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=self.dev)
 
-    def timed(self, step, pre=None, clk=None, kernel_events=None, steps=None, warmup=None):
+    def timed(self, step, pre=None, clk=None, kernel_events=None, steps=None, warmup=None,
+              counter=None):
         """W untimed steps, then K device-timed steps with the L2 flushed (and
         `pre` run) before each, outside the events.  Returns (per-step ms of
         this rank, the max over ranks of their mean).  `kernel_events`, when
-        given, is a list that `step` appends (start, end) event pairs to."""
+        given, is a list that `step` appends (start, end) event pairs to;
+        `counter`, when given, returns the library's launch count, and the
+        launches of the K timed steps go to self.timed_launches."""
         torch = self.torch
         steps = self.args.steps if steps is None else steps
         warmup = self.args.warmup if warmup is None else warmup
@@ -483,6 +486,7 @@ class Bench:
                for _ in range(steps)]
         self.ranks.barrier()
         torch.cuda.synchronize()
+        c0 = counter() if counter else 0
         with (clk if clk is not None else _NullCtx()):
             with torch.cuda.stream(self.stream):
                 for i in range(steps):
@@ -493,6 +497,7 @@ class Bench:
                     step()
                     evs[i][1].record(self.stream)
             torch.cuda.synchronize()
+        self.timed_launches = (counter() - c0) if counter else None
         ms = [a.elapsed_time(b) for a, b in evs]
         mean = float(np.mean(ms)) if ms else 0.0
         return ms, self.ranks.max(mean, self.dev)
@@ -566,12 +571,12 @@ def leg_batch64(B: Bench, storage, filt, n_views=64):
             tune = Bt.autotune(sub.handle, b, reps=1, stream=B.stream)
         Bt.set_tuning(sub.handle, tune["threads"], tune["tile_w"], use_graph=1,
                       form=tune["form_id"])
-        l0 = sub.launch_count()
     clk = ClockSampler(B.ranks.local)
     ms, ms_max = B.timed((lambda: b.render(sub.handle, B.stream)) if mine else (lambda: None),
-                         pre=(b.reset_hdr if mine else None), clk=clk)
+                         pre=(b.reset_hdr if mine else None), clk=clk,
+                         counter=(sub.launch_count if mine else None))
     if mine:
-        launches = sub.launch_count() - l0
+        launches = B.timed_launches
         sub.close()
     return {"metric": f"Mrays/s, {n_views} uneven views (c3)", "value":
             total_rays / (ms_max * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_max,
@@ -615,12 +620,10 @@ def leg_stress(B: Bench, storage, schedule, filt, W=3840, H=2160):
             hdr.copy_(bg, non_blocking=True)
             call("psc_render", sub.handle, C.byref(view), 1, B.sh())
 
-    if mine:
-        l0 = sub.launch_count()
     clk = ClockSampler(B.ranks.local)
-    ms, ms_max = B.timed(step, clk=clk)
+    ms, ms_max = B.timed(step, clk=clk, counter=(sub.launch_count if mine else None))
     if mine:
-        launches = sub.launch_count() - l0
+        launches = B.timed_launches
         sub.close()
     rays = 8 * W * H
     return {"metric": "Mrays/s, eight 3840x2160 Cumulonimbus frames (c5)",
@@ -662,10 +665,9 @@ def leg_grid(B: Bench, with_e2e=False):
             P.adjoint(sub.handle, rows=rows, stream=B.stream)
         sharding.allreduce_gradient(P.grad, P.acc)
 
-    l0 = sub.launch_count()
     clk = ClockSampler(B.ranks.local)
-    ms, ms_max = B.timed(step, clk=clk)
-    launches = sub.launch_count() - l0
+    ms, ms_max = B.timed(step, clk=clk, counter=sub.launch_count)
+    launches = B.timed_launches
     _, fwd_ms = B.timed(lambda: P.render(sub.handle, rows=rows, stream=B.stream))
     _, adj_ms = B.timed(lambda: (P.zero_grad(), P.adjoint(sub.handle, rows=rows, stream=B.stream)))
     out = {"metric": GRID_METRIC, "value": W * H / (ms_max * 1e-3) / 1e6, "unit": UNIT,
@@ -786,9 +788,8 @@ def run_frames(args, ranks: Ranks):
     except Exception as e:  # reported with the roofline, never required
         print(f"fetch-peak calibration failed: {e}", file=sys.stderr)
     clk = ClockSampler(ranks.local)
-    l0 = sub.launch_count()
-    step_ms, ms_max = B.timed(render_step, clk=clk, kernel_events=kev)
-    kernel_launches = sub.launch_count() - l0
+    step_ms, ms_max = B.timed(render_step, clk=clk, kernel_events=kev, counter=sub.launch_count)
+    kernel_launches = B.timed_launches
     kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kev])) if kev else None
     rays_step = n_frames * W * H
     value = ranks.world * rays_step / (ms_max * 1e-3) / 1e6

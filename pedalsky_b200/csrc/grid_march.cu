@@ -14,11 +14,11 @@
 // transmittance at every k-th step, evaluates its pixel's loss term
 // (I - target)^2 / N with I = L + background * T, then walks the checkpoint
 // segments backwards: each segment is recomputed from its checkpoint,
-// storing per step the light-march grid sum and the prefix sum of the
-// primary grid values within the segment, then traversed in reverse,
+// storing per step the primary and light-march grid sums and the prefix sum
+// of the primary grid values within the segment, then traversed in reverse,
 // carrying the adjoint of the transmittance.  The transmittance before a
-// step is the checkpoint's times exp(-sigma_t * step * k * prefix) and the
-// primary grid value is fetched again.  Checkpoints and segment buffers live
+// step is the checkpoint's times exp(-sigma_t * step * k * prefix).
+// Checkpoints and segment buffers live
 // in dynamic shared memory laid out [slot][thread], so every access is
 // conflict-free and nothing is kept in local memory.  d loss / d density at the primary sample and d loss /
 // d optical depth toward the sun are scattered into the gradient grid with
@@ -37,14 +37,15 @@ namespace {
 constexpr int kTileW = 16;
 constexpr int kTileH = 8;
 constexpr int kThreads = 128;
-constexpr int kAdjointCtasDefault = 6;  // see adjoint_ctas_per_sm
+constexpr int kAdjointCtasDefault = 5;  // see adjoint_ctas_per_sm
 constexpr int kMaxCp = 32;   // checkpoints per ray
 constexpr int kMaxSeg = 32;  // steps per checkpoint segment
 
 // Shared-memory words per thread of the adjoint: three transmittances per
-// checkpoint, then a prefix sum and a light sum per step of one segment.
+// checkpoint, then a prefix sum, a primary grid value and a light sum per
+// step of one segment.
 __host__ __device__ constexpr uint32_t adjoint_words(uint32_t n_cp, uint32_t k_cp) {
-  return 3u * n_cp + 2u * k_cp;
+  return 3u * n_cp + 3u * k_cp;
 }
 
 struct Tri {
@@ -93,9 +94,30 @@ __device__ __forceinline__ void grid_corners(const GridDev& g, const Tri& t, F&&
   }
 }
 
+// Trilinear fetch without per-corner branches: corner indices clamped into
+// the grid (so every load is in bounds) and the weights of corners outside
+// it zeroed, which gives the same sum as visiting the in-grid corners only;
+// a sample with no corner inside the grid loads nothing.
 __device__ __forceinline__ float grid_fetch(const GridDev& g, const Tri& t) {
+  const bool x0 = (uint32_t)t.x0 < g.nx, x1 = (uint32_t)(t.x0 + 1) < g.nx;
+  const bool y0 = (uint32_t)t.y0 < g.ny, y1 = (uint32_t)(t.y0 + 1) < g.ny;
+  const bool z0 = (uint32_t)t.z0 < g.nz, z1 = (uint32_t)(t.z0 + 1) < g.nz;
+  if (!((x0 || x1) && (y0 || y1) && (z0 || z1))) return 0.0f;
+  const float wx[2] = {x0 ? 1.0f - t.wx : 0.0f, x1 ? t.wx : 0.0f};
+  const float wy[2] = {y0 ? 1.0f - t.wy : 0.0f, y1 ? t.wy : 0.0f};
+  const float wz[2] = {z0 ? 1.0f - t.wz : 0.0f, z1 ? t.wz : 0.0f};
+  const uint32_t cx[2] = {(uint32_t)min(max(t.x0, 0), (int)g.nx - 1), (uint32_t)min(max(t.x0 + 1, 0), (int)g.nx - 1)};
+  const uint32_t cy[2] = {(uint32_t)min(max(t.y0, 0), (int)g.ny - 1), (uint32_t)min(max(t.y0 + 1, 0), (int)g.ny - 1)};
+  const uint32_t cz[2] = {(uint32_t)min(max(t.z0, 0), (int)g.nz - 1), (uint32_t)min(max(t.z0 + 1, 0), (int)g.nz - 1)};
   float v = 0.0f;
-  grid_corners(g, t, [&](uint32_t i, float w) { v = fmaf(w, __ldg(g.values + i), v); });
+#pragma unroll
+  for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz) {
+      const float* row = g.values + (cy[dy] * g.nz + cz[dz]) * g.nx;
+      const float wyz = wy[dy] * wz[dz];
+      v = fmaf(wyz, fmaf(wx[1], __ldg(row + cx[1]), wx[0] * __ldg(row + cx[0])), v);
+    }
   return v;
 }
 
@@ -255,10 +277,11 @@ __device__ __forceinline__ void grid_pixel(const MarchUniforms& u, const ViewDev
   const uint32_t kcp = g.k_cp;
   uint32_t n_exec = 0;
   // shared-memory slots: checkpoint transmittances, then the segment's
-  // prefix sums and light sums
+  // prefix sums, primary grid values and light sums
   float* const s_cp = sm;
   float* const s_pre = sm + 3u * ((u.cloud_steps + kcp - 1u) / kcp) * kThreads;
-  float* const s_gl = s_pre + kcp * kThreads;
+  float* const s_gv = s_pre + kcp * kThreads;
+  float* const s_gl = s_gv + kcp * kThreads;
 
   auto position = [&](uint32_t s, float& px3, float& py3, float& pz3, float& alt, float& ux, float& uy,
                       float& uz) {
@@ -343,6 +366,7 @@ __device__ __forceinline__ void grid_pixel(const MarchUniforms& u, const ViewDev
         const float gl = light_sum(u, g, light_geo(u, L, alt, ux, uy, uz), px3, py3, pz3, alt);
         const uint32_t b = (s - s0) * kThreads;
         s_pre[b] = pre;
+        s_gv[b] = gv;
         s_gl[b] = gl;
         pre += gv;
       }
@@ -352,7 +376,7 @@ __device__ __forceinline__ void grid_pixel(const MarchUniforms& u, const ViewDev
         const uint32_t b = (s - s0) * kThreads;
         float px3, py3, pz3, alt, ux, uy, uz;
         position(s, px3, py3, pz3, alt, ux, uy, uz);
-        const float gv = grid_fetch(g, grid_coords(g, px3, alt, pz3)), gl = s_gl[b];
+        const float gv = s_gv[b], gl = s_gl[b];
         const float p_od = kstep * s_pre[b];  // optical depth per unit sigma_t since the checkpoint
         const float bT[3] = {cp3[0] * __expf(-st[0] * p_od), cp3[1] * __expf(-st[1] * p_od),
                              cp3[2] * __expf(-st[2] * p_od)};
@@ -458,7 +482,7 @@ int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g
     return PSC_ERR_INVALID_ARGUMENT;
   const dim3 grid((v.width + kTileW - 1) / kTileW, (v.height + kTileH - 1) / kTileH);
   if (adjoint) {
-    // at most 3 x 32 + 2 x 32 words per thread (80 KiB per CTA)
+    // at most 3 x 32 + 3 x 32 words per thread (96 KiB per CTA)
     const uint32_t n_cp = (u.cloud_steps + g.k_cp - 1) / g.k_cp;
     const size_t smem = (size_t)adjoint_words(n_cp, g.k_cp) * kThreads * sizeof(float);
     const int ctas = adjoint_ctas_per_sm();

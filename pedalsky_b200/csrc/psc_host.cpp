@@ -625,9 +625,10 @@ int stage_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32_t* n_t
   return PSC_OK;
 }
 
-// The per-view form on `s`: frame records H2D, the per-view LUT bakes, then
-// one FAST kernel per view (uniforms by value) in descending cost on the
-// branch streams, forked from and joined back into `s`.
+// The per-view form on `s`: frame records H2D, then per view, in descending
+// cost over the branch streams (forked from and joined back into `s`), its
+// sky-view / aerial-perspective LUT bake and its FAST kernel (uniforms by
+// value), so a view's bake overlaps the other branches' marches.
 int enqueue_batch_per_view(psc_ctx* c, uint32_t n, cudaStream_t s, bool capturing) {
   if (!c->batch_fork) {
     PSC_CUDA(cudaEventCreateWithFlags(&c->batch_fork, cudaEventDisableTiming), "batch fork event");
@@ -640,17 +641,20 @@ int enqueue_batch_per_view(psc_ctx* c, uint32_t n, cudaStream_t s, bool capturin
   PSC_CUDA(cudaMemcpyAsync(c->d_bframes, c->h_bframes, n * fl, cudaMemcpyHostToDevice, s), "batch frames H2D");
   PSC_CUDA(cudaEventRecordWithFlags(c->batch_staged, s, capturing ? cudaEventRecordExternal : 0),
            "batch event");
-  if (psc::launch_view_lut_bakes(c->world, c->d_bframes, n, c->d_lut_h[PSC_LUT_TRANSMITTANCE],
-                                 c->d_lut_h[PSC_LUT_MULTISCATTER], c->d_bsky, c->d_bap, s))
-    return fail(PSC_ERR_CUDA, "per-view LUT bake launch failed");
   const uint32_t nb = std::min<uint32_t>(n, (uint32_t)psc_ctx::kBranches);
   PSC_CUDA(cudaEventRecord(c->batch_fork, s), "batch fork");
   for (uint32_t j = 0; j < nb; ++j)
     PSC_CUDA(cudaStreamWaitEvent(c->batch_branch[j], c->batch_fork, 0), "batch fork wait");
   for (uint32_t k = 0; k < n; ++k) {
     const uint32_t i = c->batch_order[k];
-    int rc = psc::launch_march_fast(c->h_bu[i], c->h_bv[i], c->opts, c->batch_branch[k % nb]);
-    if (rc == PSC_ERR_UNSUPPORTED) rc = psc::launch_march(c->h_bu[i], c->h_bv[i], c->opts, c->batch_branch[k % nb]);
+    cudaStream_t br = c->batch_branch[k % nb];
+    if (psc::launch_view_lut_bakes(c->world, static_cast<const char*>(c->d_bframes) + i * fl, 1,
+                                   c->d_lut_h[PSC_LUT_TRANSMITTANCE], c->d_lut_h[PSC_LUT_MULTISCATTER],
+                                   c->d_bsky + (size_t)i * PSC_SKYVIEW_W * PSC_SKYVIEW_H,
+                                   c->d_bap + (size_t)i * PSC_AP_W * PSC_AP_H * PSC_AP_D, br))
+      return fail(PSC_ERR_CUDA, "per-view LUT bake launch failed");
+    int rc = psc::launch_march_fast(c->h_bu[i], c->h_bv[i], c->opts, br);
+    if (rc == PSC_ERR_UNSUPPORTED) rc = psc::launch_march(c->h_bu[i], c->h_bv[i], c->opts, br);
     if (rc) return fail(rc, "per-view march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   for (uint32_t j = 0; j < nb; ++j) {
