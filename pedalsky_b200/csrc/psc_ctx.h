@@ -95,6 +95,7 @@ struct psc_ctx {
   psc::ViewDev* d_bv = nullptr;
   void* d_bframes = nullptr;            // per-view frame records for the LUT bakes
   float4* d_bsky = nullptr;             // per-view sky-view LUTs
+  std::vector<cudaTextureObject_t> batch_sky_tex;  // per-view sky-view LUTs through the texture unit
   float4* d_bap = nullptr;              // per-view aerial-perspective LUTs
   uint32_t* d_btiles = nullptr;
   uint32_t* d_bcounter = nullptr;

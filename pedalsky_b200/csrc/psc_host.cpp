@@ -468,7 +468,14 @@ int build_textures(psc_ctx* c) {
   return PSC_OK;
 }
 
+void destroy_batch_sky_textures(psc_ctx* c) {
+  for (cudaTextureObject_t t : c->batch_sky_tex)
+    if (t) cudaDestroyTextureObject(t);
+  c->batch_sky_tex.clear();
+}
+
 void release_batch(psc_ctx* c) {
+  destroy_batch_sky_textures(c);
   if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
   c->batch_exec = nullptr;
   c->batch_key.clear();
@@ -514,6 +521,7 @@ int reserve_batch(psc_ctx* c, uint32_t views, uint32_t tiles) {
     cudaEventSynchronize(c->batch_staged);
     if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
     c->batch_exec = nullptr;
+    destroy_batch_sky_textures(c);
     dfree(c->d_bu);
     dfree(c->d_bv);
     dfree(c->d_bframes);
@@ -533,6 +541,24 @@ int reserve_batch(psc_ctx* c, uint32_t views, uint32_t tiles) {
     PSC_CUDA(cudaMallocHost(&c->h_bu, views * sizeof(psc::MarchUniforms)), "pinned batch uniforms");
     PSC_CUDA(cudaMallocHost(&c->h_bv, views * sizeof(psc::ViewDev)), "pinned batch views");
     PSC_CUDA(cudaMallocHost(&c->h_bframes, views * fl), "pinned batch frames");
+    // each view's sky-view LUT also behind a texture object (bilinear,
+    // clamp, normalised coordinates), as the context's own sky-view LUT is
+    c->batch_sky_tex.assign(views, 0);
+    for (uint32_t i = 0; i < views; ++i) {
+      cudaResourceDesc rd{};
+      rd.resType = cudaResourceTypePitch2D;
+      rd.res.pitch2D.devPtr = c->d_bsky + (size_t)i * PSC_SKYVIEW_W * PSC_SKYVIEW_H;
+      rd.res.pitch2D.desc = cudaCreateChannelDesc<float4>();
+      rd.res.pitch2D.width = PSC_SKYVIEW_W;
+      rd.res.pitch2D.height = PSC_SKYVIEW_H;
+      rd.res.pitch2D.pitchInBytes = (size_t)PSC_SKYVIEW_W * sizeof(float4);
+      cudaTextureDesc td{};
+      td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+      td.filterMode = cudaFilterModeLinear;
+      td.readMode = cudaReadModeElementType;
+      td.normalizedCoords = 1;
+      PSC_CUDA(cudaCreateTextureObject(&c->batch_sky_tex[i], &rd, &td, nullptr), "batch sky-view texture");
+    }
     c->batch_cap_views = views;
   }
   if (tiles > c->batch_cap_tiles) {
@@ -563,10 +589,12 @@ int validate_tuning(const PscBatchTuning& t) {
 // Host staging of one batch: per-view uniform blocks, view records, frame
 // records for the LUT bakes and the cost-sorted tile list.
 // Uniform block of one batch view: its own scene, and its own sky-view and
-// aerial-perspective LUTs (baked per view into `sky` / `ap`, read with plain
-// loads; the context's sky-view texture belongs to its own frame).
+// aerial-perspective LUTs (baked per view into `sky` / `ap`; the context's
+// sky-view texture belongs to its own frame).  `sky_tex`, when not 0, is a
+// texture object over `sky`, used by the filtered forms as the single-view
+// march uses the context's; 0 reads `sky` with plain loads.
 void build_batch_view_uniforms(const psc_ctx* c, const PscBatchView& bv, float4* sky, float4* ap,
-                               psc::MarchUniforms& u) {
+                               psc::MarchUniforms& u, cudaTextureObject_t sky_tex = 0) {
   PscCloudParamsGpu p = bv.params;
   p.cloud_layer_count = bv.n_layers;
   PscCloudLayerGpu layers[8];
@@ -574,7 +602,7 @@ void build_batch_view_uniforms(const psc_ctx* c, const PscBatchView& bv, float4*
   for (uint32_t l = 0; l < bv.n_layers; ++l) layers[l] = bv.layers[l];
   build_uniforms_for(c, p, layers, bv.frame, bv.width, bv.height, u);
   u.lut_sky = sky;
-  u.tex_sky = 0;
+  u.tex_sky = c->opts.filter != PSC_FILTER_EXACT ? sky_tex : 0;
   u.lut_ap = ap;
 }
 
@@ -597,7 +625,8 @@ int stage_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32_t* n_t
   for (uint32_t i = 0; i < n; ++i) {
     const PscBatchView& bv = views[i];
     build_batch_view_uniforms(c, bv, c->d_bsky + (size_t)i * PSC_SKYVIEW_W * PSC_SKYVIEW_H,
-                              c->d_bap + (size_t)i * PSC_AP_W * PSC_AP_H * PSC_AP_D, c->h_bu[i]);
+                              c->d_bap + (size_t)i * PSC_AP_W * PSC_AP_H * PSC_AP_D, c->h_bu[i],
+                              c->batch_sky_tex[i]);
     c->h_bv[i] = psc::ViewDev{bv.width, bv.height, 0, 0, bv.depth, reinterpret_cast<float4*>(bv.out_luminance),
                               reinterpret_cast<float4*>(bv.out_transmittance), reinterpret_cast<float4*>(bv.hdr)};
     psc::frame_lite_from(bv.frame, static_cast<char*>(c->h_bframes) + i * fl);
