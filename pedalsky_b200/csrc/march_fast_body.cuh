@@ -650,10 +650,11 @@ __device__ __forceinline__ float one_minus_exp_neg(float y, float e) {
 
 // Per-thread shared-memory words of march_pixel_fast beyond the layer
 // intervals, all touched at most once per dense sample and so kept out of
-// the registers the step loop needs: the per-layer octave coefficients,
-// the compensated optical depths of the Kahan form, the radiance and the
+// the registers the step loop needs: the per-layer octave coefficients (two
+// sets for a Cumulonimbus layer: its own droplet size and 50 um), the
+// compensated optical depths of the Kahan form, the radiance and the
 // aerial-perspective distance weights.
-constexpr uint32_t kAuxWords = kMaxOct + 6 + 5;
+constexpr uint32_t kAuxWords = 2 * kMaxOct + 6 + 5;
 
 // Fetch tally of the instrumented build (TALLY = true): per ray, the
 // fetches march_pixel_fast issues, by kind, in the order of PscFetchCounts.
@@ -714,8 +715,9 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
   const float jitter = __ldg(u.blue + sy * 64u + sx);
   const uint32_t noct = u.octaves;
 
-  float* const s_coef = s_aux;                      // [kMaxOct][stride]
-  float* const s_kahan = s_aux + kMaxOct * stride;  // od r,g,b then comp r,g,b
+  float* const s_coef = s_aux;                         // [kMaxOct][stride]
+  float* const s_coef_hi = s_aux + kMaxOct * stride;   // Cumulonimbus at 50 um, [kMaxOct][stride]
+  float* const s_kahan = s_coef_hi + kMaxOct * stride; // od r,g,b then comp r,g,b
   float* const s_acc = s_kahan + 6 * stride;        // L r,g,b, sum(w t), sum(w)
   if (FULL && u.kahan) {
 #pragma unroll
@@ -754,6 +756,20 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
       for (int n = 0; n < kMaxOct; ++n)
         s_coef[n * stride + slot] =
             (n < (int)noct) ? u.apow[n] * fwd_gain * phase_with(u, cos_theta, u.cpow[n], pc) : 0.0f;
+    } else {
+      // Cumulonimbus: the droplet diameter blends from the layer's to 50 um
+      // with mt = smoothstep(0.60, 0.85, h); mt is exactly 0 below the band
+      // and exactly 1 once its clamp saturates, where mix(d, 50, mt) is
+      // exactly d or exactly 50, so those two coefficient sets are
+      // evaluated once here with the same expressions as the per-sample form
+      const PhaseConst lo = phase_consts_from_d(mixf(L.droplet_um, 50.0f, 0.0f), u.droplet_bias);
+      const PhaseConst hi = phase_consts_from_d(mixf(L.droplet_um, 50.0f, 1.0f), u.droplet_bias);
+#pragma unroll
+      for (int n = 0; n < kMaxOct; ++n) {
+        const bool on = n < (int)noct;
+        s_coef[n * stride + slot] = on ? u.apow[n] * fwd_gain * phase_with(u, cos_theta, u.cpow[n], lo) : 0.0f;
+        s_coef_hi[n * stride + slot] = on ? u.apow[n] * fwd_gain * phase_with(u, cos_theta, u.cpow[n], hi) : 0.0f;
+      }
     }
 
     for (uint32_t s = 0; s < u.cloud_steps; ++s) {
@@ -862,12 +878,15 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
             const float eng = bg * fmaf(u.powder, fmaf(-2.0f * bg, bg, 1.0f), 1.0f);
             const float enb = bb * fmaf(u.powder, fmaf(-2.0f * bb, bb, 1.0f), 1.0f);
             float cf[kMaxOct];
-            if (cb) {
-              const float mt = smoothstepf(0.60f, 0.85f, h);
+            const float mt = cb ? smoothstepf(0.60f, 0.85f, h) : 0.0f;
+            if (cb && mt > 0.0f && mt < 1.0f) {  // inside the blend band
               const PhaseConst pc = phase_consts_from_d(mixf(L.droplet_um, 50.0f, mt), u.droplet_bias);
 #pragma unroll
               for (int n = 0; n < kMaxOct; ++n)
                 cf[n] = (n < (int)noct) ? u.apow[n] * fwd_gain * phase_with(u, cos_theta, u.cpow[n], pc) : 0.0f;
+            } else if (cb && mt >= 1.0f) {
+#pragma unroll
+              for (int n = 0; n < kMaxOct; ++n) cf[n] = s_coef_hi[n * stride + slot];
             } else {
 #pragma unroll
               for (int n = 0; n < kMaxOct; ++n) cf[n] = s_coef[n * stride + slot];
