@@ -902,7 +902,7 @@ def run_frames(args, ranks: Ranks):
         legs["grid_512"] = leg_grid(B)
 
     if ranks.rank == 0:
-        roof = roofline(args, wl, W, H, rays_step, kernel_ms, peaks_fetch, counts, batched)
+        roof = roofline(args, wl, W, H, W * H, kernel_ms, peaks_fetch, counts, batched, rays_step)
         cpu = None
         if not args.no_cpu_baseline and ranks.world == 1:
             try:
@@ -943,8 +943,9 @@ def run_frames(args, ranks: Ranks):
     return 0
 
 
-def roofline(args, wl, W, H, rays, kernel_ms, peaks_fetch, counts, batched):
-    """The timed kernel against the ceiling that bounds it.  The march's
+def roofline(args, wl, W, H, rays, kernel_ms, peaks_fetch, counts, batched, rays_step):
+    """The timed kernel against the ceiling that bounds it (`rays` per launch
+    of it; `rays_step` per step, for the batched form's whole-step rate).  The march's
     working set (folded volumes, LUTs, weather) is L2-resident, so its
     fetches are served on chip: the ceiling is the L2 read bandwidth
     measured on this GPU in this run.  `achieved` counts the algorithmic
@@ -995,7 +996,7 @@ def roofline(args, wl, W, H, rays, kernel_ms, peaks_fetch, counts, batched):
             out["fetch"]["light_march_gfetch_s"] = light
             out["fetch"]["frac_of_tex_trilinear"] = light / peaks_fetch["tex_trilinear_gfetch_s"]
         if alg and batched:
-            b_ach = alg["bytes_per_ray"] * rays / (batched["ms_per_step"] * 1e-3) / 1e9
+            b_ach = alg["bytes_per_ray"] * rays_step / (batched["ms_per_step"] * 1e-3) / 1e9
             batched["fetch_gbs"] = b_ach
             batched["frac_of_l2_read"] = b_ach / peaks_fetch["l2_read_gbs"]
     return out
