@@ -171,3 +171,37 @@ def test_batch_argument_errors(small_batch, oracle_noise):
         b.render(sub.handle)
     assert e.value.code == -8
     sub.close()
+
+
+@pytest.mark.parametrize("form", [capi.BATCH_PERSISTENT, capi.BATCH_PER_VIEW])
+def test_batch_views_match_the_fp64_oracle(oracle, oracle_noise, form):
+    """Views of a seeded uneven batch (mixed cloud types, Cumulonimbus among
+    them) through psc_render_batch with the GPU's per-view sky-view / AP LUT
+    bakes and its transmittance / multi-scatter bake, composited over each
+    view's sky, against the FP64 oracle fed with its own CPU LUT bakes for
+    each view's frame; the parity bar of the march tests."""
+    from ._metrics import composite, rel_stats, ssim, tonemap
+    torch = _gpu.torch_cuda()
+    views = scenes.batch_views(6, seed=21, size_scale=0.12, storage=capi.STORAGE_F16,
+                               filt=capi.FILTER_HYBRID, composite=1)
+    sub = subsystem_for_scene(views[0], luts=None, noise=oracle_noise)
+    try:
+        b = B.Batch(views, "cuda:0", outputs=("hdr",))
+        B.set_tuning(sub.handle, 128, 16, 1, form)
+        b.reset_hdr()
+        b.render(sub.handle)
+        torch.cuda.synchronize()
+        for i, v in enumerate(views):
+            luts = oracle.bake_luts(v.frame, v.world)
+            L, T = oracle.render(v, oracle_noise, luts, precision=oracle.FP64)
+            ref = composite(L, T, v.background)
+            got = b.hdr[i].cpu().numpy()
+            st = rel_stats(got, ref)
+            st["ssim"] = ssim(tonemap(got), tonemap(ref))
+            types = [int(v.layers[k].cloud_type) for k in range(v.n_layers)]
+            print(f"\n[batch vs oracle] form {form} view {i} {v.width}x{v.height} types {types}: {st}")
+            assert np.isfinite(got).all()
+            assert st["p999"] <= 1e-3 and st["frac_gt_1e3"] <= 1e-3 and st["mean"] <= 1e-4, (i, st)
+            assert st["ssim"] >= 0.999, (i, st)
+    finally:
+        sub.close()
