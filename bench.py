@@ -828,9 +828,11 @@ def run_frames(args, ranks: Ranks):
                       form=btune["form_id"])
         _, ms_b = B.timed(lambda: bt.render(sub.handle, stream), pre=bt.reset_hdr)
         batched = {"value": ranks.world * rays_step / (ms_b * 1e-3) / 1e6, "ms_per_step": ms_b,
-                   "config": "psc_render_batch: persistent kernel from a captured CUDA graph, "
-                             "per-view LUT bakes included", "autotuned": btune}
+                   "config": "psc_render_batch in the autotuner's form and light-march batch, "
+                             "replayed from a captured CUDA graph, per-view LUT bakes included",
+                   "autotuned": btune}
         del bt
+        sub.set_options(o)  # the autotuner keeps its light-march batch in the options
 
     row_bands = None
     if n_frames == 1 and not args.no_legs:

@@ -222,7 +222,13 @@ typedef struct PscMarchOptions {
                                (CloudsTuning::half_res_render)            */
   uint32_t taa;             /* 1: TAA resolve of the cloud RT
                                (temporal_taa && !freeze_time)             */
-  uint32_t _reserved[2];
+  uint32_t light_batch;     /* light-march taps each thread fetches before
+                               combining them, FAST F16 hybrid form: 0 =
+                               all six of the reference default in one
+                               batch (other counts in 4s), 3 or 2 = batches
+                               of that many; the same sums in the same
+                               order.  Chosen by psc_autotune_batch.     */
+  uint32_t _reserved;
 } PscMarchOptions;
 
 /* One view to render: a width x height rectangle of pixels.  By default
@@ -362,6 +368,7 @@ int psc_set_layers(psc_ctx* ctx, const PscCloudLayerGpu* layers, uint32_t n);
 int psc_set_frame(psc_ctx* ctx, const PscFrameUniformsGpu* frame,
                   const PscWorldUniformsGpu* world);
 int psc_set_options(psc_ctx* ctx, const PscMarchOptions* options);
+int psc_get_options(psc_ctx* ctx, PscMarchOptions* out);
 
 /* ----------------------------------------------------------- inputs */
 
@@ -543,8 +550,11 @@ int psc_render_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, void* 
 
 /* Time every candidate launch shape on this batch (`reps` timed runs each,
  * after one warm-up): the persistent form at each CTA size and tile width,
- * and the per-view form.  Keeps the fastest in the context and returns it
- * with its median time in milliseconds.  Synchronous. */
+ * and the per-view form; then, for the FAST F16 hybrid form, the light-march
+ * fetch batch (options.light_batch 0, 3, 2) in the fastest of those.  Keeps
+ * the fastest in the context (the light batch in its options,
+ * psc_get_options) and returns the launch shape with its median time in
+ * milliseconds.  Synchronous. */
 int psc_autotune_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, uint32_t reps,
                        PscBatchTuning* best, float* best_ms, void* stream);
 

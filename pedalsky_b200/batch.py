@@ -71,6 +71,9 @@ def autotune(handle, batch: Batch, reps=3, stream=None):
     ms = C.c_float()
     call("psc_autotune_batch", handle, batch.arr, len(batch.views), reps, C.byref(best),
          C.byref(ms), C.c_void_p(stream.cuda_stream if stream is not None else None))
+    opts = capi.MarchOptions()
+    call("psc_get_options", handle, C.byref(opts))
     return {"form": "per_view" if best.form == capi.BATCH_PER_VIEW else "persistent",
             "form_id": best.form, "threads": best.threads, "tile_w": best.tile_w,
-            "tile_h": best.threads // 32 // (best.tile_w // 8) * 4, "ms": ms.value}
+            "tile_h": best.threads // 32 // (best.tile_w // 8) * 4,
+            "light_batch": opts.light_batch, "ms": ms.value}

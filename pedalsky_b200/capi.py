@@ -97,7 +97,7 @@ class MarchOptions(C.Structure):
         ("phase_mode", u32), ("hg_g_forward", f32), ("hg_g_backward", f32), ("hg_blend", f32),
         ("storage", u32), ("filter", u32), ("schedule", u32), ("kahan", u32), ("composite", u32),
         ("debug_checks", u32), ("tile_w", u32), ("tile_h", u32), ("half_res", u32), ("taa", u32),
-        ("_reserved", u32 * 2),
+        ("light_batch", u32), ("_reserved", u32),
     ]
 
 
@@ -198,6 +198,7 @@ _PROTOS = {
     "psc_set_layers": [_vp, P(CloudLayerGpu), u32],
     "psc_set_frame": [_vp, P(FrameUniformsGpu), P(WorldUniformsGpu)],
     "psc_set_options": [_vp, P(MarchOptions)],
+    "psc_get_options": [_vp, P(MarchOptions)],
     "psc_bake_noise": [_vp],
     "psc_upload_noise": [_vp, i32, _vp, C.c_size_t],
     "psc_download_noise": [_vp, i32, _vp, C.c_size_t],

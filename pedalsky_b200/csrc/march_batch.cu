@@ -31,7 +31,7 @@ __device__ __forceinline__ void unpack_tile(uint32_t w, uint32_t& view, uint32_t
 // (needs_full_paths on its uniform block), so the views of a mixed batch that
 // need no full-form path still get the lean one (64 uneven views 209.5 ->
 // 194.2 ms).
-template <int ST, int FILT, int NT, bool FULL>
+template <int ST, int FILT, int NT, bool FULL, int LB>
 __global__ void __launch_bounds__(NT, 768 / NT)
     k_march_batch(const MarchUniforms* __restrict__ views_u, const ViewDev* __restrict__ views_v,
                   const uint32_t* __restrict__ tiles, uint32_t n_tiles, uint32_t* __restrict__ counter,
@@ -67,43 +67,43 @@ __global__ void __launch_bounds__(NT, 768 / NT)
     const uint32_t py = ty * tile_h + (warp / warps_x) * 4u + (lane >> 3);
     if (px < sv.width && py < sv.height) {
       if (FULL && vfull)
-        march_pixel_fast<ST, FILT, true>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
+        march_pixel_fast<ST, FILT, true, false, LB>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
       else
-        march_pixel_fast<ST, FILT, false>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
+        march_pixel_fast<ST, FILT, false, false, LB>(su, sv, px, py, s_t0, s_t1, s_aux, NT, threadIdx.x);
     }
     __syncthreads();  // su, sv and s_tile are rewritten by the next iteration
   }
 }
 
-template <int ST, int FILT, int NT, bool FULL>
+template <int ST, int FILT, int NT, bool FULL, int LB>
 int launch_batch_full(const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles, uint32_t n_tiles,
                     uint32_t* counter, uint32_t tile_w, int sms, cudaStream_t s) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march_batch<ST, FILT, NT, FULL>, NT, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march_batch<ST, FILT, NT, FULL, LB>, NT, 0) !=
       cudaSuccess)
     return PSC_ERR_CUDA;
   per_sm = per_sm < 1 ? 1 : per_sm;
   uint32_t grid = (uint32_t)(sms * per_sm);
   if (grid > n_tiles) grid = n_tiles ? n_tiles : 1;
-  k_march_batch<ST, FILT, NT, FULL><<<grid, NT, 0, s>>>(u, v, tiles, n_tiles, counter, tile_w);
+  k_march_batch<ST, FILT, NT, FULL, LB><<<grid, NT, 0, s>>>(u, v, tiles, n_tiles, counter, tile_w);
   return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
 }
 
-template <int ST, int FILT, int NT>
+template <int ST, int FILT, int NT, int LB>
 int launch_batch_t(const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles, uint32_t n_tiles,
                    uint32_t* counter, uint32_t tile_w, int sms, bool full, cudaStream_t s) {
-  return full ? launch_batch_full<ST, FILT, NT, true>(u, v, tiles, n_tiles, counter, tile_w, sms, s)
-            : launch_batch_full<ST, FILT, NT, false>(u, v, tiles, n_tiles, counter, tile_w, sms, s);
+  return full ? launch_batch_full<ST, FILT, NT, true, LB>(u, v, tiles, n_tiles, counter, tile_w, sms, s)
+            : launch_batch_full<ST, FILT, NT, false, LB>(u, v, tiles, n_tiles, counter, tile_w, sms, s);
 }
 
-template <int ST, int FILT>
+template <int ST, int FILT, int LB = 0>
 int launch_batch_nt(int nt, const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles,
                     uint32_t n_tiles, uint32_t* counter, uint32_t tile_w, int sms, bool full,
                     cudaStream_t s) {
   switch (nt) {
-    case 64: return launch_batch_t<ST, FILT, 64>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
-    case 128: return launch_batch_t<ST, FILT, 128>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
-    case 256: return launch_batch_t<ST, FILT, 256>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
+    case 64: return launch_batch_t<ST, FILT, 64, LB>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
+    case 128: return launch_batch_t<ST, FILT, 128, LB>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
+    case 256: return launch_batch_t<ST, FILT, 256, LB>(u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
     default: return PSC_ERR_INVALID_ARGUMENT;
   }
 }
@@ -114,6 +114,11 @@ int launch_march_batch(const PscMarchOptions& o, int threads, uint32_t tile_w,
                        const MarchUniforms* u, const ViewDev* v, const uint32_t* tiles,
                        uint32_t n_tiles, uint32_t* counter, int sms, bool full, cudaStream_t s) {
   if (o.filter == PSC_FILTER_HYBRID) {
+    // the light-march fetch batch is chosen for the F16 hybrid form only
+    if (o.storage == PSC_STORAGE_F16 && o.light_batch == 2)
+      return launch_batch_nt<PSC_STORAGE_F16, PSC_FILTER_HYBRID, 2>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
+    if (o.storage == PSC_STORAGE_F16 && o.light_batch == 3)
+      return launch_batch_nt<PSC_STORAGE_F16, PSC_FILTER_HYBRID, 3>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
     if (o.storage == PSC_STORAGE_F16)
       return launch_batch_nt<PSC_STORAGE_F16, PSC_FILTER_HYBRID>(threads, u, v, tiles, n_tiles, counter, tile_w, sms, full, s);
     if (o.storage == PSC_STORAGE_U8)

@@ -16,7 +16,7 @@ constexpr int kThreads = 128;
 
 // Shared memory per CTA: the entry/exit distances of each of the view's
 // layers and kAuxWords more words, per thread (dynamic, sized at launch).
-template <int ST, int FILT, bool FULL>
+template <int ST, int FILT, bool FULL, int LB>
 __global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constant__ MarchUniforms u,
                                                             const __grid_constant__ ViewDev v) {
   extern __shared__ float s_dyn[];
@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_march_fast(const __grid_constan
   const uint32_t px = blockIdx.x * kTileW + (warp & 1u) * 8u + (lane & 7u);
   const uint32_t py = blockIdx.y * kTileH + (warp >> 1) * 4u + (lane >> 3);
   if (px >= v.width || py >= v.height) return;
-  march_pixel_fast<ST, FILT, FULL>(u, v, px, py, s_t0, s_t1, s_aux, kThreads, threadIdx.x);
+  march_pixel_fast<ST, FILT, FULL, false, LB>(u, v, px, py, s_t0, s_t1, s_aux, kThreads, threadIdx.x);
 }
 
 // The instrumented build of the same kernel (psc_count_fetches): every
@@ -70,14 +70,14 @@ cudaError_t launch_fast_tally(const MarchUniforms& u, const ViewDev& v, unsigned
   return cudaGetLastError();
 }
 
-template <int ST, int FILT>
+template <int ST, int FILT, int LB = 0>
 cudaError_t launch_fast(const MarchUniforms& u, const ViewDev& v, cudaStream_t s) {
   const dim3 grid((v.width + kTileW - 1) / kTileW, (v.height + kTileH - 1) / kTileH);
   const size_t smem = (2u * u.layer_count + kAuxWords) * kThreads * sizeof(float);
   if (needs_full_paths(&u, 1))
-    k_march_fast<ST, FILT, true><<<grid, kThreads, smem, s>>>(u, v);
+    k_march_fast<ST, FILT, true, LB><<<grid, kThreads, smem, s>>>(u, v);
   else
-    k_march_fast<ST, FILT, false><<<grid, kThreads, smem, s>>>(u, v);
+    k_march_fast<ST, FILT, false, LB><<<grid, kThreads, smem, s>>>(u, v);
   return cudaGetLastError();
 }
 
@@ -109,7 +109,12 @@ int launch_march_fast(const MarchUniforms& u, const ViewDev& v, const PscMarchOp
     else if (o.storage == PSC_STORAGE_F16) e = launch_fast<PSC_STORAGE_F16, PSC_FILTER_TEXTURE>(u, v, s);
     else return PSC_ERR_UNSUPPORTED;
   } else if (o.filter == PSC_FILTER_HYBRID) {
+    // the light-march fetch batch is chosen for the F16 hybrid form only
     if (o.storage == PSC_STORAGE_U8) e = launch_fast<PSC_STORAGE_U8, PSC_FILTER_HYBRID>(u, v, s);
+    else if (o.storage == PSC_STORAGE_F16 && o.light_batch == 2)
+      e = launch_fast<PSC_STORAGE_F16, PSC_FILTER_HYBRID, 2>(u, v, s);
+    else if (o.storage == PSC_STORAGE_F16 && o.light_batch == 3)
+      e = launch_fast<PSC_STORAGE_F16, PSC_FILTER_HYBRID, 3>(u, v, s);
     else if (o.storage == PSC_STORAGE_F16) e = launch_fast<PSC_STORAGE_F16, PSC_FILTER_HYBRID>(u, v, s);
     else return PSC_ERR_UNSUPPORTED;
   } else {

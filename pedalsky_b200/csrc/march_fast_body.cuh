@@ -475,17 +475,26 @@ __device__ __forceinline__ void light_taps(const MarchUniforms& u, const LayerCo
   }
 }
 
-template <int ST, class Prof, bool HCHECK, bool POLY, bool FULL>
+// LB: taps per fetch batch (PscMarchOptions.light_batch).  0: six taps (the
+// reference default) in one batch, other counts in batches of 4, 2, 1; 3 or
+// 2: batches of that many, then 2, 1.  The taps are summed in the same order
+// whatever the batching.
+template <int ST, class Prof, bool HCHECK, bool POLY, bool FULL, int LB = 0>
 __device__ __forceinline__ float light_march_tex(const MarchUniforms& u, const LayerConst& L,
                                                  const LightRay& lr, const Prof& prof) {
   const uint32_t n = u.light_steps;
   float od = 0.0f, comp = 0.0f;
   uint32_t i = 0;
-  if (n == 6u) {  // the reference default: all six fetches in one batch
-    light_taps<ST, Prof, HCHECK, 6, POLY, FULL>(u, L, lr, prof, 0u, od, comp);
-    return od;
+  if constexpr (LB == 0) {
+    if (n == 6u) {  // the reference default: all six fetches in one batch
+      light_taps<ST, Prof, HCHECK, 6, POLY, FULL>(u, L, lr, prof, 0u, od, comp);
+      return od;
+    }
+    for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, HCHECK, 4, POLY, FULL>(u, L, lr, prof, i, od, comp);
+  } else {
+    for (; i + (uint32_t)LB <= n; i += (uint32_t)LB)
+      light_taps<ST, Prof, HCHECK, (uint32_t)LB, POLY, FULL>(u, L, lr, prof, i, od, comp);
   }
-  for (; i + 4u <= n; i += 4u) light_taps<ST, Prof, HCHECK, 4, POLY, FULL>(u, L, lr, prof, i, od, comp);
   if (i + 2u <= n) {
     light_taps<ST, Prof, HCHECK, 2, POLY, FULL>(u, L, lr, prof, i, od, comp);
     i += 2u;
@@ -495,7 +504,7 @@ __device__ __forceinline__ float light_march_tex(const MarchUniforms& u, const L
 }
 
 // Optical depth toward the sun (cloud_march.wgsl:543-578).
-template <int ST, int FILT, bool FULL = true>
+template <int ST, int FILT, bool FULL = true, int LB = 0>
 __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerConst& L, float px,
                                           float py, float pz, float alt, float eff, uint32_t type,
                                           float ux, float uy, float uz) {
@@ -530,17 +539,17 @@ __device__ __forceinline__ float light_od(const MarchUniforms& u, const LayerCon
       lr.c1 = cv * lr.ih;
       lr.c2 = s2 * lr.ih;
       lr.c3 = -cv * __fdividef(s2, r0) * lr.ih;
-      if (FULL && type == 7u) return light_march_tex<ST, NdfCb, true, true, FULL>(u, L, lr, NdfCb{L.anvil_bias});
+      if (FULL && type == 7u) return light_march_tex<ST, NdfCb, true, true, FULL, LB>(u, L, lr, NdfCb{L.anvil_bias});
       // heights rise along the light path when cos(up, sun) >= 0 (the cubic's
       // slope stays positive over 20 km), so the first tap bounds them all
       const float t_first = 0.5f * step;
       const float h_first = fmaf(t_first, fmaf(t_first, fmaf(t_first, lr.c3, lr.c2), lr.c1), lr.c0);
       if (!FULL && cv >= 0.0f && h_first * gen.k.inv_a >= 1.0001f)  // lean form only
-        return light_march_tex<ST, NdfTop, false, true, FULL>(u, L, lr, NdfTop{gen.k});
-      return light_march_tex<ST, NdfGeneral, false, true, FULL>(u, L, lr, gen);
+        return light_march_tex<ST, NdfTop, false, true, FULL, LB>(u, L, lr, NdfTop{gen.k});
+      return light_march_tex<ST, NdfGeneral, false, true, FULL, LB>(u, L, lr, gen);
     }
-    if (FULL && type == 7u) return light_march_tex<ST, NdfCb, true, false, FULL>(u, L, lr, NdfCb{L.anvil_bias});
-    return light_march_tex<ST, NdfGeneral, false, false, FULL>(u, L, lr, gen);
+    if (FULL && type == 7u) return light_march_tex<ST, NdfCb, true, false, FULL, LB>(u, L, lr, NdfCb{L.anvil_bias});
+    return light_march_tex<ST, NdfGeneral, false, false, FULL, LB>(u, L, lr, gen);
   }
   float od = 0.0f, comp = 0.0f;
   for (uint32_t i = 0; i < u.light_steps; ++i) {
@@ -675,8 +684,9 @@ static_assert(kTallyKinds == kFetchTallyKinds, "one tally counter per PscFetchCo
 // TALLY = true is the instrumented build behind psc_count_fetches: the same
 // arithmetic, and `tc` (kTallyKinds counters of this thread) counts every
 // fetch issued; the timed kernels are built with TALLY = false, where `tc`
-// is unused and the counting compiles away.
-template <int ST, int FILT, bool FULL = true, bool TALLY = false>
+// is unused and the counting compiles away.  LB is the light-march fetch
+// batch (light_march_tex).
+template <int ST, int FILT, bool FULL = true, bool TALLY = false, int LB = 0>
 __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const ViewDev& v, uint32_t px,
                                                  uint32_t py, float* s_t0, float* s_t1, float* s_aux,
                                                  uint32_t stride, uint32_t slot, uint32_t* tc = nullptr) {
@@ -844,7 +854,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
               tc[kTallyTrans] += trans_fetched ? 1u : 0u;
               tc[kTallyLight] += (FULL && u.cone) ? 6u : u.light_steps;
             }
-            const float od = light_od<ST, FILT, FULL>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
+            const float od = light_od<ST, FILT, FULL, LB>(u, L, px3, py3, pz3, alt, eff, type, ux, uy, uz);
             const float st_r = L.sigma_t[0], st_g = L.sigma_t[1], st_b = L.sigma_t[2];
             const float xr = st_r * od, xg = st_g * od, xb = st_b * od;
             // e[n] = exp(-x * b^n); with b = 1/2 one exponential at n = 3 and

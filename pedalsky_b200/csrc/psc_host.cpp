@@ -1494,10 +1494,18 @@ int psc_set_options(psc_ctx* c, const PscMarchOptions* o) {
   if (o->filter == PSC_FILTER_TEXTURE && o->storage == PSC_STORAGE_F16 && o->schedule != PSC_SCHED_FAST)
     return fail(PSC_ERR_UNSUPPORTED, "F16 texture volumes are read by the FAST schedule only");
   if (o->half_res > 1 || o->taa > 1) return fail(PSC_ERR_INVALID_ARGUMENT, "half_res and taa are 0 or 1");
+  if (o->light_batch != 0 && o->light_batch != 2 && o->light_batch != 3)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "light_batch is 0, 2 or 3 (got %u)", o->light_batch);
   const float hv[] = {o->hg_g_forward, o->hg_g_backward, o->hg_blend};
   if (!all_finite(hv, 3)) return fail(PSC_ERR_NOT_FINITE, "non-finite HG lobe");
   if (o->storage != c->opts.storage || o->filter != c->opts.filter) c->tex_dirty = true;
   c->opts = *o;
+  return PSC_OK;
+}
+
+int psc_get_options(psc_ctx* c, PscMarchOptions* out) {
+  if (!c || !out) return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  *out = c->opts;
   return PSC_OK;
 }
 
@@ -1933,6 +1941,7 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
   // place (cudaGraphExecUpdate) instead of instantiating a new one.
   std::vector<uint64_t> key = {c->batch_tuning.form, n, n_tiles, c->batch_tuning.threads,
                                c->batch_tuning.tile_w, c->opts.storage, c->opts.filter, c->opts.composite,
+                               c->opts.light_batch,
                                (uint64_t)(uintptr_t)c->d_bu, (uint64_t)(uintptr_t)c->d_btiles,
                                (uint64_t)(uintptr_t)c->d_bframes,
                                (uint64_t)(uintptr_t)c->d_base_store, (uint64_t)c->tex_base,
@@ -1981,6 +1990,7 @@ int psc_autotune_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32
   if (!c || !views || !n) return fail(PSC_ERR_INVALID_ARGUMENT, "null or empty batch");
   if (reps == 0 || reps > 100) return fail(PSC_ERR_INVALID_ARGUMENT, "reps must be 1..100");
   const PscBatchTuning saved = c->batch_tuning;
+  const uint32_t saved_lb = c->opts.light_batch;
   // {form, threads, tile_w}: the persistent form at each launch shape, and
   // the per-view form (whose kernels have their own fixed shape)
   static const uint32_t cand[][3] = {{PSC_BATCH_PERSISTENT, 128, 16}, {PSC_BATCH_PERSISTENT, 128, 32},
@@ -1992,35 +2002,59 @@ int psc_autotune_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32
   cudaEvent_t a = nullptr, b = nullptr;
   PSC_CUDA(cudaEventCreate(&a), "event");
   PSC_CUDA(cudaEventCreate(&b), "event");
-  float best_t = INFINITY;
-  PscBatchTuning best_tu = saved;
-  int rc = PSC_OK;
-  for (const auto& cd : cand) {
-    c->batch_tuning = PscBatchTuning{cd[1], cd[2], 0, cd[0]};
-    rc = psc_render_batch(c, views, n, stream);  // warm-up
-    if (rc) break;
+  // median of `reps` timed runs of the current tuning and options, after one warm-up
+  auto time_current = [&](float* med) -> int {
+    int rc = psc_render_batch(c, views, n, stream);
+    if (rc) return rc;
     std::vector<float> ts;
-    for (uint32_t r = 0; r < reps && !rc; ++r) {
+    for (uint32_t r = 0; r < reps; ++r) {
       cudaEventRecord(a, s);
       rc = psc_render_batch(c, views, n, stream);
       cudaEventRecord(b, s);
-      if (cudaEventSynchronize(b) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "autotune sync");
+      if (rc) return rc;
+      if (cudaEventSynchronize(b) != cudaSuccess) return cuda_fail(cudaGetLastError(), "autotune sync");
       float ms = 0.0f;
       cudaEventElapsedTime(&ms, a, b);
       ts.push_back(ms);
     }
-    if (rc) break;
     std::sort(ts.begin(), ts.end());
-    const float med = ts[ts.size() / 2];
+    *med = ts[ts.size() / 2];
+    return PSC_OK;
+  };
+  float best_t = INFINITY;
+  PscBatchTuning best_tu = saved;
+  uint32_t best_lb = saved_lb;
+  int rc = PSC_OK;
+  for (const auto& cd : cand) {
+    c->batch_tuning = PscBatchTuning{cd[1], cd[2], 0, cd[0]};
+    float med = 0.0f;
+    rc = time_current(&med);
+    if (rc) break;
     if (med < best_t) {
       best_t = med;
       best_tu = c->batch_tuning;
+    }
+  }
+  // the light-march fetch batch in the fastest launch shape (F16 hybrid)
+  if (!rc && c->opts.storage == PSC_STORAGE_F16 && c->opts.filter == PSC_FILTER_HYBRID) {
+    c->batch_tuning = best_tu;
+    for (uint32_t lb : {0u, 3u, 2u}) {
+      if (lb == saved_lb) continue;  // timed above
+      c->opts.light_batch = lb;
+      float med = 0.0f;
+      rc = time_current(&med);
+      if (rc) break;
+      if (med < best_t) {
+        best_t = med;
+        best_lb = lb;
+      }
     }
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   best_tu.use_graph = saved.use_graph;
   c->batch_tuning = rc ? saved : best_tu;
+  c->opts.light_batch = rc ? saved_lb : best_lb;
   if (rc) return rc;
   if (best) *best = best_tu;
   if (best_ms) *best_ms = best_t;

@@ -149,6 +149,7 @@ def test_autotuner_picks_a_valid_shape(small_batch, oracle_noise):
     t = capi.BatchTuning()
     call("psc_get_batch_tuning", sub.handle, C.byref(t))
     assert (t.threads, t.tile_w, t.form) == (res["threads"], res["tile_w"], res["form_id"])
+    assert res["light_batch"] in (0, 2, 3)
     sub.close()
 
 
@@ -205,3 +206,49 @@ def test_batch_views_match_the_fp64_oracle(oracle, oracle_noise, form):
             assert st["ssim"] >= 0.999, (i, st)
     finally:
         sub.close()
+
+
+@pytest.mark.parametrize("light_batch", [2, 3])
+def test_light_batch_keeps_the_image(small_batch, oracle_noise, light_batch):
+    """options.light_batch changes how many light-march taps are fetched
+    together, not the sums: transmittance is bit-identical and luminance
+    within the rounding of the tap positions, in both batch forms and in
+    psc_render."""
+    torch = _gpu.torch_cuda()
+    for form in (capi.BATCH_PERSISTENT, capi.BATCH_PER_VIEW):
+        ref = _run_batch(small_batch, oracle_noise, (128, 16, 0, form))
+        sub = subsystem_for_scene(small_batch[0], luts=None, noise=oracle_noise)
+        o = capi.MarchOptions.from_buffer_copy(sub.options)
+        o.light_batch = light_batch
+        sub.set_options(o)
+        b = B.Batch(small_batch, "cuda:0", outputs=("luminance", "transmittance"))
+        B.set_tuning(sub.handle, 128, 16, 1, form)
+        b.render(sub.handle)
+        torch.cuda.synchronize()
+        for (L0, T0), L1, T1 in zip(ref, b.lum, b.trans):
+            L1, T1 = L1.cpu().numpy(), T1.cpu().numpy()
+            assert np.array_equal(T0, T1)
+            assert (np.abs(L1 - L0)[..., :3] / np.maximum(np.abs(L0[..., :3]), 1.0)).max() <= 1e-5
+        sub.close()
+    s1 = small_batch[1]
+    L0, T0 = _single(s1, oracle_noise)
+    sub = subsystem_for_scene(s1, luts=None, noise=oracle_noise)
+    o = capi.MarchOptions.from_buffer_copy(sub.options)
+    o.light_batch = light_batch
+    sub.set_options(o)
+    dev = torch.device("cuda", 0)
+    L = torch.zeros((s1.height, s1.width, 4), device=dev)
+    T = torch.zeros_like(L)
+    depth = torch.from_numpy(s1.depth).to(dev)
+    v = capi.View(s1.width, s1.height, depth.data_ptr(), L.data_ptr(), T.data_ptr(), None)
+    call("psc_render", sub.handle, C.byref(v), 1, None)
+    torch.cuda.synchronize()
+    assert np.array_equal(T.cpu().numpy(), T0)
+    assert (np.abs(L.cpu().numpy() - L0)[..., :3] / np.maximum(np.abs(L0[..., :3]), 1.0)).max() <= 1e-5
+    got = capi.MarchOptions()
+    call("psc_get_options", sub.handle, C.byref(got))
+    assert got.light_batch == light_batch
+    o.light_batch = 5
+    with pytest.raises(PscError):
+        sub.set_options(o)
+    sub.close()
