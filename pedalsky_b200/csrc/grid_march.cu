@@ -70,30 +70,6 @@ __device__ __forceinline__ Tri grid_coords(const GridDev& g, float x, float alt,
   return t;
 }
 
-// Visits the (up to 8) in-grid corners with their trilinear weights.
-template <class F>
-__device__ __forceinline__ void grid_corners(const GridDev& g, const Tri& t, F&& fn) {
-#pragma unroll
-  for (int dy = 0; dy < 2; ++dy) {
-    const int Y = t.y0 + dy;
-    if (Y < 0 || Y >= (int)g.ny) continue;
-    const float wy = dy ? t.wy : 1.0f - t.wy;
-#pragma unroll
-    for (int dz = 0; dz < 2; ++dz) {
-      const int Z = t.z0 + dz;
-      if (Z < 0 || Z >= (int)g.nz) continue;
-      const float wyz = wy * (dz ? t.wz : 1.0f - t.wz);
-      const uint32_t row = ((uint32_t)Y * g.nz + (uint32_t)Z) * g.nx;
-#pragma unroll
-      for (int dx = 0; dx < 2; ++dx) {
-        const int X = t.x0 + dx;
-        if (X < 0 || X >= (int)g.nx) continue;
-        fn(row + (uint32_t)X, wyz * (dx ? t.wx : 1.0f - t.wx));
-      }
-    }
-  }
-}
-
 // Trilinear fetch without per-corner branches: corner indices clamped into
 // the grid (so every load is in bounds) and the weights of corners outside
 // it zeroed, which gives the same sum as visiting the in-grid corners only;
@@ -121,9 +97,34 @@ __device__ __forceinline__ float grid_fetch(const GridDev& g, const Tri& t) {
   return v;
 }
 
+// Adds val x the trilinear weights into the gradient grid: the corners'
+// in-grid flags, clamped indices and weights as in grid_fetch, one atomic add
+// per in-grid corner of non-zero weight (a corner outside the grid has
+// weight zero and is skipped).
 __device__ __forceinline__ void grid_scatter(const GridDev& g, const Tri& t, float val) {
   if (val == 0.0f) return;
-  grid_corners(g, t, [&](uint32_t i, float w) { atomicAdd(g.grad + i, w * val); });
+  const bool x0 = (uint32_t)t.x0 < g.nx, x1 = (uint32_t)(t.x0 + 1) < g.nx;
+  const bool y0 = (uint32_t)t.y0 < g.ny, y1 = (uint32_t)(t.y0 + 1) < g.ny;
+  const bool z0 = (uint32_t)t.z0 < g.nz, z1 = (uint32_t)(t.z0 + 1) < g.nz;
+  if (!((x0 || x1) && (y0 || y1) && (z0 || z1))) return;
+  const float wx[2] = {x0 ? (1.0f - t.wx) * val : 0.0f, x1 ? t.wx * val : 0.0f};
+  const float wy[2] = {y0 ? 1.0f - t.wy : 0.0f, y1 ? t.wy : 0.0f};
+  const float wz[2] = {z0 ? 1.0f - t.wz : 0.0f, z1 ? t.wz : 0.0f};
+  const uint32_t cx[2] = {(uint32_t)min(max(t.x0, 0), (int)g.nx - 1), (uint32_t)min(max(t.x0 + 1, 0), (int)g.nx - 1)};
+  const uint32_t cy[2] = {(uint32_t)min(max(t.y0, 0), (int)g.ny - 1), (uint32_t)min(max(t.y0 + 1, 0), (int)g.ny - 1)};
+  const uint32_t cz[2] = {(uint32_t)min(max(t.z0, 0), (int)g.nz - 1), (uint32_t)min(max(t.z0 + 1, 0), (int)g.nz - 1)};
+#pragma unroll
+  for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz) {
+      const float wyz = wy[dy] * wz[dz];
+      float* row = g.grad + (cy[dy] * g.nz + cz[dz]) * g.nx;
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        const float w = wyz * wx[dx];
+        if (w != 0.0f) atomicAdd(row + cx[dx], w);
+      }
+    }
 }
 
 // Light march geometry (cloud_march.wgsl:543-578).
