@@ -469,7 +469,9 @@ int psc_composite(const float* luminance, const float* transmittance,
  * Synchronous; allocates and frees a 112-byte counter buffer. */
 typedef struct PscFetchCounts {
   uint64_t rays;                /* pixels marched                          */
-  uint64_t primary_steps;       /* primary steps executed                  */
+  uint64_t primary_steps;       /* primary steps executed (the steps of a
+                                   layer outside the altitude band where the
+                                   profile test can pass are not run)      */
   uint64_t live_steps;          /* steps past the profile bound: one base-
                                    shape tap and one curl tap each          */
   uint64_t weather_taps;        /* bilinear weather taps (0: uniform map)  */

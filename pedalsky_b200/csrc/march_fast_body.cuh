@@ -651,6 +651,49 @@ __device__ __forceinline__ float weather_fast(const MarchUniforms& u, float uu, 
   return lerpf(a, b, wy);
 }
 
+// The primary steps of a ray's layer segment that can pass the profile test
+// (no type grid): those whose altitude lies in the layer's band
+// [live_lo, live_hi] (LayerConst), found from the ray's geometry instead of
+// stepping through the rest.  Along the ray, |o + t d| = R + a at
+// t = tv -/+ sqrt((R + a)^2 - rp^2) with tv = -r0 cos(up, d) and rp the
+// line's closest distance to the planet centre, so the altitude stays at or
+// below a_hi on [tv - sqrt(q_hi), tv + sqrt(q_hi)] and falls below a_lo only
+// inside (tv - sqrt(q_lo), tv + sqrt(q_lo)); the hull of what remains in
+// [t0, t1] becomes step indices.  In FP64 from the FP32 r0 and cos(up, d)
+// the ray carries (their rounding moves t by about 1 m at most), with the
+// band widened by 3 m more and the index range by 2-3 steps: every step that
+// could pass the test is inside [s_begin, s_end), and the steps outside add
+// nothing and leave the transmittance as it is, so skipping them is exact.
+// Returns false when no step of the segment can pass.
+__device__ __forceinline__ bool live_step_range(float r0f, float ray_B, const LayerConst& L, float R,
+                                                float t0, float t1, float step, float jitter,
+                                                uint32_t n, uint32_t& s_begin, uint32_t& s_end) {
+  const double r0 = r0f, cv = (double)ray_B / (2.0 * fmax(r0, 1.0));
+  const double tv = -r0 * cv;
+  const double rp2 = r0 * r0 * fmax(1.0 - cv * cv, 0.0);
+  const double rh = (double)R + ((double)L.live_hi + 3.0), rl = (double)R + ((double)L.live_lo - 3.0);
+  const double qh = rh * rh - rp2;
+  if (qh < 0.0) return false;  // the line stays above the band
+  const double sh = sqrt(qh);
+  double lo = fmax((double)t0, tv - sh), hi = fmin((double)t1, tv + sh);
+  if (lo > hi) return false;
+  const double ql = rl * rl - rp2;
+  if (ql > 0.0) {  // the open interval where the altitude is below the band
+    const double sl = sqrt(ql), c = tv - sl, d = tv + sl;
+    const bool p1 = lo <= fmin(hi, c), p2 = fmax(lo, d) <= hi;
+    if (!p1 && !p2) return false;
+    const double nlo = p1 ? lo : fmax(lo, d), nhi = p2 ? hi : fmin(hi, c);
+    lo = nlo;
+    hi = nhi;
+  }
+  const double is = 1.0 / (double)step;
+  const double fb = floor((lo - (double)t0) * is - (double)jitter) - 2.0;
+  const double fe = ceil((hi - (double)t0) * is - (double)jitter) + 3.0;
+  s_begin = fb <= 0.0 ? 0u : (fb >= (double)n ? n : (uint32_t)fb);
+  s_end = fe <= 0.0 ? 0u : (fe >= (double)n ? n : (uint32_t)fe);
+  return s_begin < s_end;
+}
+
 // 1 - exp(-y) without cancellation for small y.
 __device__ __forceinline__ float one_minus_exp_neg(float y, float e) {
   return y < 0.03f ? y * fmaf(y, fmaf(y, fmaf(y, -1.0f / 24.0f, 1.0f / 6.0f), -0.5f), 1.0f)
@@ -748,6 +791,13 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
     const float segment = t1 - t0;
     if (segment <= 0.0f) continue;
     const float step = __fdividef(segment, (float)u.cloud_steps);
+    uint32_t s_begin = 0u, s_end = u.cloud_steps;
+    if (!(FULL && u.type_grid)) {  // the profile test depends on the altitude alone
+      if (!(L.live_lo <= L.live_hi)) continue;  // no step of this layer can pass it
+      if (!live_step_range(ray_r0, ray_B, L, u.planet_r, t0, t1, step, jitter, u.cloud_steps, s_begin,
+                           s_end))
+        continue;
+    }
     const bool cb = FULL && L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE;
 
     // per ray and layer: a^n * phase_n * forward gain (shared memory)
@@ -782,7 +832,7 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
       }
     }
 
-    for (uint32_t s = 0; s < u.cloud_steps; ++s) {
+    for (uint32_t s = s_begin; s < s_end; ++s) {
       if constexpr (TALLY) ++tc[kTallySteps];
       const float t = fmaf((float)s + jitter, step, t0);
       const float px3 = fmaf(dx, t, cx), py3 = fmaf(dy, t, cy), pz3 = fmaf(dz, t, cz);

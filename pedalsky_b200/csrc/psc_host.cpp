@@ -199,6 +199,49 @@ void wind_cache(const psc_ctx* c, const PscCloudParamsGpu& p, const PscFrameUnif
 
 // Flatten one view's scene (params, layers, frame) plus the context's world,
 // options and inputs into the kernel's uniform block.
+// The layer's profile (cloud_density_common.wgsl:49-91) in double, as the
+// FAST march evaluates it: types 0..6 through the coefficients in `o`,
+// Cumulonimbus by its own formula, any other type 0.
+double profile_h(const PscCloudLayerGpu& L, const psc::LayerConst& o, double h) {
+  auto S = [](double t) {
+    t = std::fmin(std::fmax(t, 0.0), 1.0);
+    return t * t * (3.0 - 2.0 * t);
+  };
+  if (o.ndf_mode) return S(h * o.ndf_inv_a) * S(h * o.ndf_inv_w1 + o.ndf_b1);
+  if (L.cloud_type != 7u) return 0.0;
+  const double base = S(h / 0.05), mid = S((h - 0.95) / -0.45);
+  const double anvil = S((h - 0.7) / 0.2) * 1.5 * std::fmin(std::fmax((double)L.anvil_bias, 0.0), 2.0);
+  const double mt = S((h - 0.65) / 0.15);
+  return base * (mid * (1.0 - mt) + anvil * mt);
+}
+
+// LayerConst::live_lo / live_hi: the hull of the normalised heights whose
+// profile can pass the FAST march's test (nd * 1.000001 - skip_k) *
+// density_scale > 1e-3, found on a 1/20000 grid with the threshold lowered by
+// 1e-4 and widened by 1e-3 of the height and then 1 m of altitude, so that
+// the kernel's FP32 evaluation of any passing step lies inside it.
+void live_band(const PscCloudLayerGpu& L, psc::LayerConst& o) {
+  const int M = 20000;
+  int first = -1, last = -1;
+  for (int i = 0; i <= M; ++i) {
+    const double h = (double)i / M;
+    if ((profile_h(L, o, h) * 1.000001 - o.skip_k) * o.density_scale > 1e-3 * (1.0 - 1e-4)) {
+      if (first < 0) first = i;
+      last = i;
+    }
+  }
+  if (first < 0) {
+    o.live_lo = 1.0f;
+    o.live_hi = 0.0f;
+    return;
+  }
+  const double thick = 1.0 / (double)o.inv_thickness;
+  const double h_lo = std::fmax((double)(first - 2) / M - 1e-3, 0.0);
+  const double h_hi = std::fmin((double)(last + 2) / M + 1e-3, 1.0);
+  o.live_lo = (float)((double)o.base_m + h_lo * thick - 1.0);
+  o.live_hi = (float)((double)o.base_m + h_hi * thick + 1.0);
+}
+
 void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscCloudLayerGpu* layers,
                         const PscFrameUniformsGpu& f, uint32_t width, uint32_t height,
                         psc::MarchUniforms& u) {
@@ -346,6 +389,7 @@ void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscC
     }
     o.skew_kx = o.skew_x * o.skew_thickness;
     o.skew_kz = o.skew_z * o.skew_thickness;
+    live_band(L, o);
     o.r_bottom = (double)w.planet_radius_m + (double)L.base_m;
     o.r_top = (double)w.planet_radius_m + (double)L.top_m;
   }

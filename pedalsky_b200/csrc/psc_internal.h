@@ -54,6 +54,11 @@ struct LayerConst {
   // value nd has (nd - skip_k) * density_scale <= 1e-3 cannot be dense.
   float skip_k;
   float skew_kx, skew_kz;  // skew_x * skew_thickness, skew_z * skew_thickness
+  // Altitude band (m) outside which no primary step can pass the profile
+  // test above (no type grid): the host's hull of the heights where it can,
+  // widened; live_lo > live_hi when no height can.  The FAST march turns it
+  // into the range of step indices it runs.
+  float live_lo, live_hi;
   double r_bottom, r_top;  // planet_radius + base/top, FP64
 };
 

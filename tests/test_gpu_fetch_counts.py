@@ -52,8 +52,10 @@ def test_fetch_counts_match_the_timed_kernel_and_the_oracle(oracle, oracle_noise
     print(f"\n[fetch counts] {storage}/{filt}: kernel {c}\n  oracle {oc}")
     n = s.width * s.height
     assert c["rays"] == n and c["depth_loads"] == n
-    # the same steps are executed (branch flips move a handful of samples)
-    assert abs(c["primary_steps"] - oc["steps"]) <= 1e-3 * oc["steps"]
+    # the kernel runs only the steps of each layer whose altitude can pass
+    # the profile test, so it executes fewer steps than the reference
+    # algorithm, and the same dense samples (branch flips move a handful)
+    assert c["live_steps"] <= c["primary_steps"] <= oc["steps"]
     assert abs(c["dense_samples"] - oc["dense"]) <= 1e-3 * oc["dense"]
     # the fetches the kernel proves unnecessary are skipped: a uniform
     # weather map is not sampled, and steps whose profile bound keeps them
