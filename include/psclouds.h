@@ -628,6 +628,26 @@ int psc_layer_gradient(psc_ctx* ctx, const PscDensityGrid* grid, const PscView* 
                        const float* background, const float* target, double* grad_base_top,
                        void* stream);
 
+/* Gradient of the procedural march's image loss with respect to the density
+ * parameters of scene layer `layer` (cloud_march.wgsl:432-530,
+ * sample_density): grad[0..3] += d loss / d coverage, shape_bias,
+ * detail_bias, density_scale (device doubles); *loss += the loss when
+ * `loss` is not null.  Same loss as psc_adjoint: I = L + background * T per
+ * pixel and channel, sum((I - target)^2) / (3 * viewport_w * viewport_h)
+ * over the view's rectangle (`background`, `target`: device float4 per
+ * pixel), so row bands of one viewport add up.  No counterpart in the
+ * reference.  Forward mode through the whole march (density, light march,
+ * octaves, step integral, transmittance, aerial perspective), FP32 per ray
+ * in the PLAIN schedule's arithmetic with exact filtering of the context's
+ * noise storage, summed in double; branch decisions (the 1e-3 density
+ * threshold, the coverage gate, the early exit) are held at their values.
+ * The shape and detail biases act through the diurnal modulation, so their
+ * derivatives are 0 for non-convective layer types or diurnal_strength 0.
+ * The view's output pointers are not used. */
+int psc_layer_param_gradient(psc_ctx* ctx, const PscView* view, uint32_t layer,
+                             const float* background, const float* target, double* grad,
+                             double* loss, void* stream);
+
 /* ------------------------------------------------ allocation-free batch */
 
 #define PSC_NOALLOC_MAX_VIEWS 64u

@@ -30,6 +30,7 @@ CUDA_UNITS = {
     "march_noalloc.cu": [],
     "grid_march.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "grid_layer_grad.cu": ["-prec-div=false", "-prec-sqrt=false"],
+    "march_param_grad.cu": [],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
     "fetch_peak.cu": [],

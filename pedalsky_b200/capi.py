@@ -220,6 +220,7 @@ _PROTOS = {
     "psc_render_grid": [_vp, P(DensityGrid), P(View), _vp],
     "psc_adjoint": [_vp, P(DensityGrid), P(View), _vp, _vp, _vp, _vp, _vp, _vp],
     "psc_layer_gradient": [_vp, P(DensityGrid), P(View), _vp, _vp, _vp, _vp],
+    "psc_layer_param_gradient": [_vp, P(View), u32, _vp, _vp, _vp, _vp, _vp],
     "psc_measure_fetch_peaks": [i32, P(FetchPeaks), _vp],
     "psc_cloud_rt_size": [u32, u32, u32, P(u32), P(u32)],
     "psc_taa_resolve": [_vp, _vp, _vp, u32, u32, _vp, _vp, _vp],

@@ -233,9 +233,21 @@ void live_band(const PscCloudLayerGpu& L, psc::LayerConst& o) {
   if (first < 0) {
     o.live_lo = 1.0f;
     o.live_hi = 0.0f;
+    o.light_h_dead = 2.0f;  // no primary step is dense, so no light march runs
     return;
   }
   const double thick = 1.0 / (double)o.inv_thickness;
+  // light-march taps: the density of a tap is exactly 0 once its profile
+  // value is at or below skip_k (the base shape is at most 1 and 1 - eff is
+  // at least skip_k); above the last height where it can exceed skip_k
+  // (threshold lowered by 1e-4, widened by 2 grid cells and 1e-3) every tap
+  // adds 0
+  {
+    int last_light = -1;
+    for (int i = 0; i <= M; ++i)
+      if (profile_h(L, o, (double)i / M) * 1.000001 > (double)o.skip_k - 1e-4) last_light = i;
+    o.light_h_dead = last_light < 0 ? -1.0f : (float)((double)(last_light + 2) / M + 1e-3);
+  }
   const double h_lo = std::fmax((double)(first - 2) / M - 1e-3, 0.0);
   const double h_hi = std::fmin((double)(last + 2) / M + 1e-3, 1.0);
   o.live_lo = (float)((double)o.base_m + h_lo * thick - 1.0);
@@ -1742,7 +1754,7 @@ namespace {
 // Input, option and view checks of a march call (psc_render,
 // psc_count_fetches); builds the noise storage form and the texture objects
 // the march reads.
-int prepare_render(psc_ctx* c, const PscView* views, uint32_t n, bool rt_form) {
+int prepare_render(psc_ctx* c, const PscView* views, uint32_t n, bool rt_form, bool outputs_required = true) {
   if (!c->have_frame) return fail(PSC_ERR_MISSING_INPUT, "psc_set_frame was not called");
   if (!c->have_base || !c->have_detail || !c->have_curl || !c->have_blue)
     return fail(PSC_ERR_MISSING_INPUT, "noise volumes missing (psc_bake_noise or psc_upload_noise)");
@@ -1768,9 +1780,10 @@ int prepare_render(psc_ctx* c, const PscView* views, uint32_t n, bool rt_form) {
         (uint64_t)v.x_offset + v.width > vw || (uint64_t)v.y_offset + v.height > vh)
       return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: rectangle %ux%u at (%u,%u) exceeds viewport %ux%u",
                   i, v.width, v.height, v.x_offset, v.y_offset, vw, vh);
-    if (!v.out_luminance && !v.out_transmittance && !(c->opts.composite && v.hdr))
+    if (outputs_required && !v.out_luminance && !v.out_transmittance && !(c->opts.composite && v.hdr))
       return fail(PSC_ERR_INVALID_ARGUMENT, "view %u has no output buffer", i);
-    if (c->opts.composite && !v.hdr) return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: composite needs hdr", i);
+    if (outputs_required && c->opts.composite && !v.hdr)
+      return fail(PSC_ERR_INVALID_ARGUMENT, "view %u: composite needs hdr", i);
     if (rt_form && (v.x_offset || v.y_offset || vw != v.width || vh != v.height))
       return fail(PSC_ERR_INVALID_ARGUMENT, "the half-res / TAA forms render whole viewports");
   }
@@ -2241,6 +2254,40 @@ int psc_layer_gradient(psc_ctx* c, const PscDensityGrid* g, const PscView* v, co
   gd.target = reinterpret_cast<const float4*>(target);
   rc = psc::launch_grid_layer_grad(u, vd, gd, grad_base_top, static_cast<cudaStream_t>(stream));
   if (rc) return fail(rc, "layer-gradient launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  ++c->launches;
+  return PSC_OK;
+}
+
+int psc_layer_param_gradient(psc_ctx* c, const PscView* v, uint32_t layer, const float* background,
+                             const float* target, double* grad, double* loss, void* stream) {
+  if (!c || !v || !background || !target || !grad)
+    return fail(PSC_ERR_INVALID_ARGUMENT, "null argument");
+  if (layer >= c->n_layers) return fail(PSC_ERR_INVALID_ARGUMENT, "layer %u of %u", layer, c->n_layers);
+  int rc = prepare_render(c, v, 1, false, false);
+  if (rc) return rc;
+  const uint32_t vw = v->viewport_w ? v->viewport_w : v->width, vh = v->viewport_h ? v->viewport_h : v->height;
+  psc::MarchUniforms u;
+  build_uniforms(c, vw, vh, u);
+  const psc::ViewDev vd{v->width, v->height, v->x_offset, v->y_offset, v->depth, nullptr, nullptr, nullptr};
+  // diurnal_modulation of the layer (as build_uniforms_for): the shape and
+  // detail biases act through it
+  const PscCloudLayerGpu& L = c->layers[layer];
+  const PscCloudParamsGpu& p = c->params;
+  const uint32_t t = L.cloud_type;
+  const bool conv = t == 0 || t == 2 || t == 3 || t == 7;
+  const float di = (p.diurnal_strength == 0.0f || !conv)
+                       ? 0.0f
+                       : smoothstep_h(-0.1f, 0.4f, c->frame.sun_direction[1]) * p.diurnal_strength;
+  const float ld_raw = p.detail_strength + L.detail_bias * di;
+  psc::ParamGradDev g;
+  g.bg = reinterpret_cast<const float4*>(background);
+  g.target = reinterpret_cast<const float4*>(target);
+  g.inv_n = (float)(1.0 / (3.0 * (double)vw * (double)vh));
+  g.layer = layer;
+  g.dlf_dshape = di * 0.5f;
+  g.dld_ddetail = (ld_raw > 0.0f && ld_raw < 1.0f) ? di : 0.0f;
+  rc = psc::launch_march_param_grad(u, vd, g, c->opts.storage, grad, loss, static_cast<cudaStream_t>(stream));
+  if (rc) return fail(rc, "parameter-gradient launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   ++c->launches;
   return PSC_OK;
 }

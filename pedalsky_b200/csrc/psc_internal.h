@@ -59,6 +59,10 @@ struct LayerConst {
   // widened; live_lo > live_hi when no height can.  The FAST march turns it
   // into the range of step indices it runs.
   float live_lo, live_hi;
+  // Normalised height above which a light-march tap's density is exactly 0
+  // (its profile value is at or below skip_k), widened; above 1 when no such
+  // height lies in the layer.  Used by the lean FAST form's light march.
+  float light_h_dead;
   double r_bottom, r_top;  // planet_radius + base/top, FP64
 };
 
@@ -172,6 +176,21 @@ int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g
 // (grid_layer_grad.cu); g.bg / g.target / g.inv_n as for the adjoint.
 int launch_grid_layer_grad(const MarchUniforms& u, const ViewDev& v, const GridDev& g, double* out,
                            cudaStream_t stream);
+
+// Tangent inputs of the procedural march's layer-parameter gradient
+// (march_param_grad.cu).
+struct ParamGradDev {
+  const float4* bg;        // background per pixel of the view
+  const float4* target;    // target image per pixel of the view
+  float inv_n;             // 1 / (3 * viewport pixels)
+  uint32_t layer;          // the differentiated layer
+  float dlf_dshape;        // d lf_bias / d shape_bias = diurnal / 2
+  float dld_ddetail;       // d layer_detail / d detail_bias (diurnal inside the clamp, else 0)
+};
+// out[0..3] += d loss / d (coverage, shape_bias, detail_bias, density_scale)
+// of layer g.layer; *loss += the loss when loss is not null.
+int launch_march_param_grad(const MarchUniforms& u, const ViewDev& v, const ParamGradDev& g, uint32_t storage,
+                            double* out, double* loss, cudaStream_t stream);
 
 // TAA resolve of one cloud RT (post.cu, shaders/clouds/cloud_taa.wgsl).
 struct TaaParams {

@@ -63,7 +63,9 @@ def test_fetch_counts_match_the_timed_kernel_and_the_oracle(oracle, oracle_noise
     assert c["weather_taps"] == 0 and c["type_loads"] == 0
     assert oc["dense"] <= c["live_steps"] + 1e-3 * oc["dense"] and c["live_steps"] < oc["base"]
     assert c["detail_taps"] <= c["live_steps"]
-    assert c["light_taps"] == 6 * c["dense_samples"]
+    # a warp's light march stops after 2 or 4 taps once every later tap of
+    # every lane lies above the layer's last height of non-zero density
+    assert 2 * c["dense_samples"] <= c["light_taps"] <= 6 * c["dense_samples"]
     assert c["skyview_taps"] == c["dense_samples"]
     assert c["transmittance_taps"] <= c["dense_samples"]
     assert abs(c["ap_taps"] - oc["ap"]) <= 1e-3 * max(oc["ap"], 1) + 2

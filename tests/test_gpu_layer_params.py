@@ -1,0 +1,129 @@
+"""GPU tests of the procedural march's layer-parameter gradient
+(`psc_layer_param_gradient`): d loss / d coverage, shape_bias, detail_bias
+and density_scale of one layer of the three-layer precision scene (Cu
+1500-2300 m, As 4000-5000 m, Ci 8000-9000 m; 128 primary + 6 light steps)
+at 160x90, PLAIN schedule, FP32 storage, exact filtering.
+
+The reference is the FP64 oracle (oracle/oracle_march.cpp): its loss
+(sum((L + background T - target)^2) / (3 pixels)) differentiated by
+Richardson-extrapolated central differences (steps e and e/2, with the
+float32-rounded parameter values), against which the forward-mode FP32
+tangent agrees to ~1e-3.  The target is the oracle's render of the same
+scene with layer 0's four parameters moved (coverage +0.04, shape_bias
++0.15, detail_bias -0.10, density_scale x1.15), so every parameter has a
+non-zero derivative.  The shape and detail biases act through the diurnal
+modulation, which is 0 for the non-convective altostratus layer."""
+import ctypes as C
+import dataclasses
+
+import numpy as np
+import pytest
+
+from pedalsky_b200 import capi, scenes
+from pedalsky_b200.capi import PscError
+from pedalsky_b200.layer_grad import PARAMS, layer_param_gradient
+from pedalsky_b200.subsystem import subsystem_for_scene
+
+from . import _gpu
+
+pytestmark = pytest.mark.gpu
+
+W, H = 160, 90
+FIELDS = ("coverage", "shape_bias", "detail_bias", "density_scale")
+
+
+def _moved(sc, layer, deltas):
+    layers = (capi.CloudLayerGpu * 8).from_buffer_copy(sc.layers)
+    for name, d in deltas.items():
+        setattr(layers[layer], name, float(np.float32(getattr(sc.layers[layer], name) + d)))
+    return dataclasses.replace(sc, layers=layers)
+
+
+@pytest.fixture(scope="module")
+def prob(oracle, oracle_noise):
+    torch = _gpu.torch_cuda()
+    sc = scenes.precision_1080p(W, H, storage=capi.STORAGE_F32, schedule=capi.SCHED_PLAIN,
+                                filt=capi.FILTER_EXACT)
+    luts = oracle.bake_luts(sc.frame, sc.world)
+    moved = _moved(sc, 0, dict(coverage=0.04, shape_bias=0.15, detail_bias=-0.10,
+                               density_scale=0.15 * sc.layers[0].density_scale))
+    Lt, Tt = oracle.render(moved, oracle_noise, luts, threads=8)
+    tgt = (Lt + sc.background * Tt).astype(np.float32)
+    sub = subsystem_for_scene(sc, luts=luts, noise=oracle_noise)
+    dev = torch.device("cuda", 0)
+    bg = torch.from_numpy(np.ascontiguousarray(sc.background, np.float32)).to(dev)
+    tg = torch.from_numpy(tgt).to(dev)
+    depth = torch.from_numpy(np.ascontiguousarray(sc.depth, np.float32)).to(dev)
+    yield dict(sc=sc, luts=luts, tgt=tgt, sub=sub, bg=bg, tg=tg, depth=depth, torch=torch)
+    sub.close()
+
+
+def _gpu_grad(p, layer, rows=None):
+    torch = p["torch"]
+    g = torch.zeros(4, dtype=torch.float64, device="cuda:0")
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda:0")
+    for r0, r1 in rows or [(0, H)]:
+        view = capi.View(W, r1 - r0, p["depth"][r0:].data_ptr(), None, None, None, W, H, 0, r0)
+        layer_param_gradient(p["sub"].handle, view, layer, p["bg"][r0:], p["tg"][r0:], g, loss)
+    torch.cuda.synchronize()
+    return g.cpu().numpy(), float(loss.cpu().numpy()[0])
+
+
+def _oracle_loss(oracle, noise, p, sc):
+    L, T = oracle.render(sc, noise, p["luts"], threads=8)
+    I = L.astype(np.float64)[..., :3] + p["sc"].background[..., :3].astype(np.float64) * T[..., :3]
+    return float(np.sum((I - p["tgt"][..., :3].astype(np.float64)) ** 2) / (3.0 * W * H))
+
+
+def _richardson(oracle, noise, p, layer, name, e):
+    x = float(getattr(p["sc"].layers[layer], name))
+
+    def cd(h):
+        lo, hi = np.float32(x - h), np.float32(x + h)
+        f_hi = _oracle_loss(oracle, noise, p, _moved(p["sc"], layer, {name: float(hi) - x}))
+        f_lo = _oracle_loss(oracle, noise, p, _moved(p["sc"], layer, {name: float(lo) - x}))
+        return (f_hi - f_lo) / (float(hi) - float(lo))
+
+    return (4.0 * cd(e / 2) - cd(e)) / 3.0
+
+
+def test_layer_parameter_gradient_matches_fp64_central_differences(oracle, oracle_noise, prob):
+    g, loss = _gpu_grad(prob, 0)
+    ref_loss = _oracle_loss(oracle, oracle_noise, prob, prob["sc"])
+    steps = dict(coverage=2e-3, shape_bias=2e-2, detail_bias=2e-2,
+                 density_scale=2e-3 * prob["sc"].layers[0].density_scale)
+    fd = np.array([_richardson(oracle, oracle_noise, prob, 0, n, steps[n]) for n in FIELDS])
+    rel = np.abs(g - fd) / np.abs(fd)
+    print(f"\nlayer 0 d loss / d {PARAMS}:\n  GPU {g}\n  FD  {fd}\n  rel {rel}\n"
+          f"  loss GPU {loss:.9e} oracle {ref_loss:.9e}")
+    assert PARAMS == FIELDS
+    assert np.all(np.abs(fd) > 0)
+    assert np.all(rel <= 2e-2), (g, fd)
+    assert abs(loss - ref_loss) <= 1e-3 * ref_loss
+
+
+def test_biases_have_no_effect_on_a_non_convective_layer(oracle, oracle_noise, prob):
+    g, _ = _gpu_grad(prob, 1)
+    print(f"\nlayer 1 (altostratus) gradient {g}")
+    assert g[1] == 0.0 and g[2] == 0.0
+    assert g[0] != 0.0 and g[3] != 0.0
+    fd = _richardson(oracle, oracle_noise, prob, 1, "coverage", 2e-3)
+    assert abs(g[0] - fd) <= 2e-2 * abs(fd), (g[0], fd)
+
+
+def test_row_bands_add_up_to_the_whole_view(prob):
+    g, loss = _gpu_grad(prob, 0)
+    gb, lb = _gpu_grad(prob, 0, rows=[(0, 37), (37, 64), (64, H)])
+    assert np.allclose(gb, g, rtol=1e-5, atol=0)
+    assert abs(lb - loss) <= 1e-5 * loss
+
+
+def test_argument_errors(prob):
+    torch = prob["torch"]
+    g = torch.zeros(4, dtype=torch.float64, device="cuda:0")
+    view = capi.View(W, H, prob["depth"].data_ptr(), None, None, None, 0, 0, 0, 0)
+    with pytest.raises(PscError):
+        layer_param_gradient(prob["sub"].handle, view, 3, prob["bg"], prob["tg"], g)
+    with pytest.raises(PscError):
+        capi.call("psc_layer_param_gradient", prob["sub"].handle, C.byref(view), 0, None,
+                  C.c_void_p(prob["tg"].data_ptr()), C.c_void_p(g.data_ptr()), None, None)
