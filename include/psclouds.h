@@ -560,6 +560,24 @@ int psc_render_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, void* 
 int psc_autotune_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, uint32_t reps,
                        PscBatchTuning* best, float* best_ms, void* stream);
 
+/* Lower each view's march step counts as far as its image allows: renders
+ * the batch at the views' own counts (params.cloud_steps / light_steps) as
+ * the reference, then, per view, the light-march length one step at a time
+ * (down to half) and then the primary step count (7/8, 3/4, 5/8, 1/2 of
+ * it, at least 8), keeping each reduction while at most `max_share` of the
+ * view's pixels differ from its reference by more than `max_rel_err`
+ * (relative, max over RGB, of the composited image L + B T with B the
+ * view's hdr contents at the call, or 1 without hdr); the first reduction
+ * that fails ends that view's search.  Writes the chosen counts into
+ * views[i].params and the median of `reps` timed runs of the batch before
+ * and after into *ms_before / *ms_after (nullable).  Renders into its own
+ * scratch outputs with compositing off, so the views' buffers are not
+ * written.  1e-3 / 1e-3 is the parity bar of this library's tests (p99.9
+ * within 1e-3).  Synchronous. */
+int psc_autotune_steps(psc_ctx* ctx, PscBatchView* views, uint32_t n, float max_rel_err,
+                       float max_share, uint32_t reps, float* ms_before, float* ms_after,
+                       void* stream);
+
 /* ------------------------------------------ voxel-grid density, adjoint */
 
 /* A voxel density source for the differentiable form of the march.  New in

@@ -77,3 +77,17 @@ def autotune(handle, batch: Batch, reps=3, stream=None):
             "form_id": best.form, "threads": best.threads, "tile_w": best.tile_w,
             "tile_h": best.threads // 32 // (best.tile_w // 8) * 4,
             "light_batch": opts.light_batch, "ms": ms.value}
+
+
+def autotune_steps(handle, batch: Batch, max_rel_err=1e-3, max_share=1e-3, reps=3, stream=None):
+    """Lower each view's primary and light-march step counts while its image
+    stays within `max_rel_err` (relative, composited over the view's hdr
+    background) on all but `max_share` of its pixels (psc_autotune_steps).
+    The chosen counts are written into the batch's view array; returns them
+    with the batch's median time before and after."""
+    before, after = C.c_float(), C.c_float()
+    call("psc_autotune_steps", handle, batch.arr, len(batch.views), float(max_rel_err), float(max_share),
+         int(reps), C.byref(before), C.byref(after),
+         C.c_void_p(stream.cuda_stream if stream is not None else None))
+    steps = [(batch.arr[i].params.cloud_steps, batch.arr[i].params.light_steps) for i in range(len(batch.views))]
+    return {"steps": steps, "ms_before": before.value, "ms_after": after.value}

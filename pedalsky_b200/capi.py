@@ -217,6 +217,8 @@ _PROTOS = {
     "psc_render_batch": [_vp, P(BatchView), u32, _vp],
     "psc_render_batch_noalloc": [_vp, P(BatchView), u32, _vp, _vp, _vp],
     "psc_autotune_batch": [_vp, P(BatchView), u32, u32, P(BatchTuning), P(C.c_float), _vp],
+    "psc_autotune_steps": [_vp, P(BatchView), u32, C.c_float, C.c_float, u32, P(C.c_float), P(C.c_float),
+                           _vp],
     "psc_render_grid": [_vp, P(DensityGrid), P(View), _vp],
     "psc_adjoint": [_vp, P(DensityGrid), P(View), _vp, _vp, _vp, _vp, _vp, _vp],
     "psc_layer_gradient": [_vp, P(DensityGrid), P(View), _vp, _vp, _vp, _vp],

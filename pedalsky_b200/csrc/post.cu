@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "psc_internal.h"
 
 namespace psc {
@@ -177,6 +179,30 @@ __global__ void k_composite_halfres(const float4* __restrict__ l, const float4* 
 
 dim3 grid16(uint32_t w, uint32_t h) { return dim3((w + 15u) / 16u, (h + 15u) / 16u); }
 
+// Pixels whose composited image I = L + B T (B = bg, or 1 without one)
+// differs from the reference's by more than `thr` relative, max over RGB;
+// one atomic add per warp.
+__global__ void k_count_rel_err(const float4* __restrict__ lr, const float4* __restrict__ tr,
+                                const float4* __restrict__ l, const float4* __restrict__ t,
+                                const float4* __restrict__ bg, uint32_t n, float thr,
+                                unsigned int* __restrict__ count) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t over = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float4 b = bg ? __ldg(bg + i) : f4(1.0f);
+    const float4 a = __ldg(lr + i), at = __ldg(tr + i), c = __ldg(l + i), ct = __ldg(t + i);
+    const float r0 = fmaf(b.x, at.x, a.x), r1 = fmaf(b.y, at.y, a.y), r2 = fmaf(b.z, at.z, a.z);
+    const float d0 = fabsf(fmaf(b.x, ct.x, c.x) - r0), d1 = fabsf(fmaf(b.y, ct.y, c.y) - r1),
+                d2 = fabsf(fmaf(b.z, ct.z, c.z) - r2);
+    const bool bad = d0 > thr * fabsf(r0) || d1 > thr * fabsf(r1) || d2 > thr * fabsf(r2) ||
+                     !(d0 == d0 && d1 == d1 && d2 == d2);
+    over += bad ? 1u : 0u;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) over += __shfl_xor_sync(0xffffffffu, over, o);
+  if ((threadIdx.x & 31u) == 0 && over) atomicAdd(count, over);
+}
+
 }  // namespace
 
 int launch_depth_halfres(const float* depth, uint32_t W, uint32_t H, float* out, uint32_t rw,
@@ -193,6 +219,14 @@ int launch_taa_resolve(const TaaParams& p, cudaStream_t s) {
 int launch_composite_halfres(const float4* l, const float4* t, uint32_t rw, uint32_t rh, float4* hdr,
                              uint32_t W, uint32_t H, cudaStream_t s) {
   k_composite_halfres<<<grid16(W, H), dim3(16, 16), 0, s>>>(l, t, rw, rh, hdr, W, H);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
+
+int launch_count_rel_err(const float4* lr, const float4* tr, const float4* l, const float4* t, const float4* bg,
+                         uint32_t n, float thr, unsigned int* count, cudaStream_t s) {
+  if (n == 0) return PSC_OK;
+  const uint32_t blocks = std::min((n + 255u) / 256u, 148u * 8u);
+  k_count_rel_err<<<blocks, 256, 0, s>>>(lr, tr, l, t, bg, n, thr, count);
   return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
 }
 

@@ -2118,6 +2118,169 @@ int psc_autotune_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, uint32
   return PSC_OK;
 }
 
+int psc_autotune_steps(psc_ctx* c, PscBatchView* views, uint32_t n, float max_rel_err, float max_share,
+                       uint32_t reps, float* ms_before, float* ms_after, void* stream) {
+  if (!c || !views || !n) return fail(PSC_ERR_INVALID_ARGUMENT, "null or empty batch");
+  if (n > PSC_MAX_BATCH_VIEWS) return fail(PSC_ERR_INVALID_ARGUMENT, "%u views exceeds %u", n, PSC_MAX_BATCH_VIEWS);
+  if (!(max_rel_err > 0.0f) || !std::isfinite(max_rel_err))
+    return fail(PSC_ERR_INVALID_ARGUMENT, "max_rel_err must be positive and finite");
+  if (!(max_share >= 0.0f && max_share < 1.0f)) return fail(PSC_ERR_INVALID_ARGUMENT, "max_share must be in [0, 1)");
+  if (reps == 0 || reps > 100) return fail(PSC_ERR_INVALID_ARGUMENT, "reps must be 1..100");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // scratch: reference L / T and candidate L / T per view, one count per view
+  std::vector<size_t> off(n + 1, 0);
+  for (uint32_t i = 0; i < n; ++i) off[i + 1] = off[i] + (size_t)views[i].width * views[i].height;
+  const size_t px = off[n];
+  float4* buf = nullptr;
+  unsigned int* d_count = nullptr;
+  PSC_CUDA(cudaMalloc(&buf, 4 * px * sizeof(float4)), "cudaMalloc step-tuner scratch");
+  if (cudaMalloc(&d_count, n * sizeof(unsigned int)) != cudaSuccess) {
+    cudaFree(buf);
+    return cuda_fail(cudaGetLastError(), "cudaMalloc step-tuner counts");
+  }
+  float4 *Lr = buf, *Tr = buf + px, *Lc = buf + 2 * px, *Tc = buf + 3 * px;
+  const uint32_t saved_composite = c->opts.composite;
+  c->opts.composite = 0;
+  auto with_outputs = [&](uint32_t i, float4* L, float4* T) {
+    PscBatchView v = views[i];
+    v.out_luminance = reinterpret_cast<float*>(L + off[i]);
+    v.out_transmittance = reinterpret_cast<float*>(T + off[i]);
+    v.hdr = nullptr;
+    return v;
+  };
+  std::vector<PscBatchView> ref(n), cand;
+  for (uint32_t i = 0; i < n; ++i) ref[i] = with_outputs(i, Lr, Tr);
+  std::vector<uint32_t> cloud(n), light(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    cloud[i] = views[i].params.cloud_steps;
+    light[i] = views[i].params.light_steps;
+  }
+  // renders the views `ids` at counts (cl, ll) and reports which stay within
+  // the bar against the reference
+  auto trial = [&](const std::vector<uint32_t>& ids, const std::vector<uint32_t>& cl,
+                   const std::vector<uint32_t>& ll, std::vector<char>& ok) -> int {
+    cand.clear();
+    for (uint32_t k = 0; k < ids.size(); ++k) {
+      PscBatchView v = with_outputs(ids[k], Lc, Tc);
+      v.params.cloud_steps = cl[k];
+      v.params.light_steps = ll[k];
+      cand.push_back(v);
+    }
+    int rc = psc_render_batch(c, cand.data(), (uint32_t)cand.size(), stream);
+    if (rc) return rc;
+    if (cudaMemsetAsync(d_count, 0, n * sizeof(unsigned int), s) != cudaSuccess)
+      return cuda_fail(cudaGetLastError(), "step-tuner count reset");
+    for (uint32_t k = 0; k < ids.size(); ++k) {
+      const uint32_t i = ids[k];
+      rc = psc::launch_count_rel_err(Lr + off[i], Tr + off[i], Lc + off[i], Tc + off[i],
+                                     reinterpret_cast<const float4*>(views[i].hdr), (uint32_t)(off[i + 1] - off[i]),
+                                     max_rel_err, d_count + k, s);
+      if (rc) return fail(rc, "step-tuner error count launch failed");
+    }
+    std::vector<unsigned int> h(ids.size());
+    if (cudaMemcpyAsync(h.data(), d_count, ids.size() * sizeof(unsigned int), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return cuda_fail(cudaGetLastError(), "step-tuner count read");
+    ok.assign(ids.size(), 0);
+    for (uint32_t k = 0; k < ids.size(); ++k) {
+      const double allowed = (double)max_share * (double)(off[ids[k] + 1] - off[ids[k]]);
+      ok[k] = (double)h[k] <= allowed;
+    }
+    return PSC_OK;
+  };
+  int rc = psc_render_batch(c, ref.data(), n, stream);
+  // light-march length: one step at a time, down to half of the view's own
+  std::vector<char> open(n, 1);
+  for (uint32_t j = 1; !rc; ++j) {
+    std::vector<uint32_t> ids, cl, ll;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t l0 = views[i].params.light_steps;
+      if (open[i] && l0 > j && 2 * (l0 - j) >= l0) {
+        ids.push_back(i);
+        cl.push_back(cloud[i]);
+        ll.push_back(l0 - j);
+      } else {
+        open[i] = 0;
+      }
+    }
+    if (ids.empty()) break;
+    std::vector<char> ok;
+    rc = trial(ids, cl, ll, ok);
+    for (uint32_t k = 0; !rc && k < ids.size(); ++k) {
+      if (ok[k]) light[ids[k]] = ll[k];
+      else open[ids[k]] = 0;
+    }
+  }
+  // primary step count: 7/8, 3/4, 5/8, 1/2 of the view's own (at least 8)
+  open.assign(n, 1);
+  for (uint32_t eighths = 7; !rc && eighths >= 4; --eighths) {
+    std::vector<uint32_t> ids, cl, ll;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t c0 = views[i].params.cloud_steps;
+      const uint32_t cn = std::max(8u, (c0 * eighths + 7u) / 8u);
+      if (open[i] && cn < cloud[i]) {
+        ids.push_back(i);
+        cl.push_back(cn);
+        ll.push_back(light[i]);
+      }
+    }
+    if (ids.empty()) continue;
+    std::vector<char> ok;
+    rc = trial(ids, cl, ll, ok);
+    for (uint32_t k = 0; !rc && k < ids.size(); ++k) {
+      if (ok[k]) cloud[ids[k]] = cl[k];
+      else open[ids[k]] = 0;
+    }
+  }
+  // median batch time before and after
+  auto time_batch = [&](const std::vector<PscBatchView>& vs, float* med) -> int {
+    if (!med) return PSC_OK;
+    int r = psc_render_batch(c, vs.data(), n, stream);
+    if (r) return r;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+      if (a) cudaEventDestroy(a);
+      return cuda_fail(cudaGetLastError(), "event");
+    }
+    std::vector<float> ts;
+    for (uint32_t k = 0; k < reps && !r; ++k) {
+      cudaEventRecord(a, s);
+      r = psc_render_batch(c, vs.data(), n, stream);
+      cudaEventRecord(b, s);
+      if (!r && cudaEventSynchronize(b) != cudaSuccess) r = cuda_fail(cudaGetLastError(), "step-tuner sync");
+      float ms = 0.0f;
+      if (!r) cudaEventElapsedTime(&ms, a, b);
+      ts.push_back(ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (r) return r;
+    std::sort(ts.begin(), ts.end());
+    *med = ts[ts.size() / 2];
+    return PSC_OK;
+  };
+  if (!rc) rc = time_batch(ref, ms_before);
+  if (!rc) {
+    std::vector<PscBatchView> tuned(ref);
+    for (uint32_t i = 0; i < n; ++i) {
+      tuned[i].params.cloud_steps = cloud[i];
+      tuned[i].params.light_steps = light[i];
+    }
+    rc = time_batch(tuned, ms_after);
+  }
+  cudaStreamSynchronize(s);
+  cudaFree(buf);
+  cudaFree(d_count);
+  c->opts.composite = saved_composite;
+  if (rc) return rc;
+  for (uint32_t i = 0; i < n; ++i) {
+    views[i].params.cloud_steps = cloud[i];
+    views[i].params.light_steps = light[i];
+  }
+  return PSC_OK;
+}
+
 }  // extern "C"
 
 namespace {

@@ -177,6 +177,12 @@ int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g
 int launch_grid_layer_grad(const MarchUniforms& u, const ViewDev& v, const GridDev& g, double* out,
                            cudaStream_t stream);
 
+// Adds to *count the pixels (of n) whose composited image L + bg T (bg = 1
+// when null) differs from the reference's by more than thr relative, max
+// over RGB (post.cu; the step autotuner's image-error test).
+int launch_count_rel_err(const float4* lr, const float4* tr, const float4* l, const float4* t, const float4* bg,
+                         uint32_t n, float thr, unsigned int* count, cudaStream_t stream);
+
 // Tangent inputs of the procedural march's layer-parameter gradient
 // (march_param_grad.cu).
 struct ParamGradDev {
