@@ -137,6 +137,15 @@ int oracle_branch_margins(const OracleScene* scene, uint32_t width, uint32_t hei
                           int threads, uint32_t row0, uint32_t row1, double* out_t,
                           double* out_d);
 
+/* The FP64 march of `scene` with the outcomes of its discontinuous tests
+ * (early exits, the 1e-3 density threshold, the aerial-perspective opacity
+ * test) replayed from the FP64 march of `ref` at each pixel: the image as a
+ * smooth function of whatever parameters differ between the two scenes.
+ * Returns the number of outcomes a replay needed beyond its record (0 when
+ * the two march the same path; -1 on bad arguments). */
+long long oracle_render_frozen(const OracleScene* ref, const OracleScene* scene, uint32_t width,
+                               uint32_t height, int threads, float* lum, float* tr);
+
 /* One FP64 primary density sample at world point p3 / altitude alt in layer
  * li with weather R value weather_r, and the layer profile ndf(h) there
  * (test support for the density bound of the GPU march's step skip). */

@@ -143,6 +143,53 @@ int oracle_branch_margins(const OracleScene* s, uint32_t w, uint32_t h, int thre
   return 0;
 }
 
+// Test support: the FP64 march of `s` with the discontinuous tests' outcomes
+// (early exits, the 1e-3 density threshold, the AP opacity test) taken from
+// the FP64 march of `ref` at the same pixel (March::branch), so that the
+// image is a smooth function of the parameters that differ between the two
+// scenes: its central differences converge to the derivative with the
+// branches held, which is what a tangent or adjoint of the march computes.
+// Returns the number of outcomes a replay needed beyond its record (0 when
+// both scenes march the same path), or -1 on bad arguments.
+long long oracle_render_frozen(const OracleScene* ref, const OracleScene* s, uint32_t w, uint32_t h,
+                               int threads, float* lum, float* tr) {
+  if (!scene_ok(ref) || !scene_ok(s) || !w || !h || !lum || !tr) return -1;
+  March<double> base_ref, base;
+  base_ref.init(ref, false);
+  base.init(s, false);
+  uint64_t misses = 0;
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel
+  {
+    March<double> mr = base_ref, m = base;
+    std::vector<uint8_t> tape;
+    mr.tape = &tape;
+    mr.tape_mode = 1;
+    m.tape = &tape;
+    m.tape_mode = 2;
+#pragma omp for schedule(dynamic, 1)
+    for (int y = 0; y < (int)h; ++y) {
+      for (uint32_t x = 0; x < w; ++x) {
+        double l4[4], t4[4];
+        tape.clear();
+        mr.pixel(x, (uint32_t)y, ref->depth, w, l4, t4);
+        m.tape_pos = 0;
+        m.pixel(x, (uint32_t)y, s->depth, w, l4, t4);
+        const size_t o = ((size_t)y * w + x) * 4;
+        for (int c = 0; c < 4; ++c) {
+          lum[o + c] = (float)l4[c];
+          tr[o + c] = (float)t4[c];
+        }
+      }
+    }
+#pragma omp critical
+    misses += m.tape_misses;
+  }
+  return (long long)misses;
+}
+
 // Test support: one primary density sample (sample_density,
 // cloud_march.wgsl:432-530) in FP64 at world point p3 and altitude `alt`, in
 // layer `li`, with weather R channel `weather_r`; also the layer's profile

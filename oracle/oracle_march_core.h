@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 #include "oracle.h"
 #include "oracle_common.h"
@@ -670,6 +671,27 @@ struct March {
     if (margin) margin[1] = std::fmin(margin[1], std::fabs((double)d - 1e-3) / 1e-3);
   }
 
+  // Branch tape (oracle_render_frozen): the outcomes of the march's tests
+  // whose result jumps the image (the early exits, the 1e-3 density
+  // threshold, the aerial-perspective opacity test), in the order they run.
+  // tape_mode 1 appends each outcome to `tape`; 2 takes each outcome from
+  // it instead of the comparison, so a march with other parameters follows
+  // the recorded path (a replay that runs past the tape counts a miss and
+  // uses the comparison).
+  std::vector<uint8_t>* tape = nullptr;
+  int tape_mode = 0;
+  mutable size_t tape_pos = 0;
+  mutable uint64_t tape_misses = 0;
+  bool branch(bool outcome) const {
+    if (tape_mode == 1) {
+      tape->push_back(outcome ? 1 : 0);
+    } else if (tape_mode == 2) {
+      if (tape_pos < tape->size()) return (*tape)[tape_pos++] != 0;
+      ++tape_misses;
+    }
+    return outcome;
+  }
+
   void pixel(uint32_t px, uint32_t py, const float* depth, uint32_t width, R lum_out[4],
              R tr_out[4]) const {
     count(ORACLE_CNT_PIXELS);
@@ -709,7 +731,7 @@ struct March {
 
     for (uint32_t i = 0; i < layer_count; ++i) {
       note_exit(max3(trans));
-      if (max3(trans) < R(0.01)) break;
+      if (branch(max3(trans) < R(0.01))) break;
       const Hit lh = hits[i];
       if (!lh.hit) continue;
       const Layer<R>& L = layers[lh.idx];
@@ -733,7 +755,7 @@ struct March {
         const uint32_t type = effective_type(wsx, wsz, L);
         const R density = sample_density(p, alt, L, wr, w, type);
         note_density(density);
-        if (density > R(1e-3)) {
+        if (branch(density > R(1e-3))) {
           count(ORACLE_CNT_DENSE);
           const R od = march_to_light(p, alt, L, wr, w, type);
           const V3<R> beer = vexp(mk<R>(-sigma_t.x * od, -sigma_t.y * od, -sigma_t.z * od));
@@ -779,7 +801,7 @@ struct March {
           trans = trans * samp;
         }
         note_exit(max3(trans));
-        if (max3(trans) < R(0.01)) break;
+        if (branch(max3(trans) < R(0.01))) break;
         t = t + step;
       }
     }
@@ -789,7 +811,7 @@ struct March {
     const R opacity = R(1) - t_lum;
     const R t_cloud = tw / std::fmax(twn, R(1e-6));
     V3<R> lo = lum;
-    if (opacity > R(1e-4)) {
+    if (branch(opacity > R(1e-4))) {
       const R ds = std::fmax(t_cloud, R(50));
       const R az = clampv<R>(std::log(ds / R(50)) / std::log(R(100000) / R(50)), R(0), R(1));
       R ap[4];

@@ -77,6 +77,7 @@ def lib() -> C.CDLL:
             ("oracle_render", [vp, u32, u32, C.c_int, C.c_int, C.c_int, u32, u32, vp, vp, vp], C.c_int),
             ("oracle_render_pixel", [vp, u32, u32, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
             ("oracle_branch_margins", [vp, u32, u32, C.c_int, u32, u32, vp, vp], C.c_int),
+            ("oracle_render_frozen", [vp, vp, u32, u32, C.c_int, vp, vp], C.c_longlong),
             ("oracle_composite", [vp, vp, vp, u32], C.c_int),
             ("oracle_density_sample", [vp, u32, vp, C.c_double, C.c_double, vp, vp], C.c_int),
             ("oracle_grid_render", [vp, vp, u32, u32, C.c_int, C.c_int, vp, vp], C.c_int),
@@ -232,6 +233,22 @@ def branch_margins(scene, noise, luts, threads=0, rows=None):
         "oracle_branch_margins")
     del keep
     return mt, md
+
+
+def render_frozen(ref_scene, scene, noise, luts, threads=0):
+    """FP64 (L, T) of `scene` with the branch outcomes (early exits, density
+    threshold, AP opacity test) of `ref_scene`'s march at each pixel, and the
+    number of outcomes the replay lacked (0 when both follow one path)."""
+    r, keep_r = make_scene(ref_scene, noise, luts)
+    s, keep = make_scene(scene, noise, luts)
+    w, h = scene.width, scene.height
+    L = np.zeros((h, w, 4), np.float32)
+    T = np.zeros((h, w, 4), np.float32)
+    misses = lib().oracle_render_frozen(C.byref(r), C.byref(s), w, h, threads, _p(L), _p(T))
+    if misses < 0:
+        raise RuntimeError("oracle_render_frozen failed")
+    del keep, keep_r
+    return L, T, int(misses)
 
 
 def density_sample(scene, noise, luts, layer, p3, alt, weather_r):

@@ -220,38 +220,61 @@ double profile_h(const PscCloudLayerGpu& L, const psc::LayerConst& o, double h) 
 // density_scale > 1e-3, found on a 1/20000 grid with the threshold lowered by
 // 1e-4 and widened by 1e-3 of the height and then 1 m of altitude, so that
 // the kernel's FP32 evaluation of any passing step lies inside it.
+// LayerConst::light_h_dead: above the last height where the profile can
+// exceed skip_k (threshold lowered by 1e-4, widened by 2 grid cells and
+// 1e-3) every light-march tap adds exactly 0: the base shape is at most 1
+// and 1 - eff is at least skip_k.
+// The scan is a pure function of the profile's inputs; the last results are
+// kept per thread, so a frame stream whose layers do not change pays for it
+// once instead of on every call.
 void live_band(const PscCloudLayerGpu& L, psc::LayerConst& o) {
+  struct Key {
+    uint32_t mode, type;
+    float inv_a, b1, inv_w1, anvil, skip_k, density_scale, inv_thickness, base_m;
+    bool operator==(const Key& k) const { return std::memcmp(this, &k, sizeof(Key)) == 0; }
+  };
+  struct Entry {
+    Key key;
+    float live_lo, live_hi, light_h_dead;
+  };
+  Key key;
+  std::memset(&key, 0, sizeof(key));
+  key = Key{o.ndf_mode, L.cloud_type, o.ndf_inv_a, o.ndf_b1, o.ndf_inv_w1, L.anvil_bias,
+            o.skip_k, o.density_scale, o.inv_thickness, o.base_m};
+  thread_local Entry cache[32];
+  thread_local uint32_t cache_n = 0, cache_next = 0;
+  for (uint32_t i = 0; i < cache_n; ++i)
+    if (cache[i].key == key) {
+      o.live_lo = cache[i].live_lo;
+      o.live_hi = cache[i].live_hi;
+      o.light_h_dead = cache[i].light_h_dead;
+      return;
+    }
   const int M = 20000;
-  int first = -1, last = -1;
+  int first = -1, last = -1, last_light = -1;
   for (int i = 0; i <= M; ++i) {
-    const double h = (double)i / M;
-    if ((profile_h(L, o, h) * 1.000001 - o.skip_k) * o.density_scale > 1e-3 * (1.0 - 1e-4)) {
+    const double nd = profile_h(L, o, (double)i / M);
+    if ((nd * 1.000001 - o.skip_k) * o.density_scale > 1e-3 * (1.0 - 1e-4)) {
       if (first < 0) first = i;
       last = i;
     }
+    if (nd * 1.000001 > (double)o.skip_k - 1e-4) last_light = i;
   }
   if (first < 0) {
     o.live_lo = 1.0f;
     o.live_hi = 0.0f;
     o.light_h_dead = 2.0f;  // no primary step is dense, so no light march runs
-    return;
-  }
-  const double thick = 1.0 / (double)o.inv_thickness;
-  // light-march taps: the density of a tap is exactly 0 once its profile
-  // value is at or below skip_k (the base shape is at most 1 and 1 - eff is
-  // at least skip_k); above the last height where it can exceed skip_k
-  // (threshold lowered by 1e-4, widened by 2 grid cells and 1e-3) every tap
-  // adds 0
-  {
-    int last_light = -1;
-    for (int i = 0; i <= M; ++i)
-      if (profile_h(L, o, (double)i / M) * 1.000001 > (double)o.skip_k - 1e-4) last_light = i;
+  } else {
+    const double thick = 1.0 / (double)o.inv_thickness;
     o.light_h_dead = last_light < 0 ? -1.0f : (float)((double)(last_light + 2) / M + 1e-3);
+    const double h_lo = std::fmax((double)(first - 2) / M - 1e-3, 0.0);
+    const double h_hi = std::fmin((double)(last + 2) / M + 1e-3, 1.0);
+    o.live_lo = (float)((double)o.base_m + h_lo * thick - 1.0);
+    o.live_hi = (float)((double)o.base_m + h_hi * thick + 1.0);
   }
-  const double h_lo = std::fmax((double)(first - 2) / M - 1e-3, 0.0);
-  const double h_hi = std::fmin((double)(last + 2) / M + 1e-3, 1.0);
-  o.live_lo = (float)((double)o.base_m + h_lo * thick - 1.0);
-  o.live_hi = (float)((double)o.base_m + h_hi * thick + 1.0);
+  cache[cache_next] = Entry{key, o.live_lo, o.live_hi, o.light_h_dead};
+  cache_next = (cache_next + 1) % 32u;
+  cache_n = std::min(cache_n + 1, 32u);
 }
 
 void build_uniforms_for(const psc_ctx* c, const PscCloudParamsGpu& p, const PscCloudLayerGpu* layers,

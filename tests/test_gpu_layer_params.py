@@ -7,12 +7,21 @@ at 160x90, PLAIN schedule, FP32 storage, exact filtering.
 The reference is the FP64 oracle (oracle/oracle_march.cpp): its loss
 (sum((L + background T - target)^2) / (3 pixels)) differentiated by
 Richardson-extrapolated central differences (steps e and e/2, with the
-float32-rounded parameter values), against which the forward-mode FP32
-tangent agrees to ~1e-3.  The target is the oracle's render of the same
-scene with layer 0's four parameters moved (coverage +0.04, shape_bias
-+0.15, detail_bias -0.10, density_scale x1.15), so every parameter has a
-non-zero derivative.  The shape and detail biases act through the diurnal
-modulation, which is 0 for the non-convective altostratus layer."""
+float32-rounded parameter values) of the march with its discontinuous tests
+held (`oracle_render_frozen`: the early exits, the 1e-3 density threshold
+and the AP opacity test replay the outcomes of the unperturbed march).  The
+tangent differentiates the march with those outcomes held too; the plain
+central differences of the march as it branches differ from both by the
+jumps of the samples that cross the 1e-3 threshold within the step (+3 %
+for layer 0's coverage, +30 % for layer 1's on this scene), a term that does
+not vanish as the step shrinks and that no pathwise derivative carries.
+
+The target is the oracle's render of the same scene with layer 0's four
+parameters moved (coverage +0.04, shape_bias +0.15, detail_bias -0.10,
+density_scale x1.15), so every parameter has a non-zero derivative; the
+diurnal modulation is on (strength 1, sun at 35 degrees), through which the
+shape and detail biases act on the convective cumulus layer; it is 0 for
+the non-convective altostratus layer."""
 import ctypes as C
 import dataclasses
 
@@ -44,6 +53,7 @@ def prob(oracle, oracle_noise):
     torch = _gpu.torch_cuda()
     sc = scenes.precision_1080p(W, H, storage=capi.STORAGE_F32, schedule=capi.SCHED_PLAIN,
                                 filt=capi.FILTER_EXACT)
+    sc.params.diurnal_strength = 1.0
     luts = oracle.bake_luts(sc.frame, sc.world)
     moved = _moved(sc, 0, dict(coverage=0.04, shape_bias=0.15, detail_bias=-0.10,
                                density_scale=0.15 * sc.layers[0].density_scale))
@@ -69,19 +79,23 @@ def _gpu_grad(p, layer, rows=None):
     return g.cpu().numpy(), float(loss.cpu().numpy()[0])
 
 
-def _oracle_loss(oracle, noise, p, sc):
-    L, T = oracle.render(sc, noise, p["luts"], threads=8)
+def _oracle_loss(oracle, noise, p, sc, frozen=True):
+    if frozen:
+        L, T, misses = oracle.render_frozen(p["sc"], sc, noise, p["luts"], threads=8)
+        assert misses == 0
+    else:
+        L, T = oracle.render(sc, noise, p["luts"], threads=8)
     I = L.astype(np.float64)[..., :3] + p["sc"].background[..., :3].astype(np.float64) * T[..., :3]
     return float(np.sum((I - p["tgt"][..., :3].astype(np.float64)) ** 2) / (3.0 * W * H))
 
 
-def _richardson(oracle, noise, p, layer, name, e):
+def _richardson(oracle, noise, p, layer, name, e, frozen=True):
     x = float(getattr(p["sc"].layers[layer], name))
 
     def cd(h):
         lo, hi = np.float32(x - h), np.float32(x + h)
-        f_hi = _oracle_loss(oracle, noise, p, _moved(p["sc"], layer, {name: float(hi) - x}))
-        f_lo = _oracle_loss(oracle, noise, p, _moved(p["sc"], layer, {name: float(lo) - x}))
+        f_hi = _oracle_loss(oracle, noise, p, _moved(p["sc"], layer, {name: float(hi) - x}), frozen)
+        f_lo = _oracle_loss(oracle, noise, p, _moved(p["sc"], layer, {name: float(lo) - x}), frozen)
         return (f_hi - f_lo) / (float(hi) - float(lo))
 
     return (4.0 * cd(e / 2) - cd(e)) / 3.0
@@ -90,15 +104,17 @@ def _richardson(oracle, noise, p, layer, name, e):
 def test_layer_parameter_gradient_matches_fp64_central_differences(oracle, oracle_noise, prob):
     g, loss = _gpu_grad(prob, 0)
     ref_loss = _oracle_loss(oracle, oracle_noise, prob, prob["sc"])
-    steps = dict(coverage=2e-3, shape_bias=2e-2, detail_bias=2e-2,
+    steps = dict(coverage=2e-3, shape_bias=2e-2, detail_bias=5e-3,
                  density_scale=2e-3 * prob["sc"].layers[0].density_scale)
     fd = np.array([_richardson(oracle, oracle_noise, prob, 0, n, steps[n]) for n in FIELDS])
+    fd_plain = _richardson(oracle, oracle_noise, prob, 0, "coverage", steps["coverage"], frozen=False)
     rel = np.abs(g - fd) / np.abs(fd)
     print(f"\nlayer 0 d loss / d {PARAMS}:\n  GPU {g}\n  FD  {fd}\n  rel {rel}\n"
-          f"  loss GPU {loss:.9e} oracle {ref_loss:.9e}")
+          f"  loss GPU {loss:.9e} oracle {ref_loss:.9e}\n"
+          f"  coverage by central differences of the branching march: {fd_plain:.6e}")
     assert PARAMS == FIELDS
     assert np.all(np.abs(fd) > 0)
-    assert np.all(rel <= 2e-2), (g, fd)
+    assert np.all(rel <= 5e-3), (g, fd)
     assert abs(loss - ref_loss) <= 1e-3 * ref_loss
 
 
@@ -108,7 +124,10 @@ def test_biases_have_no_effect_on_a_non_convective_layer(oracle, oracle_noise, p
     assert g[1] == 0.0 and g[2] == 0.0
     assert g[0] != 0.0 and g[3] != 0.0
     fd = _richardson(oracle, oracle_noise, prob, 1, "coverage", 2e-3)
-    assert abs(g[0] - fd) <= 2e-2 * abs(fd), (g[0], fd)
+    fd_ds = _richardson(oracle, oracle_noise, prob, 1, "density_scale", 2e-3 * prob["sc"].layers[1].density_scale)
+    print(f"  FD coverage {fd:.6e}, density_scale {fd_ds:.6e}")
+    assert abs(g[0] - fd) <= 5e-3 * abs(fd), (g[0], fd)
+    assert abs(g[3] - fd_ds) <= 5e-3 * abs(fd_ds), (g[3], fd_ds)
 
 
 def test_row_bands_add_up_to_the_whole_view(prob):
