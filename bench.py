@@ -925,6 +925,7 @@ def run_frames(args, ranks: Ranks):
                     "pipeline": "per frame: pinned H2D, march + composite, D2H on three "
                                 "streams, two device slots"},
             "gpu_launches": kernel_launches,
+            "library": {"path": capi.LIB_PATH.name, "build_id": capi.lib().psc_build_id().decode()},
             "kernel_ms": kernel_ms,
             "roofline": roof,
             "fetch_counts": counts,

@@ -278,6 +278,11 @@ enum {
 /* ------------------------------------------------------- diagnostics */
 const char* psc_last_error(void);
 uint32_t psc_abi_version(void);
+
+/* No counterpart in the reference: the SHA-256 (hex) of the sources and
+ * compile flags this library was built from (pedalsky_b200/build.py),
+ * so a caller can check that the binary it loaded matches its sources. */
+const char* psc_build_id(void);
 size_t psc_sizeof_params(void);     /* 112 */
 size_t psc_sizeof_layer(void);      /* 48  */
 size_t psc_sizeof_frame(void);      /* 448 */

@@ -4,11 +4,15 @@ Usage: python -m pedalsky_b200.build [--verbose]
 
 Each translation unit is compiled separately so per-file flags apply
 (noise_bake.cu needs -fmad=false for byte-exact bakes), then linked into one
-shared library next to this file.  Rebuilds only when a source or header is
-newer than the library.
+shared library next to this file.  The library carries the SHA-256 of the
+sources and flags it was built from (`psc_build_id`), also written beside
+it; a build is redone whenever that hash differs from the current sources'
+(or a source is newer than the library), so a library copied from elsewhere
+is never used for other sources.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import shutil
 import subprocess
@@ -19,6 +23,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 ROOT = HERE.parent
 LIB = HERE / "libpsclouds.so"
+LIB_ID = HERE / "libpsclouds.so.id"
 BUILD_DIR = HERE / "_build"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -58,8 +63,20 @@ def _sources() -> list[Path]:
     return sorted(CSRC.glob("*")) + [ROOT / "include" / "psclouds.h"]
 
 
+def source_hash() -> str:
+    """SHA-256 over the sources (path and bytes) and the compile flags."""
+    h = hashlib.sha256()
+    for p in _sources():
+        if p.is_file() and p.suffix in (".cu", ".cuh", ".cpp", ".h"):
+            h.update(str(p.relative_to(ROOT)).encode() + b"\0" + p.read_bytes() + b"\0")
+    h.update(repr((ARCH, NVCC_COMMON, sorted(CUDA_UNITS.items()), CXX_UNITS)).encode())
+    return h.hexdigest()
+
+
 def needs_build() -> bool:
-    if not LIB.exists():
+    if not LIB.exists() or not LIB_ID.exists():
+        return True
+    if LIB_ID.read_text().strip() != source_hash():
         return True
     t = LIB.stat().st_mtime
     return any(p.stat().st_mtime > t for p in _sources() if p.is_file())
@@ -80,6 +97,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     if not force and not needs_build():
         return LIB
     BUILD_DIR.mkdir(exist_ok=True)
+    build_id = source_hash()
     nvcc, cxx = _nvcc(), _host_cxx()
     env_ccbin = ["-ccbin", cxx]
     cmds, objs = [], []
@@ -94,7 +112,8 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     for unit in CXX_UNITS:
         obj = BUILD_DIR / (unit + ".o")
         cmds.append([cxx, "-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-I", str(ROOT / "include"),
-                     "-I", str(cuda_inc), "-c", str(CSRC / unit), "-o", str(obj)])
+                     "-I", str(cuda_inc), f'-DPSC_BUILD_ID="{build_id}"', "-c", str(CSRC / unit), "-o",
+                     str(obj)])
         objs.append(obj)
     from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
@@ -104,6 +123,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     cmd = [nvcc, *env_ccbin, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static"]
     _run(cmd, verbose)
     os.replace(tmp, LIB)
+    LIB_ID.write_text(build_id + "\n")
     return LIB
 
 

@@ -181,6 +181,7 @@ _vp = C.c_void_p
 _PROTOS = {
     "psc_last_error": [],
     "psc_abi_version": [],
+    "psc_build_id": [],
     "psc_sizeof_params": [], "psc_sizeof_layer": [], "psc_sizeof_frame": [], "psc_sizeof_world": [],
     "psc_params_default": [P(CloudParamsGpu)],
     "psc_world_default": [P(WorldUniformsGpu)],
@@ -231,7 +232,7 @@ _PROTOS = {
     "psc_composite_halfres": [_vp, _vp, u32, u32, _vp, u32, u32, _vp],
 }
 _RESTYPES = {
-    "psc_last_error": C.c_char_p, "psc_abi_version": u32, "psc_sizeof_params": C.c_size_t,
+    "psc_last_error": C.c_char_p, "psc_abi_version": u32, "psc_build_id": C.c_char_p, "psc_sizeof_params": C.c_size_t,
     "psc_sizeof_layer": C.c_size_t, "psc_sizeof_frame": C.c_size_t, "psc_sizeof_world": C.c_size_t,
 }
 EXPORTED = tuple(_PROTOS)

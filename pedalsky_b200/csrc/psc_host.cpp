@@ -1120,6 +1120,11 @@ extern "C" {
 
 const char* psc_last_error(void) { return g_last_error.c_str(); }
 uint32_t psc_abi_version(void) { return PSC_ABI_VERSION; }
+
+#ifndef PSC_BUILD_ID
+#define PSC_BUILD_ID "unknown"
+#endif
+const char* psc_build_id(void) { return PSC_BUILD_ID; }
 size_t psc_sizeof_params(void) { return sizeof(PscCloudParamsGpu); }
 size_t psc_sizeof_layer(void) { return sizeof(PscCloudLayerGpu); }
 size_t psc_sizeof_frame(void) { return sizeof(PscFrameUniformsGpu); }

@@ -233,3 +233,11 @@ def test_synthesise_layers_reports_overlap():
     with pytest.raises(PscError) as e:
         call("psc_synthesise_layers", d, 2, out)
     assert e.value.code == -3
+
+
+def test_loaded_library_was_built_from_these_sources():
+    """psc_build_id is the hash of the sources and flags the binary was
+    compiled from; the one this process loaded must match the tree."""
+    from pedalsky_b200 import build
+    got = capi.lib().psc_build_id().decode()
+    assert got == build.source_hash(), (got, build.source_hash())
