@@ -107,6 +107,13 @@ struct psc_ctx {
   cudaStream_t batch_stream = nullptr;  // capture stream
   cudaGraphExec_t batch_exec = nullptr;
   std::vector<uint64_t> batch_key;
+  // per-view LUT bakes: what each view slot's sky-view / AP LUTs were last
+  // baked from (its frame record, the world, the transmittance and
+  // multi-scatter LUTs' generation, the LUT buffers); a view whose inputs
+  // are unchanged skips its bake (batch_bake: this call's choice per view)
+  std::vector<uint64_t> batch_lut_keys;
+  std::vector<uint8_t> batch_bake;
+  uint64_t lut_generation = 0;  // bumped by every LUT upload or bake
   // per-view form (PscBatchTuning.form = 1): the views in descending
   // estimated cost, and the branch streams and fork/join events the views'
   // kernels are enqueued on (parallel branches of the captured graph)

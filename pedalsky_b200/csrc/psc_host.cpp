@@ -756,7 +756,8 @@ int enqueue_batch_per_view(psc_ctx* c, uint32_t n, cudaStream_t s, bool capturin
   for (uint32_t k = 0; k < n; ++k) {
     const uint32_t i = c->batch_order[k];
     cudaStream_t br = c->batch_branch[k % nb];
-    if (psc::launch_view_lut_bakes(c->world, static_cast<const char*>(c->d_bframes) + i * fl, 1,
+    if (c->batch_bake[i] &&
+        psc::launch_view_lut_bakes(c->world, static_cast<const char*>(c->d_bframes) + i * fl, 1,
                                    c->d_lut_h[PSC_LUT_TRANSMITTANCE], c->d_lut_h[PSC_LUT_MULTISCATTER],
                                    c->d_bsky + (size_t)i * PSC_SKYVIEW_W * PSC_SKYVIEW_H,
                                    c->d_bap + (size_t)i * PSC_AP_W * PSC_AP_H * PSC_AP_D, br))
@@ -789,8 +790,9 @@ int enqueue_batch(psc_ctx* c, uint32_t n, uint32_t n_tiles, cudaStream_t s, bool
   // next call can wait on it after a graph launch.
   PSC_CUDA(cudaEventRecordWithFlags(c->batch_staged, s, capturing ? cudaEventRecordExternal : 0),
            "batch event");
-  if (psc::launch_view_lut_bakes(c->world, c->d_bframes, n, c->d_lut_h[PSC_LUT_TRANSMITTANCE],
-                                 c->d_lut_h[PSC_LUT_MULTISCATTER], c->d_bsky, c->d_bap, s))
+  const bool any_bake = std::find(c->batch_bake.begin(), c->batch_bake.begin() + n, 1) != c->batch_bake.begin() + n;
+  if (any_bake && psc::launch_view_lut_bakes(c->world, c->d_bframes, n, c->d_lut_h[PSC_LUT_TRANSMITTANCE],
+                                             c->d_lut_h[PSC_LUT_MULTISCATTER], c->d_bsky, c->d_bap, s))
     return fail(PSC_ERR_CUDA, "per-view LUT bake launch failed");
   PSC_CUDA(cudaMemsetAsync(c->d_bcounter, 0, sizeof(uint32_t), s), "batch counter reset");
   const int rc = psc::launch_march_batch(c->opts, (int)c->batch_tuning.threads, c->batch_tuning.tile_w,
@@ -1742,6 +1744,7 @@ int psc_upload_lut(psc_ctx* c, int kind, const uint16_t* rgba16f, size_t count) 
   if (rc) return rc;
   if (!c->d_lut_h[kind]) PSC_CUDA(cudaMalloc(&c->d_lut_h[kind], count * 2), "cudaMalloc LUT");
   PSC_CUDA(cudaMemcpy(c->d_lut_h[kind], rgba16f, count * 2, cudaMemcpyHostToDevice), "LUT upload");
+  ++c->lut_generation;
   return upload_lut_float4(c, kind, rgba16f);
 }
 
@@ -1753,6 +1756,7 @@ int psc_bake_luts(psc_ctx* c, void* stream) {
   for (int k = 0; k < 4; ++k)
     if (!c->d_lut_h[k]) PSC_CUDA(cudaMalloc(&c->d_lut_h[k], lut_texels(k) * 8), "cudaMalloc LUT");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ++c->lut_generation;
   if (psc::launch_lut_bakes(c->world, c->frame, c->d_lut_h[0], c->d_lut_h[1], c->d_lut_h[2], c->d_lut_h[3], s))
     return fail(PSC_ERR_CUDA, "LUT bake launch failed");
   PSC_CUDA(cudaStreamSynchronize(s), "LUT bake");
@@ -2005,6 +2009,21 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
   uint32_t n_tiles = 0;
   rc = stage_batch(c, views, n, &n_tiles);
   if (rc) return rc;
+  // which views bake their sky-view / AP LUTs: those whose inputs changed
+  // since their slot's last bake
+  std::vector<uint64_t> lut_keys(n);
+  {
+    const uint64_t ptrs[] = {c->lut_generation, (uint64_t)(uintptr_t)c->d_bsky, (uint64_t)(uintptr_t)c->d_bap,
+                             (uint64_t)(uintptr_t)c->d_lut_h[PSC_LUT_TRANSMITTANCE],
+                             (uint64_t)(uintptr_t)c->d_lut_h[PSC_LUT_MULTISCATTER]};
+    const uint64_t seed = fnv1a(ptrs, sizeof(ptrs), fnv1a(&c->world, sizeof(c->world)));
+    const size_t fl = psc::frame_lite_size();
+    c->batch_bake.assign(n, 1);
+    for (uint32_t i = 0; i < n; ++i) {
+      lut_keys[i] = fnv1a(static_cast<const char*>(c->h_bframes) + i * fl, fl, seed);
+      c->batch_bake[i] = !(i < c->batch_lut_keys.size() && c->batch_lut_keys[i] == lut_keys[i]);
+    }
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool per_view = c->batch_tuning.form == PSC_BATCH_PER_VIEW;
   const uint64_t marches = per_view ? n : 1;  // march-kernel launches per call
@@ -2012,8 +2031,10 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
     return per_view ? enqueue_batch_per_view(c, n, st, capturing) : enqueue_batch(c, n, n_tiles, st, capturing);
   };
   if (!c->batch_tuning.use_graph) {
+    c->batch_lut_keys.clear();  // a failed enqueue may have baked some views and not others
     rc = enqueue(s, false);
     if (rc) return rc;
+    c->batch_lut_keys = lut_keys;
     c->launches += marches;
     return PSC_OK;
   }
@@ -2030,7 +2051,8 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
                                (uint64_t)(uintptr_t)c->d_bu, (uint64_t)(uintptr_t)c->d_btiles,
                                (uint64_t)(uintptr_t)c->d_bframes,
                                (uint64_t)(uintptr_t)c->d_base_store, (uint64_t)c->tex_base,
-                               (uint64_t)psc::needs_full_paths(c->h_bu, n)};
+                               (uint64_t)psc::needs_full_paths(c->h_bu, n),
+                               fnv1a(c->batch_bake.data(), n)};
   if (per_view) {
     key.push_back(fnv1a(c->h_bu, n * sizeof(psc::MarchUniforms)));
     key.push_back(fnv1a(c->h_bv, n * sizeof(psc::ViewDev)));
@@ -2065,7 +2087,9 @@ int psc_render_batch(psc_ctx* c, const PscBatchView* views, uint32_t n, void* st
     cudaGraphDestroy(g);
     c->batch_key = key;
   }
+  c->batch_lut_keys.clear();
   PSC_CUDA(cudaGraphLaunch(c->batch_exec, s), "graph launch");
+  c->batch_lut_keys = lut_keys;
   c->launches += marches;
   return PSC_OK;
 }

@@ -139,6 +139,56 @@ def test_per_view_graph_follows_uniform_changes(small_batch, oracle_noise):
     sub.close()
 
 
+@pytest.mark.parametrize("form,use_graph", [(capi.BATCH_PERSISTENT, 0), (capi.BATCH_PERSISTENT, 1),
+                                            (capi.BATCH_PER_VIEW, 0), (capi.BATCH_PER_VIEW, 1)])
+def test_view_luts_are_rebaked_exactly_when_their_inputs_change(small_batch, oracle_noise, form, use_graph):
+    """A view's sky-view / AP LUTs are baked again only when its frame (or
+    the world or the base LUTs) changed since its slot's last bake: a moved
+    sun re-bakes that view (the image equals a fresh context's), moving it
+    back restores the first image bit for bit, and repeated calls reuse the
+    LUTs (the image does not change)."""
+    torch = _gpu.torch_cuda()
+    views = list(small_batch)
+
+    def fresh(vs):
+        sub = subsystem_for_scene(vs[0], luts=None, noise=oracle_noise)
+        b = B.Batch(vs, "cuda:0", outputs=("luminance", "transmittance"))
+        B.set_tuning(sub.handle, 128, 16, use_graph, form)
+        b.render(sub.handle)
+        torch.cuda.synchronize()
+        out = [L.cpu().numpy() for L in b.lum]
+        sub.close()
+        return out
+
+    sub = subsystem_for_scene(views[0], luts=None, noise=oracle_noise)
+    try:
+        b = B.Batch(views, "cuda:0", outputs=("luminance", "transmittance"))
+        B.set_tuning(sub.handle, 128, 16, use_graph, form)
+        b.render(sub.handle)
+        b.render(sub.handle)
+        torch.cuda.synchronize()
+        first = [L.cpu().numpy().copy() for L in b.lum]
+        f0 = b.arr[1].frame
+        f = scenes.frame_for(views[1].width, views[1].height, sun_alt_deg=8.0)
+        b.arr[1].frame = f
+        b.render(sub.handle)
+        torch.cuda.synchronize()
+        moved = [L.cpu().numpy().copy() for L in b.lum]
+        import dataclasses
+        ref = fresh([views[0], dataclasses.replace(views[1], frame=f)] + views[2:])
+        for k, (a, r) in enumerate(zip(moved, ref)):
+            assert np.array_equal(a, r), k
+        assert not np.array_equal(moved[1], first[1])
+        b.arr[1].frame = f0
+        b.render(sub.handle)
+        b.render(sub.handle)
+        torch.cuda.synchronize()
+        for a, r in zip(b.lum, first):
+            assert np.array_equal(a.cpu().numpy(), r)
+    finally:
+        sub.close()
+
+
 def test_autotuner_picks_a_valid_shape(small_batch, oracle_noise):
     _gpu.torch_cuda()
     sub = subsystem_for_scene(small_batch[0], luts=None, noise=oracle_noise)
