@@ -168,7 +168,7 @@ def test_view_luts_are_rebaked_exactly_when_their_inputs_change(small_batch, ora
         b.render(sub.handle)
         torch.cuda.synchronize()
         first = [L.cpu().numpy().copy() for L in b.lum]
-        f0 = b.arr[1].frame
+        f0 = capi.FrameUniformsGpu.from_buffer_copy(b.arr[1].frame)  # a copy, not a view of the array
         f = scenes.frame_for(views[1].width, views[1].height, sun_alt_deg=8.0)
         b.arr[1].frame = f
         b.render(sub.handle)
