@@ -651,22 +651,28 @@ int psc_layer_gradient(psc_ctx* ctx, const PscDensityGrid* grid, const PscView* 
                        const float* background, const float* target, double* grad_base_top,
                        void* stream);
 
-/* Gradient of the procedural march's image loss with respect to the density
- * parameters of scene layer `layer` (cloud_march.wgsl:432-530,
- * sample_density): grad[0..3] += d loss / d coverage, shape_bias,
- * detail_bias, density_scale (device doubles); *loss += the loss when
- * `loss` is not null.  Same loss as psc_adjoint: I = L + background * T per
- * pixel and channel, sum((I - target)^2) / (3 * viewport_w * viewport_h)
- * over the view's rectangle (`background`, `target`: device float4 per
- * pixel), so row bands of one viewport add up.  No counterpart in the
- * reference.  Forward mode through the whole march (density, light march,
+/* Gradient of the procedural march's image loss with respect to the
+ * parameters of scene layer `layer`: grad[0..5] += d loss / d coverage,
+ * shape_bias, detail_bias, density_scale (what sample_density,
+ * cloud_march.wgsl:432-530, consumes), base_m and top_m (the layer's shell
+ * radii, its normalised height, skew thickness, mid-altitude wind sample
+ * and light-path end) as device doubles; *loss += the loss when `loss` is
+ * not null.  Same loss as psc_adjoint: I = L + background * T per pixel and
+ * channel, sum((I - target)^2) / (3 * viewport_w * viewport_h) over the
+ * view's rectangle (`background`, `target`: device float4 per pixel), so
+ * row bands of one viewport add up.  No counterpart in the reference.
+ * Forward mode through the whole march (sample positions, the weather,
+ * noise and LUT taps through their filter weights, density, light march,
  * octaves, step integral, transmittance, aerial perspective), FP32 per ray
  * in the PLAIN schedule's arithmetic with exact filtering of the context's
  * noise storage, summed in double; branch decisions (the 1e-3 density
- * threshold, the coverage gate, the early exit) are held at their values.
- * The shape and detail biases act through the diurnal modulation, so their
- * derivatives are 0 for non-convective layer types or diurnal_strength 0.
- * The view's output pointers are not used. */
+ * threshold, the coverage gate, the early exits, the layer hits) are held
+ * at their values.  The shape and detail biases act through the diurnal
+ * modulation, so their derivatives are 0 for non-convective layer types or
+ * diurnal_strength 0.  Not for a Cumulonimbus layer under the approx-Mie
+ * phase (its droplet size varies with height) nor a layer 1 m thick or
+ * less: PSC_ERR_UNSUPPORTED / PSC_ERR_INVALID_ARGUMENT.  The view's output
+ * pointers are not used. */
 int psc_layer_param_gradient(psc_ctx* ctx, const PscView* view, uint32_t layer,
                              const float* background, const float* target, double* grad,
                              double* loss, void* stream);

@@ -138,8 +138,9 @@ int oracle_branch_margins(const OracleScene* scene, uint32_t width, uint32_t hei
                           double* out_d);
 
 /* The FP64 march of `scene` with the outcomes of its discontinuous tests
- * (early exits, the 1e-3 density threshold, the aerial-perspective opacity
- * test) replayed from the FP64 march of `ref` at each pixel: the image as a
+ * (the layer hits and their order, the early exits, the 1e-3 density
+ * threshold, the aerial-perspective opacity test) replayed from the FP64
+ * march of `ref` at each pixel: the image as a
  * smooth function of whatever parameters differ between the two scenes.
  * Returns the number of outcomes a replay needed beyond its record (0 when
  * the two march the same path; -1 on bad arguments). */

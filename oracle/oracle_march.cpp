@@ -144,7 +144,8 @@ int oracle_branch_margins(const OracleScene* s, uint32_t w, uint32_t h, int thre
 }
 
 // Test support: the FP64 march of `s` with the discontinuous tests' outcomes
-// (early exits, the 1e-3 density threshold, the AP opacity test) taken from
+// (layer hits and order, early exits, the 1e-3 density threshold, the AP
+// opacity test) taken from
 // the FP64 march of `ref` at the same pixel (March::branch), so that the
 // image is a smooth function of the parameters that differ between the two
 // scenes: its central differences converge to the derivative with the

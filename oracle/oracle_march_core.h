@@ -672,8 +672,9 @@ struct March {
   }
 
   // Branch tape (oracle_render_frozen): the outcomes of the march's tests
-  // whose result jumps the image (the early exits, the 1e-3 density
-  // threshold, the aerial-perspective opacity test), in the order they run.
+  // whose result jumps the image (the layer hits and their order, the early
+  // exits, the 1e-3 density threshold, the aerial-perspective opacity test),
+  // in the order they run.
   // tape_mode 1 appends each outcome to `tape`; 2 takes each outcome from
   // it instead of the comparison, so a march with other parameters follows
   // the recorded path (a replay that runs past the tape counts a miss and
@@ -708,17 +709,17 @@ struct March {
     } hits[8];
     for (uint32_t l = 0; l < layer_count; ++l) {
       R t0 = 0, t1 = 0;
-      const bool ok = layer_intersect(org, dir, layers[l], &t0, &t1);
+      const bool ok = branch(layer_intersect(org, dir, layers[l], &t0, &t1));
       uint32_t flag = 0;
       if (ok) {
         t1 = std::fmin(t1, depth_t_max);
-        if (t1 > t0) flag = 1;
+        if (branch(t1 > t0)) flag = 1;
       }
       hits[l] = Hit{l, t0, t1, flag};
     }
     for (uint32_t i = 1; i < layer_count; ++i) {
       uint32_t j = i;
-      while (j > 0 && !(hits[j - 1].t0 <= hits[j].t0)) {
+      while (j > 0 && branch(!(hits[j - 1].t0 <= hits[j].t0))) {
         std::swap(hits[j], hits[j - 1]);
         --j;
       }

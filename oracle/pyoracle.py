@@ -236,8 +236,9 @@ def branch_margins(scene, noise, luts, threads=0, rows=None):
 
 
 def render_frozen(ref_scene, scene, noise, luts, threads=0):
-    """FP64 (L, T) of `scene` with the branch outcomes (early exits, density
-    threshold, AP opacity test) of `ref_scene`'s march at each pixel, and the
+    """FP64 (L, T) of `scene` with the branch outcomes (layer hits and order,
+    early exits, density threshold, AP opacity test) of `ref_scene`'s march
+    at each pixel, and the
     number of outcomes the replay lacked (0 when both follow one path)."""
     r, keep_r = make_scene(ref_scene, noise, luts)
     s, keep = make_scene(scene, noise, luts)

@@ -197,6 +197,39 @@ void wind_cache(const psc_ctx* c, const PscCloudParamsGpu& p, const PscFrameUnif
   }
 }
 
+// The wind field at the centre column and altitude `mid` (as wind_cache
+// samples it, in double): its x and z components.
+void wind_at_mid(const psc_ctx* c, double mid, double& wx, double& wz) {
+  wx = wz = 0.0;
+  if (c->h_wind.size() != 32u * 16u * 32u * 4u) return;
+  const double uy = std::fmin(std::fmax(mid / 12000.0, 0.0), 0.9999);
+  auto axis = [](double u, int n, int& i0, int& i1, double& w) {
+    const double x = u * (double)n - 0.5;
+    const double fl = std::floor(x);
+    const int i = (int)fl;
+    i0 = ((i % n) + n) % n;
+    i1 = (((i + 1) % n) + n) % n;
+    w = x - fl;
+  };
+  int x0, x1, y0, y1, z0, z1;
+  double ax, ay, az;
+  axis(0.5, 32, x0, x1, ax);
+  axis(uy, 16, y0, y1, ay);
+  axis(0.5, 32, z0, z1, az);
+  auto tx = [&](int x, int y, int z, int ch) {
+    return (double)half_bits_to_float(c->h_wind[(((size_t)z * 16 + y) * 32 + x) * 4 + ch]);
+  };
+  auto l = [](double a, double b, double t) { return a + (b - a) * t; };
+  double r[2];
+  for (int ch = 0; ch < 2; ++ch) {
+    const double a0 = l(l(tx(x0, y0, z0, ch), tx(x1, y0, z0, ch), ax), l(tx(x0, y1, z0, ch), tx(x1, y1, z0, ch), ax), ay);
+    const double a1 = l(l(tx(x0, y0, z1, ch), tx(x1, y0, z1, ch), ax), l(tx(x0, y1, z1, ch), tx(x1, y1, z1, ch), ax), ay);
+    r[ch] = l(a0, a1, az);
+  }
+  wx = r[0];
+  wz = r[1];
+}
+
 // Flatten one view's scene (params, layers, frame) plus the context's world,
 // options and inputs into the kernel's uniform block.
 // The layer's profile (cloud_density_common.wgsl:49-91) in double, as the
@@ -2501,6 +2534,38 @@ int psc_layer_param_gradient(psc_ctx* c, const PscView* v, uint32_t layer, const
   g.layer = layer;
   g.dlf_dshape = di * 0.5f;
   g.dld_ddetail = (ld_raw > 0.0f && ld_raw < 1.0f) ? di : 0.0f;
+  // base and top move the wind-cache sample (the layer's mid-altitude, d mid
+  // = (d base + d top) / 2; the field is trilinear, so a 0.5 m central
+  // difference is its slope) and the skew thickness max(top - base, 1) * s
+  {
+    const double mid = 0.5 * ((double)L.base_m + (double)L.top_m), h = 0.5;
+    double wx0, wz0, wxp, wzp, wxm, wzm;
+    wind_at_mid(c, mid, wx0, wz0);
+    wind_at_mid(c, mid + h, wxp, wzp);
+    wind_at_mid(c, mid - h, wxm, wzm);
+    const double dwx = (wxp - wxm) / (2.0 * h) * 0.5, dwz = (wzp - wzm) / (2.0 * h) * 0.5;  // per unit base or top
+    const double drift = (double)p.wind_drift_strength * (double)c->frame.simulated_seconds;
+    g.dwind[0][0] = g.dwind[0][1] = (float)(dwx * drift);
+    g.dwind[1][0] = g.dwind[1][1] = (float)(dwz * drift);
+    for (int k = 0; k < 3; ++k) g.dskew[k][0] = g.dskew[k][1] = 0.0f;
+    const psc::LayerConst& o = u.layers[layer];
+    if (o.skew_thickness != 0.0f) {  // skew active (wind_cache)
+      const double sp = std::sqrt(wx0 * wx0 + wz0 * wz0);
+      const double dsp = (wx0 * dwx + wz0 * dwz) / sp;
+      g.dskew[0][0] = g.dskew[0][1] = (float)((dwx * sp - wx0 * dsp) / (sp * sp));
+      g.dskew[1][0] = g.dskew[1][1] = (float)((dwz * sp - wz0 * dsp) / (sp * sp));
+      if (L.top_m - L.base_m > 1.0f) {
+        g.dskew[2][0] = -p.wind_skew_strength;
+        g.dskew[2][1] = p.wind_skew_strength;
+      }
+    }
+  }
+  if (L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE)
+    return fail(PSC_ERR_UNSUPPORTED,
+                "the layer-parameter gradient covers height-independent phase (not the Cumulonimbus droplet "
+                "blend under the approx-Mie phase)");
+  if (!(L.top_m - L.base_m > 1.0f))
+    return fail(PSC_ERR_INVALID_ARGUMENT, "the layer must be more than 1 m thick for its range gradient");
   rc = psc::launch_march_param_grad(u, vd, g, c->opts.storage, grad, loss, static_cast<cudaStream_t>(stream));
   if (rc) return fail(rc, "parameter-gradient launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   ++c->launches;

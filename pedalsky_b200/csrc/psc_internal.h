@@ -192,9 +192,13 @@ struct ParamGradDev {
   uint32_t layer;          // the differentiated layer
   float dlf_dshape;        // d lf_bias / d shape_bias = diurnal / 2
   float dld_ddetail;       // d layer_detail / d detail_bias (diurnal inside the clamp, else 0)
+  // derivatives with respect to (base_m, top_m) of the layer's wind offset
+  // (x, z) and of its skew direction (x, z) and skew thickness
+  float dwind[2][2];
+  float dskew[3][2];
 };
-// out[0..3] += d loss / d (coverage, shape_bias, detail_bias, density_scale)
-// of layer g.layer; *loss += the loss when loss is not null.
+// out[0..5] += d loss / d (coverage, shape_bias, detail_bias, density_scale,
+// base_m, top_m) of layer g.layer; *loss += the loss when loss is not null.
 int launch_march_param_grad(const MarchUniforms& u, const ViewDev& v, const ParamGradDev& g, uint32_t storage,
                             double* out, double* loss, cudaStream_t stream);
 

@@ -1,7 +1,8 @@
 """Host helper for the layer-parameter gradient of the procedural march
-(`psc_layer_param_gradient`): d loss / d coverage, shape_bias, detail_bias
-and density_scale of one scene layer, for the composite loss of the grid
-adjoint (sum((L + background T - target)^2) / (3 viewport pixels)).
+(`psc_layer_param_gradient`): d loss / d coverage, shape_bias, detail_bias,
+density_scale, base_m and top_m of one scene layer, for the composite loss
+of the grid adjoint (sum((L + background T - target)^2) / (3 viewport
+pixels)).
 
 Torch is plumbing for device memory only.  A view whose rectangle is a row
 band of its viewport adds that band's share, so bands (or ranks) add up to
@@ -14,11 +15,11 @@ import ctypes as C
 from .capi import call
 from .subsystem import _stream_handle
 
-PARAMS = ("coverage", "shape_bias", "detail_bias", "density_scale")
+PARAMS = ("coverage", "shape_bias", "detail_bias", "density_scale", "base_m", "top_m")
 
 
 def layer_param_gradient(handle, view, layer: int, background, target, grad, loss=None, stream=None) -> None:
-    """Add d loss / d PARAMS of scene layer `layer` to `grad` (4 device
+    """Add d loss / d PARAMS of scene layer `layer` to `grad` (6 device
     doubles) and the loss to `loss` (1 device double, optional).
     `background` and `target` are device float32 tensors of shape
     (view.height, view.width, 4) covering the view's rectangle."""
