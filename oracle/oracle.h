@@ -141,11 +141,12 @@ int oracle_branch_margins(const OracleScene* scene, uint32_t width, uint32_t hei
  * (the layer hits and their order, the early exits, the 1e-3 density
  * threshold, the aerial-perspective opacity test) replayed from the FP64
  * march of `ref` at each pixel: the image as a
- * smooth function of whatever parameters differ between the two scenes.
+ * smooth function of whatever parameters differ between the two scenes,
+ * written in double.
  * Returns the number of outcomes a replay needed beyond its record (0 when
  * the two march the same path; -1 on bad arguments). */
 long long oracle_render_frozen(const OracleScene* ref, const OracleScene* scene, uint32_t width,
-                               uint32_t height, int threads, float* lum, float* tr);
+                               uint32_t height, int threads, double* lum, double* tr);
 
 /* One FP64 primary density sample at world point p3 / altitude alt in layer
  * li with weather R value weather_r, and the layer profile ndf(h) there

@@ -150,10 +150,12 @@ int oracle_branch_margins(const OracleScene* s, uint32_t w, uint32_t h, int thre
 // image is a smooth function of the parameters that differ between the two
 // scenes: its central differences converge to the derivative with the
 // branches held, which is what a tangent or adjoint of the march computes.
-// Returns the number of outcomes a replay needed beyond its record (0 when
-// both scenes march the same path), or -1 on bad arguments.
+// The image stays in double (central differences of millimetre steps need
+// more than FP32's 7 digits).  Returns the number of outcomes a replay
+// needed beyond its record (0 when both scenes march the same path), or -1
+// on bad arguments.
 long long oracle_render_frozen(const OracleScene* ref, const OracleScene* s, uint32_t w, uint32_t h,
-                               int threads, float* lum, float* tr) {
+                               int threads, double* lum, double* tr) {
   if (!scene_ok(ref) || !scene_ok(s) || !w || !h || !lum || !tr) return -1;
   March<double> base_ref, base;
   base_ref.init(ref, false);
@@ -180,8 +182,8 @@ long long oracle_render_frozen(const OracleScene* ref, const OracleScene* s, uin
         m.pixel(x, (uint32_t)y, s->depth, w, l4, t4);
         const size_t o = ((size_t)y * w + x) * 4;
         for (int c = 0; c < 4; ++c) {
-          lum[o + c] = (float)l4[c];
-          tr[o + c] = (float)t4[c];
+          lum[o + c] = l4[c];
+          tr[o + c] = t4[c];
         }
       }
     }

@@ -236,15 +236,15 @@ def branch_margins(scene, noise, luts, threads=0, rows=None):
 
 
 def render_frozen(ref_scene, scene, noise, luts, threads=0):
-    """FP64 (L, T) of `scene` with the branch outcomes (layer hits and order,
+    """FP64 (L, T) (float64 arrays) of `scene` with the branch outcomes (layer hits and order,
     early exits, density threshold, AP opacity test) of `ref_scene`'s march
     at each pixel, and the
     number of outcomes the replay lacked (0 when both follow one path)."""
     r, keep_r = make_scene(ref_scene, noise, luts)
     s, keep = make_scene(scene, noise, luts)
     w, h = scene.width, scene.height
-    L = np.zeros((h, w, 4), np.float32)
-    T = np.zeros((h, w, 4), np.float32)
+    L = np.zeros((h, w, 4), np.float64)
+    T = np.zeros((h, w, 4), np.float64)
     misses = lib().oracle_render_frozen(C.byref(r), C.byref(s), w, h, threads, _p(L), _p(T))
     if misses < 0:
         raise RuntimeError("oracle_render_frozen failed")

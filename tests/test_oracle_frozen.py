@@ -33,7 +33,7 @@ def test_replay_of_its_own_branches_is_the_march(oracle, oracle_noise):
     L0, T0 = oracle.render(sc, oracle_noise, luts, threads=4)
     L1, T1, misses = oracle.render_frozen(sc, sc, oracle_noise, luts, threads=4)
     assert misses == 0
-    assert np.array_equal(L0, L1) and np.array_equal(T0, T1)
+    assert np.array_equal(L0, L1.astype(np.float32)) and np.array_equal(T0, T1.astype(np.float32))
 
 
 def test_branch_held_loss_is_smooth_in_coverage(oracle, oracle_noise):
