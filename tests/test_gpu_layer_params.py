@@ -29,15 +29,13 @@ convective cumulus layer; it is 0 for the non-convective altostratus layer.
 
 The range derivatives pass through the trilinear noise taps, whose weights
 are piecewise linear in position: the loss has a kink wherever a sample or
-light tap crosses a texel boundary, so its slope is an average over the
-kinks inside the window it is measured on: the FP64 central differences of
-the cumulus base are -2753 over 1 m, -2677 / -2671 over 8 / 4 mm and
--2588 ... -2594 over 2 mm ... 0.25 mm (the branch-held image in double, so
-that millimetre steps resolve).  The FP32 tangent's own sample positions are
-rounded at the millimetre scale, so it sits somewhere in that band (-2660
-on the B200).  The test takes the differences over 8, 4, 2 and 1 mm and
-requires the tangent inside the band they span, widened by 2 % of their
-median."""
+light tap crosses a texel boundary, so central differences over metres
+average the slope over many kinks (-2753 over 1 m for the cumulus base
+against -2650 ... -2658 over 8 ... 1 mm).  They are therefore taken over 8,
+4, 2 and 1 mm (the branch-held image in double, so that millimetre steps
+resolve, each step the float32-rounded parameter values' own difference),
+and the tangent must lie within 2 % of their median (measured on the B200:
+0.15-0.9 %)."""
 import ctypes as C
 import dataclasses
 
@@ -151,8 +149,8 @@ def _central(oracle, noise, p, layer, name, h, target):
 
 @pytest.mark.parametrize("layer", [0, 1])
 def test_altitude_range_gradient_matches_fp64_central_differences(oracle, oracle_noise, prob, layer):
-    """The tangent lies in the band the FP64 central differences span over
-    8, 4, 2 and 1 mm windows, widened by 2 % of their median."""
+    """The tangent lies within 2 % of the median of the FP64 central
+    differences over 8, 4, 2 and 1 mm."""
     g, _ = _gpu_grad(prob, layer, target="tg_r")
     for k, name in ((4, "base_m"), (5, "top_m")):
         fd = np.array([_central(oracle, oracle_noise, prob, layer, name, h, "tgt_r")
@@ -161,7 +159,7 @@ def test_altitude_range_gradient_matches_fp64_central_differences(oracle, oracle
         print(f"\nlayer {layer} d loss / d {name}: GPU {g[k]:.6g}, FD at 8/4/2/1 mm {fd}, "
               f"rel to the median {abs(g[k] - mid) / abs(mid):.2e}")
         assert abs(mid) > 0
-        assert fd.min() - 2e-2 * abs(mid) <= g[k] <= fd.max() + 2e-2 * abs(mid), (g[k], fd)
+        assert abs(g[k] - mid) <= 2e-2 * abs(mid), (g[k], fd)
 
 
 def test_biases_have_no_effect_on_a_non_convective_layer(oracle, oracle_noise, prob):
