@@ -241,3 +241,30 @@ def test_loaded_library_was_built_from_these_sources():
     from pedalsky_b200 import build
     got = capi.lib().psc_build_id().decode()
     assert got == build.source_hash(), (got, build.source_hash())
+
+
+def test_new_entry_points_validate_their_arguments_before_device_work():
+    """The step tuner and the layer-parameter gradient reject bad arguments
+    (and missing inputs) with an error code, without touching a GPU."""
+    c = _ctx()
+    try:
+        views = (capi.BatchView * 1)()
+        before, after = C.c_float(), C.c_float()
+        for args in ((None, 1, 1e-3, 1e-3, 3), (views, 0, 1e-3, 1e-3, 3), (views, 1, 0.0, 1e-3, 3),
+                     (views, 1, float("inf"), 1e-3, 3), (views, 1, 1e-3, 1.0, 3), (views, 1, 1e-3, -0.1, 3),
+                     (views, 1, 1e-3, 1e-3, 0), (views, 1, 1e-3, 1e-3, 101)):
+            with pytest.raises(PscError) as e:
+                call("psc_autotune_steps", c, args[0], args[1], args[2], args[3], args[4], C.byref(before),
+                     C.byref(after), None)
+            assert e.value.code == -1, args
+        v = capi.View(8, 8, None, None, None, None)
+        g = (C.c_double * 6)()
+        with pytest.raises(PscError) as e:
+            call("psc_layer_param_gradient", c, C.byref(v), 0, None, None, g, None, None)
+        assert e.value.code == -1
+        bg = (C.c_float * 256)()
+        with pytest.raises(PscError) as e:  # the context has no layers yet
+            call("psc_layer_param_gradient", c, C.byref(v), 0, bg, bg, g, None, None)
+        assert e.value.code == -1
+    finally:
+        capi.lib().psc_destroy(c)
