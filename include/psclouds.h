@@ -576,9 +576,10 @@ int psc_autotune_batch(psc_ctx* ctx, const PscBatchView* views, uint32_t n, uint
  * that fails ends that view's search.  Writes the chosen counts into
  * views[i].params and the median of `reps` timed runs of the batch before
  * and after into *ms_before / *ms_after (nullable).  Renders into its own
- * scratch outputs with compositing off, so the views' buffers are not
- * written.  1e-3 / 1e-3 is the parity bar of this library's tests (p99.9
- * within 1e-3).  Synchronous. */
+ * scratch outputs with compositing off (64 bytes per pixel of the batch,
+ * allocated and freed by the call), so the views' buffers are not written.
+ * 1e-3 / 1e-3 is the parity bar of this library's tests (p99.9 within
+ * 1e-3).  Synchronous. */
 int psc_autotune_steps(psc_ctx* ctx, PscBatchView* views, uint32_t n, float max_rel_err,
                        float max_share, uint32_t reps, float* ms_before, float* ms_after,
                        void* stream);
