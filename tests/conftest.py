@@ -13,6 +13,13 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 
 
+def pytest_sessionstart(session):
+    # the library under test is the one built from this tree: rebuild it when
+    # its embedded source hash differs (a no-op when it is up to date)
+    from pedalsky_b200 import build
+    build.build()
+
+
 @pytest.fixture(scope="session")
 def oracle():
     from oracle import pyoracle
