@@ -74,15 +74,19 @@ __device__ __forceinline__ Tri grid_coords(const GridDev& g, float x, float alt,
 // the grid (so every load is in bounds) and the weights of corners outside
 // it zeroed, which gives the same sum as visiting the in-grid corners only;
 // a sample with no corner inside the grid loads nothing.
+// The two x corners come as one 8-byte pair (GridDev::pairs, zero outside
+// the grid), so x needs neither clamping nor weight flags: x0 = -1 .. nx-1
+// has a pair, any other x0 no in-grid corner.  The sum equals the clamped
+// per-corner form term for term (an outside corner adds weight x 0).
 __device__ __forceinline__ float grid_fetch(const GridDev& g, const Tri& t) {
-  const bool x0 = (uint32_t)t.x0 < g.nx, x1 = (uint32_t)(t.x0 + 1) < g.nx;
+  const bool xin = (uint32_t)(t.x0 + 1) <= g.nx;
   const bool y0 = (uint32_t)t.y0 < g.ny, y1 = (uint32_t)(t.y0 + 1) < g.ny;
   const bool z0 = (uint32_t)t.z0 < g.nz, z1 = (uint32_t)(t.z0 + 1) < g.nz;
-  if (!((x0 || x1) && (y0 || y1) && (z0 || z1))) return 0.0f;
-  const float wx[2] = {x0 ? 1.0f - t.wx : 0.0f, x1 ? t.wx : 0.0f};
+  if (!(xin && (y0 || y1) && (z0 || z1))) return 0.0f;
+  const float wx0 = 1.0f - t.wx, wx1 = t.wx;
   const float wy[2] = {y0 ? 1.0f - t.wy : 0.0f, y1 ? t.wy : 0.0f};
   const float wz[2] = {z0 ? 1.0f - t.wz : 0.0f, z1 ? t.wz : 0.0f};
-  const uint32_t cx[2] = {(uint32_t)min(max(t.x0, 0), (int)g.nx - 1), (uint32_t)min(max(t.x0 + 1, 0), (int)g.nx - 1)};
+  const uint32_t k = (uint32_t)(t.x0 + 1), stride = g.nx + 1u;
   const uint32_t cy[2] = {(uint32_t)min(max(t.y0, 0), (int)g.ny - 1), (uint32_t)min(max(t.y0 + 1, 0), (int)g.ny - 1)};
   const uint32_t cz[2] = {(uint32_t)min(max(t.z0, 0), (int)g.nz - 1), (uint32_t)min(max(t.z0 + 1, 0), (int)g.nz - 1)};
   float v = 0.0f;
@@ -90,9 +94,9 @@ __device__ __forceinline__ float grid_fetch(const GridDev& g, const Tri& t) {
   for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
     for (int dz = 0; dz < 2; ++dz) {
-      const float* row = g.values + (cy[dy] * g.nz + cz[dz]) * g.nx;
+      const float2 p = __ldg(g.pairs + (cy[dy] * g.nz + cz[dz]) * stride + k);
       const float wyz = wy[dy] * wz[dz];
-      v = fmaf(wyz, fmaf(wx[1], __ldg(row + cx[1]), wx[0] * __ldg(row + cx[0])), v);
+      v = fmaf(wyz, fmaf(wx1, p.y, wx0 * p.x), v);
     }
   return v;
 }
@@ -101,16 +105,19 @@ __device__ __forceinline__ float grid_fetch(const GridDev& g, const Tri& t) {
 // in-grid flags, clamped indices and weights as in grid_fetch, one atomic add
 // per in-grid corner of non-zero weight (a corner outside the grid has
 // weight zero and is skipped).
+// (into the pair layout GridDev::grad_pairs: one 8-byte vector atomic add
+// per in-grid (y, z) corner pair of non-zero weight; the pair slots outside
+// the grid collect weight that the fold ignores)
 __device__ __forceinline__ void grid_scatter(const GridDev& g, const Tri& t, float val) {
   if (val == 0.0f) return;
-  const bool x0 = (uint32_t)t.x0 < g.nx, x1 = (uint32_t)(t.x0 + 1) < g.nx;
+  const bool xin = (uint32_t)(t.x0 + 1) <= g.nx;
   const bool y0 = (uint32_t)t.y0 < g.ny, y1 = (uint32_t)(t.y0 + 1) < g.ny;
   const bool z0 = (uint32_t)t.z0 < g.nz, z1 = (uint32_t)(t.z0 + 1) < g.nz;
-  if (!((x0 || x1) && (y0 || y1) && (z0 || z1))) return;
-  const float wx[2] = {x0 ? (1.0f - t.wx) * val : 0.0f, x1 ? t.wx * val : 0.0f};
+  if (!(xin && (y0 || y1) && (z0 || z1))) return;
+  const float wx0 = (1.0f - t.wx) * val, wx1 = t.wx * val;
   const float wy[2] = {y0 ? 1.0f - t.wy : 0.0f, y1 ? t.wy : 0.0f};
   const float wz[2] = {z0 ? 1.0f - t.wz : 0.0f, z1 ? t.wz : 0.0f};
-  const uint32_t cx[2] = {(uint32_t)min(max(t.x0, 0), (int)g.nx - 1), (uint32_t)min(max(t.x0 + 1, 0), (int)g.nx - 1)};
+  const uint32_t k = (uint32_t)(t.x0 + 1), stride = g.nx + 1u;
   const uint32_t cy[2] = {(uint32_t)min(max(t.y0, 0), (int)g.ny - 1), (uint32_t)min(max(t.y0 + 1, 0), (int)g.ny - 1)};
   const uint32_t cz[2] = {(uint32_t)min(max(t.z0, 0), (int)g.nz - 1), (uint32_t)min(max(t.z0 + 1, 0), (int)g.nz - 1)};
 #pragma unroll
@@ -118,12 +125,8 @@ __device__ __forceinline__ void grid_scatter(const GridDev& g, const Tri& t, flo
 #pragma unroll
     for (int dz = 0; dz < 2; ++dz) {
       const float wyz = wy[dy] * wz[dz];
-      float* row = g.grad + (cy[dy] * g.nz + cz[dz]) * g.nx;
-#pragma unroll
-      for (int dx = 0; dx < 2; ++dx) {
-        const float w = wyz * wx[dx];
-        if (w != 0.0f) atomicAdd(row + cx[dx], w);
-      }
+      if (wyz != 0.0f)
+        atomicAdd(g.grad_pairs + (cy[dy] * g.nz + cz[dz]) * stride + k, make_float2(wyz * wx0, wyz * wx1));
     }
 }
 
@@ -473,10 +476,40 @@ cudaError_t launch_adjoint(const MarchUniforms& u, const ViewDev& v, const GridD
   return cudaGetLastError();
 }
 
+__global__ void k_grid_pairs(const float* __restrict__ v, float2* __restrict__ p, uint32_t nx, uint32_t rows) {
+  const uint32_t stride = nx + 1u;
+  const uint64_t n = (uint64_t)rows * stride;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = (uint32_t)(i / stride), k = (uint32_t)(i % stride);
+    const float* row = v + (size_t)r * nx;
+    p[i] = make_float2(k > 0u ? __ldg(row + k - 1u) : 0.0f, k < nx ? __ldg(row + k) : 0.0f);
+  }
+}
+
+__global__ void k_grid_fold(const float2* __restrict__ gp, float* __restrict__ grad, uint32_t nx, uint32_t rows) {
+  const uint64_t n = (uint64_t)rows * nx;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = (uint32_t)(i / nx), x = (uint32_t)(i % nx);
+    const float2* row = gp + (size_t)r * (nx + 1u);
+    grad[i] += __ldg(row + x + 1u).x + __ldg(row + x).y;
+  }
+}
+
 }  // namespace
+
+int launch_grid_pairs(const float* values, float2* pairs, uint32_t nx, uint32_t rows, cudaStream_t s) {
+  k_grid_pairs<<<148u * 8u, 256, 0, s>>>(values, pairs, nx, rows);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
+
+int launch_grid_fold(const float2* grad_pairs, float* grad, uint32_t nx, uint32_t rows, cudaStream_t s) {
+  k_grid_fold<<<148u * 8u, 256, 0, s>>>(grad_pairs, grad, nx, rows);
+  return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
+}
 
 int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g, bool adjoint,
                       cudaStream_t s) {
+  if (!g.pairs || (adjoint && !g.grad_pairs)) return PSC_ERR_INVALID_ARGUMENT;
   if (u.octaves == 0 || u.octaves > (uint32_t)kMaxOct) return PSC_ERR_UNSUPPORTED;
   if (adjoint && (g.k_cp == 0 || g.k_cp > (uint32_t)kMaxSeg ||
                   (u.cloud_steps + g.k_cp - 1) / g.k_cp > (uint32_t)kMaxCp))

@@ -1532,6 +1532,8 @@ int psc_destroy(psc_ctx* c) {
   dfree(c->d_rt_t);
   dfree(c->d_rt_depth);
   dfree(c->d_check);
+  dfree(c->d_grid_pairs);
+  dfree(c->d_grad_pairs);
   for (auto& tv : c->taa) free_taa_view(tv);
   dfree(c->d_blue);
   dfree(c->d_weather);
@@ -2443,6 +2445,28 @@ int prepare_grid(psc_ctx* c, const PscDensityGrid* g, const PscView* v, bool adj
   return PSC_OK;
 }
 
+// The grid values as x pairs (GridDev::pairs) on `s`, and for the adjoint a
+// zeroed gradient in the same layout (GridDev::grad_pairs).
+int stage_grid_pairs(psc_ctx* c, psc::GridDev& gd, bool adjoint, cudaStream_t s) {
+  const size_t n = (size_t)gd.ny * gd.nz * (gd.nx + 1u);
+  if (c->grid_pairs_cap < n) {
+    dfree(c->d_grid_pairs);
+    dfree(c->d_grad_pairs);
+    c->grid_pairs_cap = 0;
+    PSC_CUDA(cudaMalloc(&c->d_grid_pairs, n * sizeof(float2)), "cudaMalloc grid pairs");
+    PSC_CUDA(cudaMalloc(&c->d_grad_pairs, n * sizeof(float2)), "cudaMalloc gradient pairs");
+    c->grid_pairs_cap = n;
+  }
+  if (psc::launch_grid_pairs(gd.values, c->d_grid_pairs, gd.nx, gd.ny * gd.nz, s))
+    return fail(PSC_ERR_CUDA, "grid pair launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  gd.pairs = c->d_grid_pairs;
+  if (adjoint) {
+    PSC_CUDA(cudaMemsetAsync(c->d_grad_pairs, 0, n * sizeof(float2), s), "gradient pair reset");
+    gd.grad_pairs = c->d_grad_pairs;
+  }
+  return PSC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2452,6 +2476,8 @@ int psc_render_grid(psc_ctx* c, const PscDensityGrid* g, const PscView* v, void*
   psc::ViewDev vd;
   psc::GridDev gd;
   int rc = prepare_grid(c, g, v, false, u, vd, gd);
+  if (rc) return rc;
+  rc = stage_grid_pairs(c, gd, false, static_cast<cudaStream_t>(stream));
   if (rc) return rc;
   rc = psc::launch_grid_march(u, vd, gd, false, static_cast<cudaStream_t>(stream));
   if (rc) return fail(rc, "grid march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -2474,8 +2500,13 @@ int psc_adjoint(psc_ctx* c, const PscDensityGrid* g, const PscView* v, const flo
   gd.target = reinterpret_cast<const float4*>(target);
   gd.loss = loss;
   gd.grad_scale = grad_density_scale;
-  rc = psc::launch_grid_march(u, vd, gd, true, static_cast<cudaStream_t>(stream));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  rc = stage_grid_pairs(c, gd, true, s);
+  if (rc) return rc;
+  rc = psc::launch_grid_march(u, vd, gd, true, s);
   if (rc) return fail(rc, "adjoint launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  rc = psc::launch_grid_fold(gd.grad_pairs, grad_values, gd.nx, gd.ny * gd.nz, s);
+  if (rc) return fail(rc, "gradient fold launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   ++c->launches;
   return PSC_OK;
 }
