@@ -175,3 +175,40 @@ def test_lut_bakes_are_sane(oracle):
     assert np.isfinite(sky).all() and np.isfinite(ap).all()
     # AP transmittance falls with distance
     assert ap[0, 16, 16, 3] > ap[-1, 16, 16, 3]
+
+
+_PROFILE_SCENE = {}
+
+
+def _profile(oracle, oracle_noise, cloud_type, h, anvil_bias=1.0):
+    """The oracle's ndf(h) of one layer of the given type (via its density
+    sample, which also returns the layer profile at the sample's height)."""
+    import dataclasses
+    if not _PROFILE_SCENE:
+        s = scenes.plain_320x180(8, 8)
+        _PROFILE_SCENE.update(s=s, luts=oracle.bake_luts(s.frame, s.world))
+    s, luts = _PROFILE_SCENE["s"], _PROFILE_SCENE["luts"]
+    layers = (capi.CloudLayerGpu * 8).from_buffer_copy(s.layers)
+    layers[0].cloud_type, layers[0].anvil_bias = cloud_type, anvil_bias
+    s2 = dataclasses.replace(s, layers=layers)
+    L = s2.layers[0]
+    alt = L.base_m + h * (L.top_m - L.base_m)
+    _, prof = oracle.density_sample(s2, oracle_noise, luts, 0, [0.0, alt, 0.0], alt, 1.0)
+    return prof
+
+
+def test_profile_known_answers(oracle, oracle_noise):
+    """The reference's own profile tests (crates/ps-synthesis/src/ndf.rs:66-112,
+    its CPU mirror of the march's profile, which agrees with the WGSL
+    cloud_density_common.wgsl:49-91 for these types): cumulus is zero at base
+    and top and peaks below h = 0.55 above 0.5; the cumulonimbus anvil is
+    non-zero at h = 0.92 and mid-cloud at h = 0.4; an unknown type is 0."""
+    assert abs(_profile(oracle, oracle_noise, 0, 0.0)) < 1e-3
+    assert abs(_profile(oracle, oracle_noise, 0, 1.0)) < 1e-3
+    hs = np.arange(0.0, 1.0 + 1e-9, 0.05)
+    vals = [_profile(oracle, oracle_noise, 0, h) for h in hs]
+    k = int(np.argmax(vals))
+    assert hs[k] < 0.55 and vals[k] > 0.5, (hs[k], vals[k])
+    assert _profile(oracle, oracle_noise, 7, 0.92) > 0.05
+    assert _profile(oracle, oracle_noise, 7, 0.4) > 0.05
+    assert _profile(oracle, oracle_noise, 99, 0.5) == 0.0
