@@ -190,3 +190,36 @@ def test_argument_errors(prob):
     with pytest.raises(PscError):
         capi.call("psc_layer_param_gradient", prob["sub"].handle, C.byref(view), 0, None,
                   C.c_void_p(prob["tg"].data_ptr()), C.c_void_p(g.data_ptr()), None, None)
+
+
+@pytest.mark.parametrize("variant", ["cone", "kahan"])
+def test_light_path_variants(oracle, oracle_noise, variant):
+    """The cone light sampling (cloud_march.wgsl:599-666) and the Kahan
+    option: the cumulus coverage and top derivatives against the FP64
+    branch-held central differences, as above."""
+    torch = _gpu.torch_cuda()
+    sc = scenes.precision_1080p(W, H, storage=capi.STORAGE_F32, schedule=capi.SCHED_PLAIN,
+                                filt=capi.FILTER_EXACT, kahan=int(variant == "kahan"))
+    sc.params.diurnal_strength = 1.0
+    if variant == "cone":
+        sc.params.cone_light_sampling = 1
+    luts = oracle.bake_luts(sc.frame, sc.world)
+    moved = _moved(sc, 0, dict(coverage=0.04, top_m=-60.0))
+    Lt, Tt = oracle.render(moved, oracle_noise, luts, threads=8)
+    tgt = (Lt + sc.background * Tt).astype(np.float32)
+    sub = subsystem_for_scene(sc, luts=luts, noise=oracle_noise)
+    try:
+        dev = torch.device("cuda", 0)
+        p = dict(sc=sc, luts=luts, tgt=tgt, sub=sub, torch=torch,
+                 bg=torch.from_numpy(np.ascontiguousarray(sc.background, np.float32)).to(dev),
+                 tg=torch.from_numpy(tgt).to(dev),
+                 depth=torch.from_numpy(np.ascontiguousarray(sc.depth, np.float32)).to(dev))
+        g, _ = _gpu_grad(p, 0)
+        fd_cov = _richardson(oracle, oracle_noise, p, 0, "coverage", 2e-3)
+        fd_top = np.array([_central(oracle, oracle_noise, p, 0, "top_m", h, "tgt") for h in (4e-3, 2e-3, 1e-3)])
+        mid = float(np.median(fd_top))
+        print(f"\n[{variant}] coverage GPU {g[0]:.6e} FD {fd_cov:.6e}; top GPU {g[5]:.6g} FD {fd_top}")
+        assert abs(g[0] - fd_cov) <= 5e-3 * abs(fd_cov)
+        assert abs(g[5] - mid) <= 2e-2 * abs(mid)
+    finally:
+        sub.close()
