@@ -736,9 +736,10 @@ __device__ __forceinline__ float one_minus_exp_neg(float y, float e) {
 // intervals, all touched at most once per dense sample and so kept out of
 // the registers the step loop needs: the per-layer octave coefficients (two
 // sets for a Cumulonimbus layer: its own droplet size and 50 um), the
-// compensated optical depths of the Kahan form, the radiance and the
-// aerial-perspective distance weights.
-constexpr uint32_t kAuxWords = 2 * kMaxOct + 6 + 5;
+// compensated optical depths of the Kahan form, the radiance, the
+// aerial-perspective distance weights and (lean form) the ray's layer order
+// and hit mask.
+constexpr uint32_t kAuxWords = 2 * kMaxOct + 6 + 5 + 2;
 
 // Fetch tally of the instrumented build (TALLY = true): per ray, the
 // fetches march_pixel_fast issues, by kind, in the order of PscFetchCounts.
@@ -781,15 +782,25 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
       s_t1[j * stride + slot] = rs.t1[j];
     }
   }
-  const uint32_t order = rs.order, hit_mask = rs.hit_mask;
+  // the lean form keeps the layer order and hit mask in shared memory too,
+  // and recomputes cos(view, sun) and the forward gain per layer: values
+  // that the step loop does not read stay out of its registers (1080p
+  // frame 3.949 -> 3.898 ms, the same image; the full form is left as it
+  // was, where the change measured 0.8 % slower on the 4K frames)
+  uint32_t* const s_ord = reinterpret_cast<uint32_t*>(s_aux + (kAuxWords - 2) * stride);
+  const uint32_t order = FULL ? rs.order : 0u, hit_mask = FULL ? rs.hit_mask : 0u;
+  if constexpr (!FULL) {
+    s_ord[slot] = rs.order;
+    s_ord[stride + slot] = rs.hit_mask;
+  }
   const float ray_r0 = rs.r0, ray_h0 = rs.h0;
   // distance from the planet centre along the ray: r(t)^2 = A + t (B + t)
   const float ray_A = ray_r0 * ray_r0, ray_B = 2.0f * ray_r0 * rs.cos_view;
   const float dx = rs.dir[0], dy = rs.dir[1], dz = rs.dir[2];
   const float cx = u.cam[0], cy = u.cam[1], cz = u.cam[2];
-  const float cos_theta = fmaf(dx, u.sun[0], fmaf(dy, u.sun[1], dz * u.sun[2]));
-  const float fwd_gain =
-      u.forward_bias > 0.0f ? 1.0f + u.forward_bias * smoothstepf(0.0f, 1.0f, fmaxf(cos_theta, 0.0f))
+  const float cos_theta_r = fmaf(dx, u.sun[0], fmaf(dy, u.sun[1], dz * u.sun[2]));
+  const float fwd_gain_r =
+      u.forward_bias > 0.0f ? 1.0f + u.forward_bias * smoothstepf(0.0f, 1.0f, fmaxf(cos_theta_r, 0.0f))
                             : 1.0f;
   uint32_t sx = (px + v.x_off) & 63u, sy = (py + v.y_off) & 63u;
   if (u.temporal_jitter) {
@@ -816,8 +827,8 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
 
   for (uint32_t k = 0; k < nl; ++k) {
     if (fmaxf(Tr, fmaxf(Tg, Tb)) < 0.01f) break;
-    const uint32_t li = (order >> (4u * k)) & 15u;
-    if (!((hit_mask >> li) & 1u)) continue;
+    const uint32_t li = ((FULL ? order : s_ord[slot]) >> (4u * k)) & 15u;
+    if (!(((FULL ? hit_mask : s_ord[stride + slot]) >> li) & 1u)) continue;
     const float t0 = s_t0[li * stride + slot], t1 = s_t1[li * stride + slot];
     const LayerConst& L = u.layers[li];
     const float segment = t1 - t0;
@@ -834,6 +845,11 @@ __device__ __forceinline__ void march_pixel_fast(const MarchUniforms& u, const V
         continue;
     }
     const bool cb = FULL && L.cloud_type == 7u && u.phase_mode == PSC_PHASE_APPROX_MIE;
+    const float cos_theta = FULL ? cos_theta_r : fmaf(dx, u.sun[0], fmaf(dy, u.sun[1], dz * u.sun[2]));
+    const float fwd_gain =
+        FULL ? fwd_gain_r
+             : (u.forward_bias > 0.0f ? 1.0f + u.forward_bias * smoothstepf(0.0f, 1.0f, fmaxf(cos_theta, 0.0f))
+                                      : 1.0f);
 
     // per ray and layer: a^n * phase_n * forward gain (shared memory)
     if (u.phase_mode == PSC_PHASE_DUAL_LOBE_HG) {
