@@ -78,7 +78,7 @@ PARITY = {
 # ncu figures of the timed kernel on the benchmark command: DRAM bytes read +
 # written per launch and the fraction of issue slots busy (the binding limit).
 NCU_KERNEL = {("precision_1080p", "fast", "f16", "hybrid", 1920, 1080):
-              {"traffic": 136916992, "issue_active": 0.813}}
+              {"traffic": 132197120, "issue_active": 0.837}}
 
 
 def workload_config(wl, W, H):
