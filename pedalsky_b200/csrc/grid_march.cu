@@ -74,30 +74,27 @@ __device__ __forceinline__ Tri grid_coords(const GridDev& g, float x, float alt,
 // the grid (so every load is in bounds) and the weights of corners outside
 // it zeroed, which gives the same sum as visiting the in-grid corners only;
 // a sample with no corner inside the grid loads nothing.
-// The two x corners come as one 8-byte pair (GridDev::pairs, zero outside
-// the grid), so x needs neither clamping nor weight flags: x0 = -1 .. nx-1
-// has a pair, any other x0 no in-grid corner.  The sum equals the clamped
-// per-corner form term for term (an outside corner adds weight x 0).
+// The four (x, z) corners of a y row come as one 16-byte quad
+// (GridDev::quads, zero outside the grid), so x and z need neither clamping
+// nor weight flags: x0 = -1 .. nx-1 and z0 = -1 .. nz-1 have a quad, any
+// other no in-grid corner.  The sum equals the clamped per-corner form term
+// for term (an outside corner adds weight x 0).
 __device__ __forceinline__ float grid_fetch(const GridDev& g, const Tri& t) {
-  const bool xin = (uint32_t)(t.x0 + 1) <= g.nx;
+  const bool xin = (uint32_t)(t.x0 + 1) <= g.nx, zin = (uint32_t)(t.z0 + 1) <= g.nz;
   const bool y0 = (uint32_t)t.y0 < g.ny, y1 = (uint32_t)(t.y0 + 1) < g.ny;
-  const bool z0 = (uint32_t)t.z0 < g.nz, z1 = (uint32_t)(t.z0 + 1) < g.nz;
-  if (!(xin && (y0 || y1) && (z0 || z1))) return 0.0f;
+  if (!(xin && zin && (y0 || y1))) return 0.0f;
   const float wx0 = 1.0f - t.wx, wx1 = t.wx;
+  const float wz0 = 1.0f - t.wz, wz1 = t.wz;
   const float wy[2] = {y0 ? 1.0f - t.wy : 0.0f, y1 ? t.wy : 0.0f};
-  const float wz[2] = {z0 ? 1.0f - t.wz : 0.0f, z1 ? t.wz : 0.0f};
-  const uint32_t k = (uint32_t)(t.x0 + 1), stride = g.nx + 1u;
+  const uint32_t k = (uint32_t)(t.x0 + 1), zk = (uint32_t)(t.z0 + 1), stride = g.nx + 1u;
   const uint32_t cy[2] = {(uint32_t)min(max(t.y0, 0), (int)g.ny - 1), (uint32_t)min(max(t.y0 + 1, 0), (int)g.ny - 1)};
-  const uint32_t cz[2] = {(uint32_t)min(max(t.z0, 0), (int)g.nz - 1), (uint32_t)min(max(t.z0 + 1, 0), (int)g.nz - 1)};
   float v = 0.0f;
 #pragma unroll
-  for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-    for (int dz = 0; dz < 2; ++dz) {
-      const float2 p = __ldg(g.pairs + (cy[dy] * g.nz + cz[dz]) * stride + k);
-      const float wyz = wy[dy] * wz[dz];
-      v = fmaf(wyz, fmaf(wx1, p.y, wx0 * p.x), v);
-    }
+  for (int dy = 0; dy < 2; ++dy) {
+    const float4 q = __ldg(g.quads + (cy[dy] * (g.nz + 1u) + zk) * stride + k);
+    v = fmaf(wy[dy] * wz0, fmaf(wx1, q.y, wx0 * q.x), v);
+    v = fmaf(wy[dy] * wz1, fmaf(wx1, q.w, wx0 * q.z), v);
+  }
   return v;
 }
 
@@ -476,13 +473,16 @@ cudaError_t launch_adjoint(const MarchUniforms& u, const ViewDev& v, const GridD
   return cudaGetLastError();
 }
 
-__global__ void k_grid_pairs(const float* __restrict__ v, float2* __restrict__ p, uint32_t nx, uint32_t rows) {
-  const uint32_t stride = nx + 1u;
-  const uint64_t n = (uint64_t)rows * stride;
+__global__ void k_grid_quads(const float* __restrict__ v, float4* __restrict__ q, uint32_t nx, uint32_t ny,
+                             uint32_t nz) {
+  const uint32_t sx = nx + 1u, sz = nz + 1u;
+  const uint64_t n = (uint64_t)ny * sz * sx;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t r = (uint32_t)(i / stride), k = (uint32_t)(i % stride);
-    const float* row = v + (size_t)r * nx;
-    p[i] = make_float2(k > 0u ? __ldg(row + k - 1u) : 0.0f, k < nx ? __ldg(row + k) : 0.0f);
+    const uint32_t xk = (uint32_t)(i % sx), zk = (uint32_t)((i / sx) % sz), y = (uint32_t)(i / ((uint64_t)sx * sz));
+    auto at = [&](uint32_t z, uint32_t x) {  // z, x shifted by one: 0 is outside
+      return (z >= 1u && z <= nz && x >= 1u && x <= nx) ? __ldg(v + ((size_t)y * nz + (z - 1u)) * nx + (x - 1u)) : 0.0f;
+    };
+    q[i] = make_float4(at(zk, xk), at(zk, xk + 1u), at(zk + 1u, xk), at(zk + 1u, xk + 1u));
   }
 }
 
@@ -497,8 +497,8 @@ __global__ void k_grid_fold(const float2* __restrict__ gp, float* __restrict__ g
 
 }  // namespace
 
-int launch_grid_pairs(const float* values, float2* pairs, uint32_t nx, uint32_t rows, cudaStream_t s) {
-  k_grid_pairs<<<148u * 8u, 256, 0, s>>>(values, pairs, nx, rows);
+int launch_grid_quads(const float* values, float4* quads, uint32_t nx, uint32_t ny, uint32_t nz, cudaStream_t s) {
+  k_grid_quads<<<148u * 8u, 256, 0, s>>>(values, quads, nx, ny, nz);
   return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
 }
 
@@ -509,7 +509,7 @@ int launch_grid_fold(const float2* grad_pairs, float* grad, uint32_t nx, uint32_
 
 int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g, bool adjoint,
                       cudaStream_t s) {
-  if (!g.pairs || (adjoint && !g.grad_pairs)) return PSC_ERR_INVALID_ARGUMENT;
+  if (!g.quads || (adjoint && !g.grad_pairs)) return PSC_ERR_INVALID_ARGUMENT;
   if (u.octaves == 0 || u.octaves > (uint32_t)kMaxOct) return PSC_ERR_UNSUPPORTED;
   if (adjoint && (g.k_cp == 0 || g.k_cp > (uint32_t)kMaxSeg ||
                   (u.cloud_steps + g.k_cp - 1) / g.k_cp > (uint32_t)kMaxCp))

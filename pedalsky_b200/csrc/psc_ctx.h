@@ -97,11 +97,12 @@ struct psc_ctx {
   float4* d_bsky = nullptr;             // per-view sky-view LUTs
   std::vector<cudaTextureObject_t> batch_sky_tex;  // per-view sky-view LUTs through the texture unit
   float4* d_bap = nullptr;              // per-view aerial-perspective LUTs
-  // voxel-grid form: the grid values and the adjoint's gradient as x pairs
-  // (GridDev::pairs / grad_pairs), grown to the largest grid seen
-  float2* d_grid_pairs = nullptr;
+  // voxel-grid form: the grid values as corner quads and the adjoint's
+  // gradient as x pairs (GridDev::quads / grad_pairs), grown to the largest
+  // grid seen
+  float4* d_grid_quads = nullptr;
   float2* d_grad_pairs = nullptr;
-  size_t grid_pairs_cap = 0;
+  size_t grid_pairs_cap = 0;  // entries of the quad array (the pair array holds as many)
   uint32_t* d_btiles = nullptr;
   uint32_t* d_bcounter = nullptr;
   psc::MarchUniforms* h_bu = nullptr;   // pinned staging

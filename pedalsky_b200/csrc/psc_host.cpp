@@ -1532,7 +1532,7 @@ int psc_destroy(psc_ctx* c) {
   dfree(c->d_rt_t);
   dfree(c->d_rt_depth);
   dfree(c->d_check);
-  dfree(c->d_grid_pairs);
+  dfree(c->d_grid_quads);
   dfree(c->d_grad_pairs);
   for (auto& tv : c->taa) free_taa_view(tv);
   dfree(c->d_blue);
@@ -2445,23 +2445,24 @@ int prepare_grid(psc_ctx* c, const PscDensityGrid* g, const PscView* v, bool adj
   return PSC_OK;
 }
 
-// The grid values as x pairs (GridDev::pairs) on `s`, and for the adjoint a
-// zeroed gradient in the same layout (GridDev::grad_pairs).
-int stage_grid_pairs(psc_ctx* c, psc::GridDev& gd, bool adjoint, cudaStream_t s) {
-  const size_t n = (size_t)gd.ny * gd.nz * (gd.nx + 1u);
-  if (c->grid_pairs_cap < n) {
-    dfree(c->d_grid_pairs);
+// The grid values as (x, z) corner quads (GridDev::quads) on `s`, and for the
+// adjoint a zeroed gradient in x pairs (GridDev::grad_pairs).
+int stage_grid_layout(psc_ctx* c, psc::GridDev& gd, bool adjoint, cudaStream_t s) {
+  const size_t nq = (size_t)gd.ny * (gd.nz + 1u) * (gd.nx + 1u);  // quads
+  const size_t np = (size_t)gd.ny * gd.nz * (gd.nx + 1u);         // gradient pairs
+  if (c->grid_pairs_cap < nq) {
+    dfree(c->d_grid_quads);
     dfree(c->d_grad_pairs);
     c->grid_pairs_cap = 0;
-    PSC_CUDA(cudaMalloc(&c->d_grid_pairs, n * sizeof(float2)), "cudaMalloc grid pairs");
-    PSC_CUDA(cudaMalloc(&c->d_grad_pairs, n * sizeof(float2)), "cudaMalloc gradient pairs");
-    c->grid_pairs_cap = n;
+    PSC_CUDA(cudaMalloc(&c->d_grid_quads, nq * sizeof(float4)), "cudaMalloc grid quads");
+    PSC_CUDA(cudaMalloc(&c->d_grad_pairs, nq * sizeof(float2)), "cudaMalloc gradient pairs");
+    c->grid_pairs_cap = nq;
   }
-  if (psc::launch_grid_pairs(gd.values, c->d_grid_pairs, gd.nx, gd.ny * gd.nz, s))
-    return fail(PSC_ERR_CUDA, "grid pair launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-  gd.pairs = c->d_grid_pairs;
+  if (psc::launch_grid_quads(gd.values, c->d_grid_quads, gd.nx, gd.ny, gd.nz, s))
+    return fail(PSC_ERR_CUDA, "grid quad launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  gd.quads = c->d_grid_quads;
   if (adjoint) {
-    PSC_CUDA(cudaMemsetAsync(c->d_grad_pairs, 0, n * sizeof(float2), s), "gradient pair reset");
+    PSC_CUDA(cudaMemsetAsync(c->d_grad_pairs, 0, np * sizeof(float2), s), "gradient pair reset");
     gd.grad_pairs = c->d_grad_pairs;
   }
   return PSC_OK;
@@ -2477,7 +2478,7 @@ int psc_render_grid(psc_ctx* c, const PscDensityGrid* g, const PscView* v, void*
   psc::GridDev gd;
   int rc = prepare_grid(c, g, v, false, u, vd, gd);
   if (rc) return rc;
-  rc = stage_grid_pairs(c, gd, false, static_cast<cudaStream_t>(stream));
+  rc = stage_grid_layout(c, gd, false, static_cast<cudaStream_t>(stream));
   if (rc) return rc;
   rc = psc::launch_grid_march(u, vd, gd, false, static_cast<cudaStream_t>(stream));
   if (rc) return fail(rc, "grid march launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -2501,7 +2502,7 @@ int psc_adjoint(psc_ctx* c, const PscDensityGrid* g, const PscView* v, const flo
   gd.loss = loss;
   gd.grad_scale = grad_density_scale;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  rc = stage_grid_pairs(c, gd, true, s);
+  rc = stage_grid_layout(c, gd, true, s);
   if (rc) return rc;
   rc = psc::launch_grid_march(u, vd, gd, true, s);
   if (rc) return fail(rc, "adjoint launch failed: %s", cudaGetErrorString(cudaGetLastError()));

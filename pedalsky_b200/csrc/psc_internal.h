@@ -169,19 +169,21 @@ struct GridDev {
   const float4* target;    // adjoint: target image per pixel of the view
   double* loss;            // adjoint: accumulated loss
   double* grad_scale;      // adjoint: accumulated d loss / d density_scale
-  // the values as x pairs: entry k of a (y, z) row holds (v[k - 1], v[k]),
-  // zero outside the grid, k = 0..nx (launch_grid_pairs); the adjoint adds
-  // its gradient into the same pair layout (grad_pairs) and folds it into
-  // grad afterwards (launch_grid_fold)
-  const float2* pairs;
+  // the values as (x, z) corner quads: entry (y, zk, xk) holds
+  // v[y][zk-1][xk-1], v[y][zk-1][xk], v[y][zk][xk-1], v[y][zk][xk], zero
+  // outside the grid, zk = 0..nz, xk = 0..nx (launch_grid_quads); the adjoint
+  // adds its gradient into x pairs, entry xk of a (y, z) row for
+  // (x = xk - 1, xk) (grad_pairs), and folds them into grad afterwards
+  // (launch_grid_fold)
+  const float4* quads;
   float2* grad_pairs;
 };
 int launch_grid_march(const MarchUniforms& u, const ViewDev& v, const GridDev& g, bool adjoint,
                       cudaStream_t stream);
-// pairs[r (nx + 1) + k] = (v[r nx + k - 1], v[r nx + k]), zero outside, for
-// the rows r < rows (= ny nz) of an nx-wide grid
-int launch_grid_pairs(const float* values, float2* pairs, uint32_t nx, uint32_t rows, cudaStream_t stream);
+// quads[(y (nz + 1) + zk) (nx + 1) + xk] as GridDev::quads from the ny x nz x
+// nx values
 // grad[r nx + x] += gp[r (nx + 1) + x + 1].x + gp[r (nx + 1) + x].y
+int launch_grid_quads(const float* values, float4* quads, uint32_t nx, uint32_t ny, uint32_t nz, cudaStream_t stream);
 int launch_grid_fold(const float2* grad_pairs, float* grad, uint32_t nx, uint32_t rows, cudaStream_t stream);
 // d loss / d (base_m, top_m) of layer 0 in the grid form, added to out[0..1]
 // (grid_layer_grad.cu); g.bg / g.target / g.inv_n as for the adjoint.
