@@ -706,6 +706,57 @@ def leg_grid(B: Bench, with_e2e=False):
     return out
 
 
+def leg_layer_params(B: Bench, W=480, H=270):
+    """d loss / d (coverage, shape_bias, detail_bias, density_scale, base_m,
+    top_m) of the cumulus layer of the three-layer frame at W x H
+    (psc_layer_param_gradient: the PLAIN march in forward mode with six
+    tangents), the loss against the frame rendered with the layer's coverage
+    0.04 higher.  Each rank computes the whole view (replicas)."""
+    from pedalsky_b200 import capi, scenes
+    from pedalsky_b200.capi import call
+    from pedalsky_b200.layer_grad import layer_param_gradient
+    from pedalsky_b200.subsystem import subsystem_for_scene
+    torch = B.torch
+    sc = scenes.precision_1080p(W, H, storage=capi.STORAGE_F32, schedule=capi.SCHED_PLAIN,
+                                filt=capi.FILTER_EXACT)
+    sc.params.diurnal_strength = 1.0
+    sub = subsystem_for_scene(sc, device=B.ranks.local, luts=None)
+    dev = B.dev
+    bg = torch.from_numpy(np.ascontiguousarray(sc.background, np.float32)).to(dev)
+    depth = torch.from_numpy(np.ascontiguousarray(sc.depth, np.float32)).to(dev)
+    L = torch.zeros((H, W, 4), device=dev)
+    T = torch.zeros_like(L)
+    layers = (capi.CloudLayerGpu * 8).from_buffer_copy(sc.layers)
+    layers[0].coverage += 0.04
+    call("psc_set_layers", sub.handle, layers, sc.n_layers)
+    view = capi.View(W, H, depth.data_ptr(), L.data_ptr(), T.data_ptr(), None)
+    with torch.cuda.stream(B.stream):
+        call("psc_render", sub.handle, C.byref(view), 1, B.sh())
+    torch.cuda.synchronize()
+    target = (L + bg * T).contiguous()
+    call("psc_set_layers", sub.handle, sc.layers, sc.n_layers)
+    grad = torch.zeros(6, dtype=torch.float64, device=dev)
+    loss = torch.zeros(1, dtype=torch.float64, device=dev)
+    gview = capi.View(W, H, depth.data_ptr(), None, None, None)
+
+    def step():
+        grad.zero_()
+        loss.zero_()
+        layer_param_gradient(sub.handle, gview, 0, bg, target, grad, loss, stream=B.stream)
+
+    clk = ClockSampler(B.ranks.local)
+    ms, ms_max = B.timed(step, clk=clk, counter=sub.launch_count)
+    out = {"value": W * H / (ms_max * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_max,
+           "gpu_launches": B.timed_launches, "scaling": "replicas",
+           "config": {"workload": f"precision_1080p {W}x{H}, layer 0 (Cu), six parameters",
+                      "schedule": "plain", "storage": "f32", "filter": "exact"},
+           "gradient": [float(x) for x in grad.cpu().numpy()], "loss": float(loss.cpu().numpy()[0]),
+           "parity": "tests/test_gpu_layer_params.py (FP64 branch-held central differences)",
+           "clocks": clk.summary(), "step_ms": [round(x, 4) for x in ms]}
+    sub.close()
+    return out
+
+
 def _hbm_peak():
     hbm = measured_peaks().get("hbm_gbs")
     return (hbm, "measured (MEASURED_PEAKS.json)") if hbm else (6650.0, "fallback")
@@ -902,6 +953,7 @@ def run_frames(args, ranks: Ranks):
         legs["batch_64"] = leg_batch64(B, storage, filt)
         legs["stress_2160p"] = leg_stress(B, storage, schedule, filt)
         legs["grid_512"] = leg_grid(B)
+        legs["layer_params_480x270"] = leg_layer_params(B)
 
     if ranks.rank == 0:
         roof = roofline(args, wl, W, H, W * H, kernel_ms, peaks_fetch, counts, batched, rays_step)
