@@ -6,9 +6,9 @@ Each translation unit is compiled separately so per-file flags apply
 (noise_bake.cu needs -fmad=false for byte-exact bakes), then linked into one
 shared library next to this file.  The library carries the SHA-256 of the
 sources and flags it was built from (`psc_build_id`), also written beside
-it; a build is redone whenever that hash differs from the current sources'
-(or a source is newer than the library), so a library copied from elsewhere
-is never used for other sources.
+it; a build is redone whenever that hash differs from the current sources',
+so a library copied from elsewhere is never used for other sources, and a
+copied tree (another directory, other file times) keeps its built library.
 """
 from __future__ import annotations
 
@@ -36,6 +36,7 @@ CUDA_UNITS = {
     "grid_march.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "grid_layer_grad.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "march_param_grad.cu": [],
+    "march_range_grad.cu": [],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
     "fetch_peak.cu": [],
@@ -69,17 +70,17 @@ def source_hash() -> str:
     for p in _sources():
         if p.is_file() and p.suffix in (".cu", ".cuh", ".cpp", ".h"):
             h.update(str(p.relative_to(ROOT)).encode() + b"\0" + p.read_bytes() + b"\0")
-    h.update(repr((ARCH, NVCC_COMMON, sorted(CUDA_UNITS.items()), CXX_UNITS)).encode())
+    # the include directory enters by its place in the tree, not this
+    # machine's absolute path, so a copied tree keeps its hash
+    flags = [f if f != str(ROOT / "include") else "include" for f in NVCC_COMMON]
+    h.update(repr((ARCH, flags, sorted(CUDA_UNITS.items()), CXX_UNITS)).encode())
     return h.hexdigest()
 
 
 def needs_build() -> bool:
     if not LIB.exists() or not LIB_ID.exists():
         return True
-    if LIB_ID.read_text().strip() != source_hash():
-        return True
-    t = LIB.stat().st_mtime
-    return any(p.stat().st_mtime > t for p in _sources() if p.is_file())
+    return LIB_ID.read_text().strip() != source_hash()
 
 
 def _run(cmd: list[str], verbose: bool) -> None:
