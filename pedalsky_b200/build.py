@@ -36,7 +36,6 @@ CUDA_UNITS = {
     "grid_march.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "grid_layer_grad.cu": ["-prec-div=false", "-prec-sqrt=false"],
     "march_param_grad.cu": [],
-    "march_range_grad.cu": [],
     "noise_bake.cu": ["-fmad=false"],
     "atmosphere.cu": [],
     "fetch_peak.cu": [],
