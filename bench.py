@@ -110,6 +110,9 @@ def parse(argv=None):
                     help="skip the plain FP32-storage drop-in and the batched form of the frame")
     ap.add_argument("--no-legs", action="store_true",
                     help="skip the 64-view, 8x4K and grid-adjoint legs of the default run")
+    ap.add_argument("--legs", default="all",
+                    help="comma-separated legs of the default run (batch_64, stress_2160p, "
+                         "grid_512, layer_params_480x270, passes_1080p) or all")
     ap.add_argument("--width", type=int, default=None, help="default: the workload's size")
     ap.add_argument("--height", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -757,6 +760,121 @@ def leg_layer_params(B: Bench, W=480, H=270):
     return out
 
 
+def leg_passes(B: Bench, storage, schedule, filt, full_ms=None, W=1920, H=1080):
+    """The passes around the march on the headline frame (W x H): the
+    half-res frame (march into the floor(W/2) x floor(H/2) cloud RT, depth
+    downsample, Catmull-Rom composite into the W x H target), the same with
+    the TAA resolve, and alone the HBM-bound kernels (bytes per pixel over
+    the device time against the HBM peak, the L2 flushed before each step):
+    the Catmull-Rom composite (k_composite_halfres: the RT's L and T once, 8
+    B per output pixel at 2x2, and the target read and written, 32 B), the
+    TAA resolve of a W x H cloud RT (k_taa_resolve: current and history L/T
+    read, resolve written, 96 B per pixel) and the full-res two-pass
+    composite (k_composite: 64 B per pixel); then the per-frame atmosphere
+    LUT bake (transmittance, multi-scatter, sky-view, aerial perspective) and
+    the once-per-context noise bake by wall clock.  Each rank runs the same
+    frame (replicas)."""
+    import time
+    from pedalsky_b200 import capi, scenes
+    from pedalsky_b200.capi import call
+    from pedalsky_b200.subsystem import subsystem_for_scene
+    torch, dev, sh = B.torch, B.dev, B.sh()
+    sc = scenes.precision_1080p(W, H, storage=storage, schedule=schedule, filt=filt)
+    sub = subsystem_for_scene(sc, device=B.ranks.local, luts=None)
+    bg = torch.from_numpy(np.ascontiguousarray(sc.background, np.float32)).to(dev)
+    depth = torch.from_numpy(np.ascontiguousarray(sc.depth, np.float32)).to(dev)
+    hdr = torch.empty_like(bg)
+    rw, rh = C.c_uint32(), C.c_uint32()
+    call("psc_cloud_rt_size", W, H, 1, C.byref(rw), C.byref(rh))
+    rw, rh = rw.value, rh.value
+    peak, src = _hbm_peak()
+    out = {"config": {"workload": f"precision_1080p {W}x{H}, cloud RT {rw}x{rh} at half res",
+                      "storage": B.args.storage, "schedule": B.args.schedule, "filter": B.args.filter,
+                      "l2": "flushed before every step"},
+           "parity": "tests/test_gpu_post.py, tests/test_gpu_march.py (half-res and TAA against the "
+                     "FP64 restatements of the composite and the resolve)"}
+    o0 = capi.MarchOptions.from_buffer_copy(sub.options)
+    view = capi.View(W, H, depth.data_ptr(), None, None, hdr.data_ptr())
+
+    def frame_leg(half_res, taa):
+        o = capi.MarchOptions.from_buffer_copy(o0)
+        o.composite, o.half_res, o.taa = 1, half_res, taa
+        sub.set_options(o)
+        call("psc_invalidate_taa_history", sub.handle)
+        clk = ClockSampler(B.ranks.local)
+        ms, ms_max = B.timed(lambda: (hdr.copy_(bg, non_blocking=True),
+                                      call("psc_render", sub.handle, C.byref(view), 1, sh)),
+                             clk=clk, counter=sub.launch_count)
+        r = {"ms_per_step": ms_max, "Mpixels_per_s": W * H / (ms_max * 1e-3) / 1e6,
+             "march_rays_per_step": rw * rh if half_res else W * H,
+             "gpu_launches": B.timed_launches, "clocks": clk.summary(),
+             "step_ms": [round(x, 4) for x in ms]}
+        if full_ms:
+            r["speedup_vs_full_res_frame"] = full_ms / ms_max
+        return r
+
+    out["half_res_frame"] = frame_leg(1, 0)
+    out["half_res_taa_frame"] = frame_leg(1, 1)
+    sub.set_options(o0)
+
+    def hbm_leg(kernel, step, bytes_per_step, launches):
+        clk = ClockSampler(B.ranks.local)
+        ms, ms_max = B.timed(step, clk=clk)
+        ach = bytes_per_step / (ms_max * 1e-3) / 1e9
+        return {"kernel": kernel, "ms_per_step": ms_max, "gpu_launches": launches * B.args.steps,
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                             "frac": ach / peak, "traffic": None, "peak_source": src,
+                             "bytes_per_step": bytes_per_step},
+                "clocks": clk.summary(), "step_ms": [round(x, 4) for x in ms]}
+
+    rl = torch.rand((rh, rw, 4), device=dev)
+    rt = torch.rand((rh, rw, 4), device=dev)
+    out["composite_halfres"] = hbm_leg(
+        "k_composite_halfres",
+        lambda: call("psc_composite_halfres", C.c_void_p(rl.data_ptr()), C.c_void_p(rt.data_ptr()),
+                     rw, rh, C.c_void_p(hdr.data_ptr()), W, H, sh),
+        rw * rh * 32 + W * H * 32, 1)
+    del rl, rt
+    cl = torch.rand((H, W, 4), device=dev)
+    ct = torch.rand((H, W, 4), device=dev)
+    call("psc_invalidate_taa_history", sub.handle)
+    with torch.cuda.stream(B.stream):  # the first resolve after an invalidate bootstraps
+        call("psc_taa_resolve", sub.handle, C.c_void_p(cl.data_ptr()), C.c_void_p(ct.data_ptr()), W, H,
+             None, None, sh)
+    torch.cuda.synchronize()
+    out["taa_resolve"] = hbm_leg(
+        "k_taa_resolve",
+        lambda: call("psc_taa_resolve", sub.handle, C.c_void_p(cl.data_ptr()), C.c_void_p(ct.data_ptr()),
+                     W, H, None, None, sh),
+        W * H * 96, 1)
+    out["composite"] = hbm_leg(
+        "k_composite",
+        lambda: call("psc_composite", C.c_void_p(cl.data_ptr()), C.c_void_p(ct.data_ptr()),
+                     C.c_void_p(hdr.data_ptr()), W, H, sh),
+        W * H * 64, 1)
+    del cl, ct
+
+    clk = ClockSampler(B.ranks.local)
+    ms, ms_max = B.timed(lambda: call("psc_bake_luts", sub.handle, sh), clk=clk, counter=sub.launch_count)
+    out["lut_bake"] = {"ms_per_step": ms_max, "gpu_launches": B.timed_launches, "bound": "ALU, once per frame",
+                       "luts": "transmittance 256x64, multi-scatter 32x32, sky-view 192x108, "
+                               "aerial perspective 32x32x64",
+                       "clocks": clk.summary(), "step_ms": [round(x, 4) for x in ms]}
+    walls = []
+    for i in range(4):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        call("psc_bake_noise", sub.handle)
+        torch.cuda.synchronize()
+        if i:
+            walls.append(1e3 * (time.perf_counter() - t0))
+    out["noise_bake"] = {"wall_ms": float(np.median(walls)), "bound": "ALU, once per context",
+                         "note": "base 128^3 RGBA8, detail 32^3, curl 128^2, their storage forms and "
+                                 "folds, and the host blue-noise tile; median of 3 after one"}
+    sub.close()
+    return out
+
+
 def _hbm_peak():
     hbm = measured_peaks().get("hbm_gbs")
     return (hbm, "measured (MEASURED_PEAKS.json)") if hbm else (6650.0, "fallback")
@@ -950,10 +1068,14 @@ def run_frames(args, ranks: Ranks):
 
     legs = {}
     if wl == WORKLOAD and not args.no_legs and schedule == capi.SCHED_FAST:
-        legs["batch_64"] = leg_batch64(B, storage, filt)
-        legs["stress_2160p"] = leg_stress(B, storage, schedule, filt)
-        legs["grid_512"] = leg_grid(B)
-        legs["layer_params_480x270"] = leg_layer_params(B)
+        want = set(args.legs.split(",")) if args.legs != "all" else None
+        for name, run in (("batch_64", lambda: leg_batch64(B, storage, filt)),
+                          ("stress_2160p", lambda: leg_stress(B, storage, schedule, filt)),
+                          ("grid_512", lambda: leg_grid(B)),
+                          ("layer_params_480x270", lambda: leg_layer_params(B)),
+                          ("passes_1080p", lambda: leg_passes(B, storage, schedule, filt, full_ms=ms_max))):
+            if want is None or name in want:
+                legs[name] = run()
 
     if ranks.rank == 0:
         roof = roofline(args, wl, W, H, W * H, kernel_ms, peaks_fetch, counts, batched, rays_step)

@@ -397,11 +397,18 @@ int psc_upload_wind(psc_ctx* ctx, const uint16_t* rgba16f, size_t count);
 /* One atmosphere LUT, RGBA16F texels in x-fastest order. */
 int psc_upload_lut(psc_ctx* ctx, int kind, const uint16_t* rgba16f,
                    size_t count);
-/* Bake all four atmosphere LUTs on the device from the current frame and
- * world uniforms (shaders/atmosphere/{transmittance,multiscatter,skyview,
- * aerialperspective}.comp.wgsl). */
+/* Bake the atmosphere LUTs on the device from the current frame and world
+ * uniforms (shaders/atmosphere/{transmittance,multiscatter,skyview,
+ * aerialperspective}.comp.wgsl): the sky-view and aerial-perspective LUTs
+ * every call, the transmittance and multi-scatter LUTs only when the world
+ * uniforms differ from their last bake's or either was uploaded since (the
+ * reference re-bakes those two only when its static inputs are dirty,
+ * crates/ps-atmosphere/src/lib.rs:494-560).  Device work only, queued on
+ * `stream` (later renders on the same stream see the new LUTs); with a NULL
+ * stream the call returns once the bake has finished. */
 int psc_bake_luts(psc_ctx* ctx, void* stream);
-/* Copy one LUT back to the host as RGBA16F. */
+/* Copy one LUT back to the host as RGBA16F (waits for the device's work in
+ * flight first, a bake on any stream included). */
 int psc_download_lut(psc_ctx* ctx, int kind, uint16_t* rgba16f, size_t count);
 
 /* ----------------------------------------------------------- render */

@@ -13,7 +13,9 @@
 //     (the reference's 9 offset-bilinear taps are an exact rewriting of it),
 //     then L >= 0, T in [0, 1] and dst = L + dst * T on all four channels.
 // All three are one thread per output pixel, 16x16 CTAs; every index is
-// clamped into its image.
+// clamped into its image.  The composite stages its RT footprint in shared
+// memory (k_composite_halfres_tiled) whenever the RT is no larger than the
+// target.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -141,22 +143,32 @@ __device__ __forceinline__ void cr_weights(float f, float w[4]) {
   w[3] = f * f * (-0.5f + 0.5f * f);
 }
 
+// First Catmull-Rom tap + 1 of target pixel x (W wide) over an RT rw wide
+// (the texel left of the sample point), and the fraction f in [0, 1), with
+// every rounding explicit (no contraction into FMAs), so the two composite
+// kernels and the tiled kernel's footprint bounds agree exactly.
+__device__ __forceinline__ int cr_base(uint32_t x, uint32_t W, uint32_t rw, float& f) {
+  const float sp = __fmul_rn(__fdiv_rn(__fadd_rn((float)x, 0.5f), (float)W), (float)rw);
+  const float b = floorf(__fsub_rn(sp, 0.5f));
+  f = __fsub_rn(sp, __fadd_rn(b, 0.5f));
+  return (int)b;
+}
+
 __global__ void k_composite_halfres(const float4* __restrict__ l, const float4* __restrict__ t,
                                     uint32_t rw, uint32_t rh, float4* __restrict__ hdr, uint32_t W,
                                     uint32_t H) {
   const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= W || y >= H) return;
-  const float spx = ((float)x + 0.5f) / (float)W * (float)rw;
-  const float spy = ((float)y + 0.5f) / (float)H * (float)rh;
-  const float bx = floorf(spx - 0.5f), by = floorf(spy - 0.5f);
+  float fx, fy;
+  const int bx = cr_base(x, W, rw, fx), by = cr_base(y, H, rh, fy);
   float wx[4], wy[4];
-  cr_weights(spx - (bx + 0.5f), wx);
-  cr_weights(spy - (by + 0.5f), wy);
+  cr_weights(fx, wx);
+  cr_weights(fy, wy);
   int ix[4], iy[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    ix[k] = clampi((int)bx - 1 + k, (int)rw);
-    iy[k] = clampi((int)by - 1 + k, (int)rh);
+    ix[k] = clampi(bx - 1 + k, (int)rw);
+    iy[k] = clampi(by - 1 + k, (int)rh);
   }
   float4 sl = f4(0.0f), st = f4(0.0f);
 #pragma unroll
@@ -172,6 +184,63 @@ __global__ void k_composite_halfres(const float4* __restrict__ l, const float4* 
     st = fma4(rt, wy[j], st);
   }
   const float4 L = max4(sl, f4(0.0f)), T = clamp4(st, f4(0.0f), f4(1.0f));
+  const size_t o = (size_t)y * W + x;
+  const float4 d = hdr[o];
+  hdr[o] = make_float4(fmaf(d.x, T.x, L.x), fmaf(d.y, T.y, L.y), fmaf(d.z, T.z, L.z), fmaf(d.w, T.w, L.w));
+}
+
+constexpr int kCrTile = 24;  // RT texels per axis staged by one CTA
+
+// k_composite_halfres with the RT footprint of the CTA's 16 x 16 target
+// pixels staged once in shared memory: every RT texel is read from L2 about
+// (footprint / 8)^2 = 2.25 times instead of 16 times per target pixel from
+// L1.  Used while the RT is no larger than the target, where the footprint
+// is at most 20 x 20 texels.  The same taps, weights and order as
+// k_composite_halfres: the same image bit for bit.
+__global__ void __launch_bounds__(256) k_composite_halfres_tiled(const float4* __restrict__ l,
+                                                                 const float4* __restrict__ t, uint32_t rw,
+                                                                 uint32_t rh, float4* __restrict__ hdr,
+                                                                 uint32_t W, uint32_t H) {
+  __shared__ float4 sl[kCrTile][kCrTile], st[kCrTile][kCrTile];
+  const uint32_t x0 = blockIdx.x * 16u, y0 = blockIdx.y * 16u;
+  float f;
+  const int sx0 = cr_base(x0, W, rw, f) - 1, sy0 = cr_base(y0, H, rh, f) - 1;
+  const int sx1 = cr_base(min(x0 + 15u, W - 1u), W, rw, f) + 2;
+  const int sy1 = cr_base(min(y0 + 15u, H - 1u), H, rh, f) + 2;
+  const int nx = min(sx1 - sx0 + 1, kCrTile), ny = min(sy1 - sy0 + 1, kCrTile);
+  for (int i = (int)(threadIdx.y * 16u + threadIdx.x); i < nx * ny; i += 256) {
+    const int jy = i / nx, jx = i - jy * nx;
+    const int idx = clampi(sy0 + jy, (int)rh) * (int)rw + clampi(sx0 + jx, (int)rw);
+    sl[jy][jx] = __ldg(l + idx);
+    st[jy][jx] = __ldg(t + idx);
+  }
+  __syncthreads();
+  const uint32_t x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x >= W || y >= H) return;
+  float fx, fy;
+  const int bx = cr_base(x, W, rw, fx), by = cr_base(y, H, rh, fy);
+  float wx[4], wy[4];
+  cr_weights(fx, wx);
+  cr_weights(fy, wy);
+  int jx[4], jy[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {  // tile slot (sx0 + j) holds RT texel clamp(sx0 + j)
+    jx[k] = min(max(bx - 1 + k - sx0, 0), nx - 1);
+    jy[k] = min(max(by - 1 + k - sy0, 0), ny - 1);
+  }
+  float4 acl = f4(0.0f), act = f4(0.0f);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    float4 rl = f4(0.0f), rt = f4(0.0f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      rl = fma4(sl[jy[j]][jx[k]], wx[k], rl);
+      rt = fma4(st[jy[j]][jx[k]], wx[k], rt);
+    }
+    acl = fma4(rl, wy[j], acl);
+    act = fma4(rt, wy[j], act);
+  }
+  const float4 L = max4(acl, f4(0.0f)), T = clamp4(act, f4(0.0f), f4(1.0f));
   const size_t o = (size_t)y * W + x;
   const float4 d = hdr[o];
   hdr[o] = make_float4(fmaf(d.x, T.x, L.x), fmaf(d.y, T.y, L.y), fmaf(d.z, T.z, L.z), fmaf(d.w, T.w, L.w));
@@ -218,7 +287,11 @@ int launch_taa_resolve(const TaaParams& p, cudaStream_t s) {
 
 int launch_composite_halfres(const float4* l, const float4* t, uint32_t rw, uint32_t rh, float4* hdr,
                              uint32_t W, uint32_t H, cudaStream_t s) {
-  k_composite_halfres<<<grid16(W, H), dim3(16, 16), 0, s>>>(l, t, rw, rh, hdr, W, H);
+  if (W == 0 || H == 0 || rw == 0 || rh == 0) return PSC_OK;
+  if (rw <= W && rh <= H)
+    k_composite_halfres_tiled<<<grid16(W, H), dim3(16, 16), 0, s>>>(l, t, rw, rh, hdr, W, H);
+  else
+    k_composite_halfres<<<grid16(W, H), dim3(16, 16), 0, s>>>(l, t, rw, rh, hdr, W, H);
   return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
 }
 

@@ -119,7 +119,17 @@ struct psc_ctx {
   // are unchanged skips its bake (batch_bake: this call's choice per view)
   std::vector<uint64_t> batch_lut_keys;
   std::vector<uint8_t> batch_bake;
-  uint64_t lut_generation = 0;  // bumped by every LUT upload or bake
+  // bumped whenever the transmittance or multi-scatter LUT changes (an
+  // upload of either, a bake of both); the per-view sky-view / AP bakes of
+  // the batched march read those two
+  uint64_t lut_generation = 0;
+  // the world uniforms and lut_generation the last bake of the transmittance
+  // and multi-scatter LUTs produced: psc_bake_luts re-bakes them only when
+  // either differs (the reference's static_dirty latch,
+  // crates/ps-atmosphere/src/lib.rs:494-560)
+  bool static_luts_baked = false;
+  PscWorldUniformsGpu static_luts_world{};
+  uint64_t static_luts_generation = 0;
   // per-view form (PscBatchTuning.form = 1): the views in descending
   // estimated cost, and the branch streams and fork/join events the views'
   // kernels are enqueued on (parallel branches of the captured graph)

@@ -837,10 +837,10 @@ int enqueue_batch(psc_ctx* c, uint32_t n, uint32_t n_tiles, cudaStream_t s, bool
   return PSC_OK;
 }
 
-int upload_lut_float4(psc_ctx* c, int kind, const uint16_t* h16) {
+// The float4 copy of LUT `kind` and, for the transmittance and sky-view
+// LUTs, the texture objects over it; created once per context.
+int ensure_lut_float4(psc_ctx* c, int kind) {
   const size_t n = lut_texels(kind);
-  std::vector<float> f(n * 4);
-  for (size_t i = 0; i < n * 4; ++i) f[i] = half_bits_to_float(h16[i]);
   if (!c->d_lut[kind]) {
     PSC_CUDA(cudaMalloc(&c->d_lut[kind], n * sizeof(float4)), "cudaMalloc LUT");
     if (kind == PSC_LUT_TRANSMITTANCE) {
@@ -863,11 +863,10 @@ int upload_lut_float4(psc_ctx* c, int kind, const uint16_t* h16) {
       PSC_CUDA(cudaCreateTextureObject(&c->tex_lut[kind], &rd, &td, nullptr), "LUT texture object");
     }
   }
-  PSC_CUDA(cudaMemcpy(c->d_lut[kind], f.data(), n * sizeof(float4), cudaMemcpyHostToDevice), "LUT upload");
   if (kind == PSC_LUT_SKYVIEW) {
     // the sky-view LUT also lives in a float4 array behind a texture object
     // (bilinear, clamp, normalised coordinates), refreshed on every upload
-    const size_t row = PSC_SKYVIEW_W * sizeof(float4);
+    // and bake
     if (!c->arr_sky) {
       const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float4>();
       PSC_CUDA(cudaMallocArray(&c->arr_sky, &fmt, PSC_SKYVIEW_W, PSC_SKYVIEW_H), "cudaMallocArray sky-view");
@@ -881,6 +880,19 @@ int upload_lut_float4(psc_ctx* c, int kind, const uint16_t* h16) {
       td.normalizedCoords = 1;
       PSC_CUDA(cudaCreateTextureObject(&c->tex_lut[kind], &rd, &td, nullptr), "sky-view texture object");
     }
+  }
+  return PSC_OK;
+}
+
+int upload_lut_float4(psc_ctx* c, int kind, const uint16_t* h16) {
+  const size_t n = lut_texels(kind);
+  std::vector<float> f(n * 4);
+  for (size_t i = 0; i < n * 4; ++i) f[i] = half_bits_to_float(h16[i]);
+  int rc = ensure_lut_float4(c, kind);
+  if (rc) return rc;
+  PSC_CUDA(cudaMemcpy(c->d_lut[kind], f.data(), n * sizeof(float4), cudaMemcpyHostToDevice), "LUT upload");
+  if (kind == PSC_LUT_SKYVIEW) {
+    const size_t row = PSC_SKYVIEW_W * sizeof(float4);
     PSC_CUDA(cudaMemcpy2DToArray(c->arr_sky, 0, 0, c->d_lut[kind], row, row, PSC_SKYVIEW_H,
                                  cudaMemcpyDeviceToDevice), "sky-view array copy");
   }
@@ -1779,7 +1791,7 @@ int psc_upload_lut(psc_ctx* c, int kind, const uint16_t* rgba16f, size_t count) 
   if (rc) return rc;
   if (!c->d_lut_h[kind]) PSC_CUDA(cudaMalloc(&c->d_lut_h[kind], count * 2), "cudaMalloc LUT");
   PSC_CUDA(cudaMemcpy(c->d_lut_h[kind], rgba16f, count * 2, cudaMemcpyHostToDevice), "LUT upload");
-  ++c->lut_generation;
+  if (kind == PSC_LUT_TRANSMITTANCE || kind == PSC_LUT_MULTISCATTER) ++c->lut_generation;
   return upload_lut_float4(c, kind, rgba16f);
 }
 
@@ -1788,20 +1800,30 @@ int psc_bake_luts(psc_ctx* c, void* stream) {
   if (!c->have_frame) return fail(PSC_ERR_MISSING_INPUT, "psc_set_frame must precede psc_bake_luts");
   int rc = ensure_device(c);
   if (rc) return rc;
-  for (int k = 0; k < 4; ++k)
-    if (!c->d_lut_h[k]) PSC_CUDA(cudaMalloc(&c->d_lut_h[k], lut_texels(k) * 8), "cudaMalloc LUT");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  ++c->lut_generation;
-  if (psc::launch_lut_bakes(c->world, c->frame, c->d_lut_h[0], c->d_lut_h[1], c->d_lut_h[2], c->d_lut_h[3], s))
-    return fail(PSC_ERR_CUDA, "LUT bake launch failed");
-  PSC_CUDA(cudaStreamSynchronize(s), "LUT bake");
-  std::vector<uint16_t> h;
   for (int k = 0; k < 4; ++k) {
-    h.resize(lut_texels(k) * 4);
-    PSC_CUDA(cudaMemcpy(h.data(), c->d_lut_h[k], h.size() * 2, cudaMemcpyDeviceToHost), "LUT readback");
-    rc = upload_lut_float4(c, k, h.data());
+    if (!c->d_lut_h[k]) PSC_CUDA(cudaMalloc(&c->d_lut_h[k], lut_texels(k) * 8), "cudaMalloc LUT");
+    rc = ensure_lut_float4(c, k);
     if (rc) return rc;
   }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // transmittance and multi-scatter depend on the world only: baked when it
+  // changed, or when either LUT was uploaded, since their last bake
+  const bool statics = !(c->static_luts_baked && c->static_luts_generation == c->lut_generation &&
+                         std::memcmp(&c->static_luts_world, &c->world, sizeof(c->world)) == 0);
+  if (psc::launch_lut_bakes(c->world, c->frame, statics, c->d_lut_h, c->d_lut, s))
+    return fail(PSC_ERR_CUDA, "LUT bake launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  c->launches += statics ? 4 : 2;
+  const size_t row = PSC_SKYVIEW_W * sizeof(float4);
+  PSC_CUDA(cudaMemcpy2DToArrayAsync(c->arr_sky, 0, 0, c->d_lut[PSC_LUT_SKYVIEW], row, row, PSC_SKYVIEW_H,
+                                    cudaMemcpyDeviceToDevice, s), "sky-view array copy");
+  if (statics) {
+    ++c->lut_generation;
+    c->static_luts_baked = true;
+    c->static_luts_world = c->world;
+    c->static_luts_generation = c->lut_generation;
+  }
+  for (int k = 0; k < 4; ++k) c->have_lut[k] = true;
+  if (!s) PSC_CUDA(cudaStreamSynchronize(s), "LUT bake");
   return PSC_OK;
 }
 
@@ -1812,6 +1834,7 @@ int psc_download_lut(psc_ctx* c, int kind, uint16_t* out, size_t count) {
   if (!c->d_lut_h[kind]) return fail(PSC_ERR_MISSING_INPUT, "LUT %d not present", kind);
   int rc = ensure_device(c);
   if (rc) return rc;
+  PSC_CUDA(cudaDeviceSynchronize(), "LUT download: device work in flight");  // a bake on any stream
   PSC_CUDA(cudaMemcpy(out, c->d_lut_h[kind], count * 2, cudaMemcpyDeviceToHost), "LUT download");
   return PSC_OK;
 }

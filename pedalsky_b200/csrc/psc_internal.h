@@ -278,9 +278,11 @@ size_t frame_lite_size();
 int launch_view_lut_bakes(const PscWorldUniformsGpu& world, const void* d_frames, uint32_t n,
                           const uint16_t* trans_f16, const uint16_t* ms_f16, float4* sky,
                           float4* ap, cudaStream_t stream);
-// Atmosphere LUT bakes (atmosphere.cu).
-int launch_lut_bakes(const PscWorldUniformsGpu& world, const PscFrameUniformsGpu& frame,
-                     uint16_t* trans_f16, uint16_t* ms_f16, uint16_t* sky_f16,
-                     uint16_t* ap_f16, cudaStream_t stream);
+// Atmosphere LUT bakes (atmosphere.cu): the sky-view and aerial LUTs, and
+// with `statics` first the transmittance and multi-scatter LUTs, each
+// written as RGBA16F (lut_f16[kind]) and as float4 of the same rounded
+// values (lut_f32[kind]), kinds in PSC_LUT_* order.
+int launch_lut_bakes(const PscWorldUniformsGpu& world, const PscFrameUniformsGpu& frame, bool statics,
+                     uint16_t* const lut_f16[4], float4* const lut_f32[4], cudaStream_t stream);
 
 }  // namespace psc

@@ -86,6 +86,63 @@ def test_lut_bake_matches_oracle(oracle):
         sub.close()
 
 
+def test_lut_bake_rebakes_the_world_luts_only_when_their_inputs_change():
+    """psc_bake_luts re-bakes transmittance and multi-scatter only when the
+    world uniforms changed or either LUT was uploaded since their last bake
+    (2 launches, else 4); a bake queued on a stream is seen by a render on
+    that stream."""
+    import ctypes as C
+    torch = _gpu.torch_cuda()
+    from pedalsky_b200.subsystem import subsystem_for_scene
+    s = scenes.precision_1080p(160, 90)
+    sub = subsystem_for_scene(s, luts=None)
+
+    def lut(kind):
+        n = {capi.LUT_TRANSMITTANCE: 256 * 64, capi.LUT_MULTISCATTER: 32 * 32,
+             capi.LUT_SKYVIEW: 192 * 108, capi.LUT_AERIAL: 32 * 32 * 64}[kind] * 4
+        out = np.zeros(n, np.uint16)
+        call("psc_download_lut", sub.handle, kind, capi.ptr(out), n)
+        return out
+
+    def bake(stream=None):
+        n0 = sub.launch_count()
+        call("psc_bake_luts", sub.handle, C.c_void_p(stream.cuda_stream) if stream else None)
+        torch.cuda.synchronize()
+        return sub.launch_count() - n0
+
+    try:
+        ref = {k: lut(k) for k in range(4)}
+        assert bake() == 2
+        for k in range(4):
+            assert np.array_equal(lut(k), ref[k]), k
+        # an upload of the transmittance LUT: the next bake re-bakes both
+        zero = np.zeros_like(ref[capi.LUT_TRANSMITTANCE])
+        call("psc_upload_lut", sub.handle, capi.LUT_TRANSMITTANCE, capi.ptr(zero), zero.size)
+        assert bake() == 4
+        assert np.array_equal(lut(capi.LUT_TRANSMITTANCE), ref[capi.LUT_TRANSMITTANCE])
+        # a denser atmosphere: new transmittance and multi-scatter
+        w = capi.WorldUniformsGpu.from_buffer_copy(s.world)
+        w.mie_scattering[0] *= 2.0
+        call("psc_set_frame", sub.handle, C.byref(s.frame), C.byref(w))
+        assert bake() == 4
+        assert not np.array_equal(lut(capi.LUT_TRANSMITTANCE), ref[capi.LUT_TRANSMITTANCE])
+        assert bake() == 2
+        # back to the scene's world, baked on a side stream, rendered on it
+        call("psc_set_frame", sub.handle, C.byref(s.frame), C.byref(s.world))
+        assert bake() == 4
+        L0, T0 = _gpu.render(s, sub=sub)
+        st = torch.cuda.Stream()
+        call("psc_upload_lut", sub.handle, capi.LUT_SKYVIEW, capi.ptr(np.zeros_like(ref[2])), ref[2].size)
+        with torch.cuda.stream(st):
+            call("psc_bake_luts", sub.handle, C.c_void_p(st.cuda_stream))
+            L1, T1 = _gpu.render(s, sub=sub)
+        assert np.array_equal(L0, L1) and np.array_equal(T0, T1)
+        for k in range(4):
+            assert np.array_equal(lut(k), ref[k]), k
+    finally:
+        sub.close()
+
+
 SCHEDULES = {"plain": capi.SCHED_PLAIN, "fast": capi.SCHED_FAST}
 
 
