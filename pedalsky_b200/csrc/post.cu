@@ -13,9 +13,9 @@
 //     (the reference's 9 offset-bilinear taps are an exact rewriting of it),
 //     then L >= 0, T in [0, 1] and dst = L + dst * T on all four channels.
 // All three are one thread per output pixel, 16x16 CTAs; every index is
-// clamped into its image.  The composite stages its RT footprint in shared
-// memory (k_composite_halfres_tiled) whenever the RT is no larger than the
-// target.
+// clamped into its image.  Whenever the RT is at most half the target per
+// axis (the half-res RT), the composite runs a 2x2 quad of target pixels per
+// thread from one 5x5 RT window (k_composite_halfres_quad).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -146,7 +146,7 @@ __device__ __forceinline__ void cr_weights(float f, float w[4]) {
 // First Catmull-Rom tap + 1 of target pixel x (W wide) over an RT rw wide
 // (the texel left of the sample point), and the fraction f in [0, 1), with
 // every rounding explicit (no contraction into FMAs), so the two composite
-// kernels and the tiled kernel's footprint bounds agree exactly.
+// kernels agree exactly.
 __device__ __forceinline__ int cr_base(uint32_t x, uint32_t W, uint32_t rw, float& f) {
   const float sp = __fmul_rn(__fdiv_rn(__fadd_rn((float)x, 0.5f), (float)W), (float)rw);
   const float b = floorf(__fsub_rn(sp, 0.5f));
@@ -189,61 +189,81 @@ __global__ void k_composite_halfres(const float4* __restrict__ l, const float4* 
   hdr[o] = make_float4(fmaf(d.x, T.x, L.x), fmaf(d.y, T.y, L.y), fmaf(d.z, T.z, L.z), fmaf(d.w, T.w, L.w));
 }
 
-constexpr int kCrTile = 24;  // RT texels per axis staged by one CTA
-
-// k_composite_halfres with the RT footprint of the CTA's 16 x 16 target
-// pixels staged once in shared memory: every RT texel is read from L2 about
-// (footprint / 8)^2 = 2.25 times instead of 16 times per target pixel from
-// L1.  Used while the RT is no larger than the target, where the footprint
-// is at most 20 x 20 texels.  The same taps, weights and order as
-// k_composite_halfres: the same image bit for bit.
-__global__ void __launch_bounds__(256) k_composite_halfres_tiled(const float4* __restrict__ l,
-                                                                 const float4* __restrict__ t, uint32_t rw,
-                                                                 uint32_t rh, float4* __restrict__ hdr,
-                                                                 uint32_t W, uint32_t H) {
-  __shared__ float4 sl[kCrTile][kCrTile], st[kCrTile][kCrTile];
-  const uint32_t x0 = blockIdx.x * 16u, y0 = blockIdx.y * 16u;
-  float f;
-  const int sx0 = cr_base(x0, W, rw, f) - 1, sy0 = cr_base(y0, H, rh, f) - 1;
-  const int sx1 = cr_base(min(x0 + 15u, W - 1u), W, rw, f) + 2;
-  const int sy1 = cr_base(min(y0 + 15u, H - 1u), H, rh, f) + 2;
-  const int nx = min(sx1 - sx0 + 1, kCrTile), ny = min(sy1 - sy0 + 1, kCrTile);
-  for (int i = (int)(threadIdx.y * 16u + threadIdx.x); i < nx * ny; i += 256) {
-    const int jy = i / nx, jx = i - jy * nx;
-    const int idx = clampi(sy0 + jy, (int)rh) * (int)rw + clampi(sx0 + jx, (int)rw);
-    sl[jy][jx] = __ldg(l + idx);
-    st[jy][jx] = __ldg(t + idx);
-  }
-  __syncthreads();
-  const uint32_t x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-  if (x >= W || y >= H) return;
-  float fx, fy;
-  const int bx = cr_base(x, W, rw, fx), by = cr_base(y, H, rh, fy);
-  float wx[4], wy[4];
-  cr_weights(fx, wx);
-  cr_weights(fy, wy);
-  int jx[4], jy[4];
+// k_composite_halfres for a 2x2 quad of target pixels per thread, while the
+// RT is at most half the target per axis: the quad's taps then lie in one
+// 5x5 window of RT texels (neighbouring pixels' first taps differ by at most
+// one), read once per thread a row at a time.  Each row's horizontal
+// 4-tap sums serve both pixel rows of the quad, so a pixel costs 12.5 RT
+// loads instead of 32.  Every pixel sums the same taps with the same
+// weights in the same order as k_composite_halfres: the same image bit for
+// bit.
+__global__ void __launch_bounds__(256) k_composite_halfres_quad(const float4* __restrict__ l,
+                                                                const float4* __restrict__ t, uint32_t rw,
+                                                                uint32_t rh, float4* __restrict__ hdr,
+                                                                uint32_t W, uint32_t H) {
+  const uint32_t x0 = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
+  const uint32_t y0 = 2u * (blockIdx.y * blockDim.y + threadIdx.y);
+  if (x0 >= W || y0 >= H) return;
+  const uint32_t x1 = min(x0 + 1u, W - 1u), y1 = min(y0 + 1u, H - 1u);
+  float fx0, fx1, fy0, fy1;
+  const int bx0 = cr_base(x0, W, rw, fx0), bx1 = cr_base(x1, W, rw, fx1);
+  const int by0 = cr_base(y0, H, rh, fy0), by1 = cr_base(y1, H, rh, fy1);
+  const bool dx = bx1 != bx0, dy = by1 != by0;  // 0 or 1 texel further on
+  float wx0[4], wx1[4], wy0[4], wy1[4];
+  cr_weights(fx0, wx0);
+  cr_weights(fx1, wx1);
+  cr_weights(fy0, wy0);
+  cr_weights(fy1, wy1);
+  int col[5];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {  // tile slot (sx0 + j) holds RT texel clamp(sx0 + j)
-    jx[k] = min(max(bx - 1 + k - sx0, 0), nx - 1);
-    jy[k] = min(max(by - 1 + k - sy0, 0), ny - 1);
-  }
-  float4 acl = f4(0.0f), act = f4(0.0f);
+  for (int c = 0; c < 5; ++c) col[c] = clampi(bx0 - 1 + c, (int)rw);
+  float4 a00l = f4(0.0f), a01l = f4(0.0f), a10l = f4(0.0f), a11l = f4(0.0f);  // a<y><x>
+  float4 a00t = f4(0.0f), a01t = f4(0.0f), a10t = f4(0.0f), a11t = f4(0.0f);
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    float4 rl = f4(0.0f), rt = f4(0.0f);
+  for (int r = 0; r < 5; ++r) {
+    const int row = clampi(by0 - 1 + r, (int)rh) * (int)rw;
+    float4 cl[5], ct[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      cl[c] = __ldg(l + row + col[c]);
+      ct[c] = __ldg(t + row + col[c]);
+    }
+    float4 h0l = f4(0.0f), h1l = f4(0.0f), h0t = f4(0.0f), h1t = f4(0.0f);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      rl = fma4(sl[jy[j]][jx[k]], wx[k], rl);
-      rt = fma4(st[jy[j]][jx[k]], wx[k], rt);
+      h0l = fma4(cl[k], wx0[k], h0l);
+      h0t = fma4(ct[k], wx0[k], h0t);
+      h1l = fma4(dx ? cl[k + 1] : cl[k], wx1[k], h1l);
+      h1t = fma4(dx ? ct[k + 1] : ct[k], wx1[k], h1t);
     }
-    acl = fma4(rl, wy[j], acl);
-    act = fma4(rt, wy[j], act);
+    if (r < 4) {  // row r is tap row r of the upper pixels
+      a00l = fma4(h0l, wy0[r], a00l);
+      a01l = fma4(h1l, wy0[r], a01l);
+      a00t = fma4(h0t, wy0[r], a00t);
+      a01t = fma4(h1t, wy0[r], a01t);
+    }
+    // and tap row r - dy of the lower ones
+    const bool lower = dy ? r >= 1 : r < 4;
+    const float wl = dy ? wy1[r >= 1 ? r - 1 : 0] : wy1[r < 4 ? r : 3];
+    if (lower) {
+      a10l = fma4(h0l, wl, a10l);
+      a11l = fma4(h1l, wl, a11l);
+      a10t = fma4(h0t, wl, a10t);
+      a11t = fma4(h1t, wl, a11t);
+    }
   }
-  const float4 L = max4(acl, f4(0.0f)), T = clamp4(act, f4(0.0f), f4(1.0f));
-  const size_t o = (size_t)y * W + x;
-  const float4 d = hdr[o];
-  hdr[o] = make_float4(fmaf(d.x, T.x, L.x), fmaf(d.y, T.y, L.y), fmaf(d.z, T.z, L.z), fmaf(d.w, T.w, L.w));
+  auto put = [&](uint32_t x, uint32_t y, float4 sl, float4 st) {
+    const float4 L = max4(sl, f4(0.0f)), T = clamp4(st, f4(0.0f), f4(1.0f));
+    const size_t o = (size_t)y * W + x;
+    const float4 d = hdr[o];
+    hdr[o] = make_float4(fmaf(d.x, T.x, L.x), fmaf(d.y, T.y, L.y), fmaf(d.z, T.z, L.z), fmaf(d.w, T.w, L.w));
+  };
+  put(x0, y0, a00l, a00t);
+  if (x0 + 1u < W) put(x0 + 1u, y0, a01l, a01t);
+  if (y0 + 1u < H) {
+    put(x0, y0 + 1u, a10l, a10t);
+    if (x0 + 1u < W) put(x0 + 1u, y0 + 1u, a11l, a11t);
+  }
 }
 
 dim3 grid16(uint32_t w, uint32_t h) { return dim3((w + 15u) / 16u, (h + 15u) / 16u); }
@@ -288,8 +308,9 @@ int launch_taa_resolve(const TaaParams& p, cudaStream_t s) {
 int launch_composite_halfres(const float4* l, const float4* t, uint32_t rw, uint32_t rh, float4* hdr,
                              uint32_t W, uint32_t H, cudaStream_t s) {
   if (W == 0 || H == 0 || rw == 0 || rh == 0) return PSC_OK;
-  if (rw <= W && rh <= H)
-    k_composite_halfres_tiled<<<grid16(W, H), dim3(16, 16), 0, s>>>(l, t, rw, rh, hdr, W, H);
+  if (2u * rw <= W && 2u * rh <= H)  // the half-res RT: quads' first taps differ by at most one
+    k_composite_halfres_quad<<<grid16((W + 1u) / 2u, (H + 1u) / 2u), dim3(16, 16), 0, s>>>(l, t, rw, rh, hdr,
+                                                                                         W, H);
   else
     k_composite_halfres<<<grid16(W, H), dim3(16, 16), 0, s>>>(l, t, rw, rh, hdr, W, H);
   return cudaGetLastError() == cudaSuccess ? PSC_OK : PSC_ERR_CUDA;
