@@ -79,10 +79,12 @@ def test_half_res_march_and_catmull_rom_composite(halfres_ref, oracle_noise, sch
     _check(f"halfres_composite/{sched}/{storage}/{filt}", hdr, ref)
 
 
-def test_composite_halfres_entry_point_matches_oracle():
+@pytest.mark.parametrize("rw,rh,W,H", [(37, 21, 75, 43),   # the quad kernel, odd target edges
+                                        (60, 40, 64, 48),   # more than half: the one-pixel kernel
+                                        (96, 54, 64, 36)])  # an RT larger than its target
+def test_composite_halfres_entry_point_matches_oracle(rw, rh, W, H):
     torch = _torch()
     rng = np.random.default_rng(5)
-    rw, rh, W, H = 37, 21, 75, 43
     L = rng.uniform(-100.0, 4000.0, (rh, rw, 4)).astype(np.float32)
     T = rng.uniform(-0.2, 1.2, (rh, rw, 4)).astype(np.float32)
     bg = rng.uniform(100.0, 9000.0, (H, W, 4)).astype(np.float32)
