@@ -189,14 +189,49 @@ __global__ void k_composite_halfres(const float4* __restrict__ l, const float4* 
   hdr[o] = make_float4(fmaf(d.x, T.x, L.x), fmaf(d.y, T.y, L.y), fmaf(d.z, T.z, L.z), fmaf(d.w, T.w, L.w));
 }
 
+// The Catmull-Rom sums of one RT array for a 2x2 quad of target pixels
+// (k_composite_halfres_quad): rows r = 0..4 of the 5x5 window starting at
+// texel (col[0], by0 - 1), each row's horizontal sums serving both pixel
+// rows; a<y><x> receive the quad's four sums.
+__device__ __forceinline__ void cr_quad_sums(const float4* __restrict__ src, const int col[5], int by0,
+                                             uint32_t rw, uint32_t rh, bool dx, bool dy, const float wx0[4],
+                                             const float wx1[4], const float wy0[4], const float wy1[4],
+                                             float4& a00, float4& a01, float4& a10, float4& a11) {
+  a00 = a01 = a10 = a11 = f4(0.0f);
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    const int row = clampi(by0 - 1 + r, (int)rh) * (int)rw;
+    float4 cv[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) cv[c] = __ldg(src + row + col[c]);
+    float4 h0 = f4(0.0f), h1 = f4(0.0f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      h0 = fma4(cv[k], wx0[k], h0);
+      h1 = fma4(dx ? cv[k + 1] : cv[k], wx1[k], h1);
+    }
+    if (r < 4) {  // row r is tap row r of the upper pixels
+      a00 = fma4(h0, wy0[r], a00);
+      a01 = fma4(h1, wy0[r], a01);
+    }
+    // and tap row r - dy of the lower ones
+    if (dy ? r >= 1 : r < 4) {
+      const float wl = dy ? wy1[r >= 1 ? r - 1 : 0] : wy1[r < 4 ? r : 3];
+      a10 = fma4(h0, wl, a10);
+      a11 = fma4(h1, wl, a11);
+    }
+  }
+}
+
 // k_composite_halfres for a 2x2 quad of target pixels per thread, while the
 // RT is at most half the target per axis: the quad's taps then lie in one
 // 5x5 window of RT texels (neighbouring pixels' first taps differ by at most
-// one), read once per thread a row at a time.  Each row's horizontal
-// 4-tap sums serve both pixel rows of the quad, so a pixel costs 12.5 RT
-// loads instead of 32.  Every pixel sums the same taps with the same
-// weights in the same order as k_composite_halfres: the same image bit for
-// bit.
+// one), read once per thread a row at a time, the luminance window and then
+// the transmittance window (so one array's row is live at a time).  Each
+// row's horizontal 4-tap sums serve both pixel rows of the quad, so a pixel
+// costs 12.5 RT loads instead of 32.  Every pixel sums the same taps with
+// the same weights in the same order as k_composite_halfres: the same image
+// bit for bit.
 __global__ void __launch_bounds__(256) k_composite_halfres_quad(const float4* __restrict__ l,
                                                                 const float4* __restrict__ t, uint32_t rw,
                                                                 uint32_t rh, float4* __restrict__ hdr,
@@ -217,41 +252,9 @@ __global__ void __launch_bounds__(256) k_composite_halfres_quad(const float4* __
   int col[5];
 #pragma unroll
   for (int c = 0; c < 5; ++c) col[c] = clampi(bx0 - 1 + c, (int)rw);
-  float4 a00l = f4(0.0f), a01l = f4(0.0f), a10l = f4(0.0f), a11l = f4(0.0f);  // a<y><x>
-  float4 a00t = f4(0.0f), a01t = f4(0.0f), a10t = f4(0.0f), a11t = f4(0.0f);
-#pragma unroll
-  for (int r = 0; r < 5; ++r) {
-    const int row = clampi(by0 - 1 + r, (int)rh) * (int)rw;
-    float4 cl[5], ct[5];
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      cl[c] = __ldg(l + row + col[c]);
-      ct[c] = __ldg(t + row + col[c]);
-    }
-    float4 h0l = f4(0.0f), h1l = f4(0.0f), h0t = f4(0.0f), h1t = f4(0.0f);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      h0l = fma4(cl[k], wx0[k], h0l);
-      h0t = fma4(ct[k], wx0[k], h0t);
-      h1l = fma4(dx ? cl[k + 1] : cl[k], wx1[k], h1l);
-      h1t = fma4(dx ? ct[k + 1] : ct[k], wx1[k], h1t);
-    }
-    if (r < 4) {  // row r is tap row r of the upper pixels
-      a00l = fma4(h0l, wy0[r], a00l);
-      a01l = fma4(h1l, wy0[r], a01l);
-      a00t = fma4(h0t, wy0[r], a00t);
-      a01t = fma4(h1t, wy0[r], a01t);
-    }
-    // and tap row r - dy of the lower ones
-    const bool lower = dy ? r >= 1 : r < 4;
-    const float wl = dy ? wy1[r >= 1 ? r - 1 : 0] : wy1[r < 4 ? r : 3];
-    if (lower) {
-      a10l = fma4(h0l, wl, a10l);
-      a11l = fma4(h1l, wl, a11l);
-      a10t = fma4(h0t, wl, a10t);
-      a11t = fma4(h1t, wl, a11t);
-    }
-  }
+  float4 a00l, a01l, a10l, a11l, a00t, a01t, a10t, a11t;  // a<y><x>
+  cr_quad_sums(l, col, by0, rw, rh, dx, dy, wx0, wx1, wy0, wy1, a00l, a01l, a10l, a11l);
+  cr_quad_sums(t, col, by0, rw, rh, dx, dy, wx0, wx1, wy0, wy1, a00t, a01t, a10t, a11t);
   auto put = [&](uint32_t x, uint32_t y, float4 sl, float4 st) {
     const float4 L = max4(sl, f4(0.0f)), T = clamp4(st, f4(0.0f), f4(1.0f));
     const size_t o = (size_t)y * W + x;
