@@ -78,19 +78,27 @@ __device__ __forceinline__ float dist_boundary(const Atmo& A, float3 p, float3 d
   return fmaxf(tm, 0.0f);
 }
 
+__device__ __forceinline__ float3 texel_rgb(uint2 w) {
+  const __half2 lo = *reinterpret_cast<const __half2*>(&w.x), hi = *reinterpret_cast<const __half2*>(&w.y);
+  return f3(__low2float(lo), __high2float(lo), __low2float(hi));
+}
+
 __device__ float3 sample_rgba16f(const uint16_t* lut, int W, int H, float u, float v) {
   const float x = u * (float)W - 0.5f, y = v * (float)H - 0.5f;
   const float fx = floorf(x), fy = floorf(y);
   const float wx = x - fx, wy = y - fy;
   const int x0 = min(max((int)fx, 0), W - 1), x1 = min(max((int)fx + 1, 0), W - 1);
   const int y0 = min(max((int)fy, 0), H - 1), y1 = min(max((int)fy + 1, 0), H - 1);
-  const __half* h = reinterpret_cast<const __half*>(lut);
+  // one 8-byte load per texel (RGBA16F), RGB used
+  const uint2* q = reinterpret_cast<const uint2*>(lut);
+  const float3 a = texel_rgb(q[y0 * W + x0]), b = texel_rgb(q[y0 * W + x1]);
+  const float3 cc = texel_rgb(q[y1 * W + x0]), d = texel_rgb(q[y1 * W + x1]);
+  const float ta[3] = {a.x, a.y, a.z}, tb[3] = {b.x, b.y, b.z}, tc[3] = {cc.x, cc.y, cc.z},
+              td[3] = {d.x, d.y, d.z};
   float o[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const float a = __half2float(h[(y0 * W + x0) * 4 + c]), b = __half2float(h[(y0 * W + x1) * 4 + c]);
-    const float cc = __half2float(h[(y1 * W + x0) * 4 + c]), d = __half2float(h[(y1 * W + x1) * 4 + c]);
-    const float top = fmaf(wx, b - a, a), bot = fmaf(wx, d - cc, cc);
+    const float top = fmaf(wx, tb[c] - ta[c], ta[c]), bot = fmaf(wx, td[c] - tc[c], tc[c]);
     o[c] = fmaf(wy, bot - top, top);
   }
   return f3(o[0], o[1], o[2]);
